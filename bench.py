@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark: FWI gradient throughput of the B200 acoustic propagator.
+
+Workload (one "step" = one full gradient evaluation): the 400 x 1200 model,
+dx 10 m, dt 0.8 ms, 3000 time steps, 8th-order stencil, 30-cell PML, 32
+Ricker shots, 1200 receivers, L2 misfit on pressure against data modelled in
+the true model; forward with checkpoints, residual, hand-written adjoint,
+dL/dvp.  Metric: Gcell-updates/s, one unit = one (shot, padded cell, time
+step) forward update plus its adjoint update (recompute not counted).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints ONE JSON line on rank 0.  Under torchrun (N > 1) every rank models
+its own 32 shots of the same survey (weak scaling) and the per-rank
+gradients are summed with one NCCL all-reduce inside the timed step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FWI gradient Gcell-updates/s (fwd+adjoint, batched) vs plain fwd kernel, 1 B200"
+UNIT = "Gcell-updates/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nt", type=int, default=3000, help="time steps of the workload (3000 = full)")
+    ap.add_argument("--no-extras", action="store_true")
+    return ap.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get(kernel, {}).get("dram_bytes_per_launch")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sms.append(float(parts[1]))
+                    maxes.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        if not sms:
+            return None
+        return {"sm_mhz": float(np.median(sms)), "sm_max_mhz": float(max(maxes)), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (oracle restatement of the reference; never the product path)
+# ---------------------------------------------------------------------------
+def cpu_gradient_rate(w, n_shots: int, nt: int, reps: int = 1):
+    from oracle import oracle as orc
+    from geobrain_b200.wave.boundary import bc_pml
+    damp = bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp.max()), free_surface=False).astype(np.float32)
+    S = n_shots
+    sx = w.src_x[np.linspace(0, w.n_shots - 1, S).astype(int)]
+    kw = dict(nz=w.nz, nx=w.nx, dz=w.dx, nt=nt, dt=w.dt, nabc=w.nabc, free_surface=False, src_x=sx,
+              src_z=np.ones(S, np.int64), src_v=np.tile(w.wavelet[:nt], (S, 1)), rcv_x=w.rcv_x, rcv_z=w.rcv_z,
+              damp=damp, vp=w.vp, rho=w.rho, half=w.fd_order // 2, dtype=np.float32)
+    res = np.random.default_rng(0).standard_normal((S, nt, w.rcv_x.size)).astype(np.float32)
+    best = None
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        orc.gradient(**kw, res_p=res)
+        el = time.perf_counter() - t0
+        best = el if best is None else min(best, el)
+    units = S * w.cells * nt
+    return units / best / 1e9, orc.max_threads(), f"{S} shots x {nt} steps of the {w.nz}x{w.nx} grid " \
+                                                    f"(forward + adjoint, fp32 C oracle, OpenMP)"
+
+
+def run_reference_arm(args):
+    """--impl reference: the reference algorithm's CPU restatement on the host
+    cores, same metric and config, bounded sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from geobrain_b200 import synthetic
+    w = synthetic.fwi_400x1200(nt=args.nt)
+    S, nt = 2, min(60, args.nt)
+    for _ in range(max(args.warmup, 0)):
+        cpu_gradient_rate(w, S, nt)
+    rates = []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r, cores, sample = cpu_gradient_rate(w, S, nt)
+        rates.append(r)
+    el = time.perf_counter() - t0
+    v = float(np.mean(rates))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "fwi_400x1200", "fd_order": 8, "n_shots": 32, "nt": args.nt,
+                   "grid": [400, 1200], "nabc": 30, "sample": sample},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from geobrain_b200 import synthetic, wave
+    from geobrain_b200.wave import engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    w = synthetic.fwi_400x1200(nt=args.nt)
+    S = w.n_shots
+    # weak scaling: rank r models shots shifted by r / world of a shot spacing
+    if world > 1:
+        spacing = (w.nx - 1) / (S + 1)
+        w.src_x = np.clip(np.round(w.src_x + rank * spacing / world), 0, w.nx - 1).astype(np.int64)
+    damp = wave.bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp_true.max()), free_surface=False)
+    damp_t = torch.tensor(damp, dtype=torch.float32, device=dev)
+    src_v = torch.tensor(np.tile(w.wavelet, (S, 1)), device=dev)
+    common = dict(nx=w.nx, nz=w.nz, dx=w.dx, dz=w.dx, nt=w.nt, dt=w.dt, nabc=w.nabc, free_surface=False,
+                  src_x=w.src_x, src_z=w.src_z, src_n=S, src_v=src_v, rcv_x=w.rcv_x, rcv_z=w.rcv_z,
+                  rcv_n=w.rcv_x.size, damp=damp_t, device=dev, fd_order=w.fd_order)
+    rho_t = torch.tensor(w.rho, device=dev)
+    with torch.no_grad():
+        d_obs = wave.acoustic_forward_kernel(vp=torch.tensor(w.vp_true, device=dev), rho=rho_t, want_energy=False,
+                                             **common)["p"].contiguous()
+
+    def gradient_step(vp_dev, d_obs_dev):
+        vp = vp_dev.detach().requires_grad_(True)
+        out = wave.acoustic_forward_kernel(vp=vp, rho=rho_t, **common)
+        res = out["p"] - d_obs_dev
+        loss = 0.5 * (res * res).sum()
+        loss.backward()
+        g = vp.grad
+        if world > 1:
+            dist.all_reduce(g)
+        return g, loss
+
+    vp0 = torch.tensor(w.vp, device=dev)
+    geo = engine.Geometry(w.nz, w.nx, w.nabc, w.nt, float(w.dt), float(w.dx), w.fd_order // 2, False)
+    plan = engine.get_plan(geo, w.src_x, w.src_z, w.rcv_x, w.rcv_z)
+
+    # CPU baseline first (rank 0, N = 1 only), outside every timed region
+    cpu = None
+    if rank == 0 and world == 1:
+        v, cores, sample = cpu_gradient_rate(w, 2, min(60, w.nt))
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+
+    for _ in range(max(args.warmup, 3)):
+        gradient_step(vp0, d_obs)
+    torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = torch.tensor([e0.elapsed_time(e1)], device=dev)
+        if world > 1:
+            dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+        return float(ms.item())
+
+    plan.set_profiling(True)
+    with ClockSampler(local) as clk:
+        ms_total = timed(lambda: gradient_step(vp0, d_obs), args.steps)
+    prof = plan.profile()
+    plan.set_profiling(False)
+    clocks = clk.summary()
+
+    units = S * w.cells * w.nt * world
+    ms_step = ms_total / args.steps
+    value = units / (ms_step * 1e-3) / 1e9
+
+    # end to end: pinned host inputs copied in, gradient and loss read back, every step
+    vp_host = torch.tensor(w.vp).pin_memory()
+    dobs_host = d_obs.cpu().pin_memory()
+    g_host = torch.empty((w.nz, w.nx), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        vp_d = vp_host.to(dev, non_blocking=True)
+        do_d = dobs_host.to(dev, non_blocking=True)
+        g, loss = gradient_step(vp_d, do_d)
+        g_host.copy_(g, non_blocking=True)
+        return float(loss.item())
+
+    e2e_step()
+    ms_e2e = timed(e2e_step, args.steps) / args.steps
+    h2d = vp_host.numel() * 4 + dobs_host.numel() * 4
+    d2h = g_host.numel() * 4 + 4
+
+    # roofline of the kernels, from the CUDA-event phase timings of the timed region
+    peak, peak_kind = measured_peaks()
+    nt, cells = w.nt, w.cells
+    per_step_fwd = prof["forward_ms"] / args.steps / nt          # ms per forward launch (fwd + energy)
+    per_step_rec = prof["recompute_ms"] / args.steps / nt        # ms per recompute launch (fwd + imaging)
+    per_step_adj = prof["adjoint_ms"] / args.steps / nt          # ms per adjoint launch
+    b_fwd = S * cells * (24 + 8 / S)                              # fields r+w, a1 / a2 shared by the shots
+    b_rec = S * cells * (24 + 4 + 8 / S)                          # + imaging field written
+    b_adj = S * cells * (24 + 4 + 16 / S)                         # + imaging read, coefficients, gradient sums
+    kern = {
+        "fwd_step (forward)": {"ms_per_launch": per_step_fwd, "bytes_per_launch": b_fwd},
+        "fwd_step (recompute)": {"ms_per_launch": per_step_rec, "bytes_per_launch": b_rec},
+        "adj_step": {"ms_per_launch": per_step_adj, "bytes_per_launch": b_adj},
+    }
+    for k, v in kern.items():
+        v["achieved_gbs"] = v["bytes_per_launch"] / (v["ms_per_launch"] * 1e-3) / 1e9 if v["ms_per_launch"] else 0
+        v["frac"] = v["achieved_gbs"] / peak
+    # dominant kernel by share of the timed region; fwd_step runs twice per
+    # gradient (forward pass and recompute), adj_step once
+    t_fwd = (per_step_fwd + per_step_rec) * nt
+    t_adj = per_step_adj * nt
+    if t_fwd >= t_adj:
+        tname = "fwd_step"
+        achieved = (b_fwd + b_rec) / ((per_step_fwd + per_step_rec) * 1e-3) / 1e9
+    else:
+        tname = "adj_step"
+        achieved = b_adj / (per_step_adj * 1e-3) / 1e9
+    roofline = {"kernel": tname, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak,
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s",
+                "share_of_step": max(t_fwd, t_adj) / ms_step, "traffic": ncu_traffic(tname)}
+    grad_bytes = units / world * (56 + 16 / S)
+    grad_roof = {"algorithmic_bytes_per_unit": 56 + 16 / S,
+                 "achieved": grad_bytes / (ms_step * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                 "frac": grad_bytes / (ms_step * 1e-3) / 1e9 / peak}
+
+    extras = {}
+    if not args.no_extras and world == 1:
+        extras = plain_forward_rates(torch, wave, synthetic, dev)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian-field model, Ricker shots)",
+        "config": {"workload": "fwi_400x1200", "grid": [w.nz, w.nx], "nabc": w.nabc, "dx": w.dx, "dt": w.dt,
+                   "nt": w.nt, "fd_order": w.fd_order, "n_shots_per_gpu": S, "n_receivers": int(w.rcv_x.size),
+                   "misfit": "L2 on pressure", "checkpoints": "fp32, auto segment length",
+                   "l2": "inputs larger than L2 (fields 2 x 222 MB per state, no flush needed)",
+                   "parallelism": f"shots{world}" if world > 1 else "single GPU"},
+        "e2e": {"value": units / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e},
+        "roofline": roofline,
+        "gradient_roofline": grad_roof,
+        "kernels": kern,
+        "phase_ms_per_step": {k: prof[k] / args.steps for k in ("forward_ms", "recompute_ms", "adjoint_ms")},
+        "gpu_launches": int(prof["launches"]),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+        "extras": extras,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def plain_forward_rates(torch, wave, synthetic, dev):
+    """Plain forward kernel rates beside the gradient: the 400 x 1200 grid
+    with one shot and with 32 shots, and the 100 x 200 4th-order workload."""
+    out = {}
+    for name, w, shots in (("fwd_400x1200_1shot", synthetic.fwi_400x1200(nt=3000, n_shots=1), 1),
+                           ("fwd_400x1200_32shots", synthetic.fwi_400x1200(nt=1000), 32),
+                           ("fwd_100x200_1shot", synthetic.plain_forward_100x200(), 1)):
+        damp = torch.tensor(wave.bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp.max()), False),
+                            dtype=torch.float32, device=dev)
+        kw = dict(nx=w.nx, nz=w.nz, dx=w.dx, dz=w.dx, nt=w.nt, dt=w.dt, nabc=w.nabc, free_surface=False,
+                  src_x=w.src_x, src_z=w.src_z, src_n=w.n_shots,
+                  src_v=torch.tensor(np.tile(w.wavelet, (w.n_shots, 1)), device=dev), rcv_x=w.rcv_x,
+                  rcv_z=w.rcv_z, rcv_n=w.rcv_x.size, damp=damp, vp=torch.tensor(w.vp, device=dev),
+                  rho=torch.tensor(w.rho, device=dev), device=dev, fd_order=w.fd_order)
+        for _ in range(2):
+            wave.acoustic_forward_kernel(**kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        reps = 3
+        for _ in range(reps):
+            wave.acoustic_forward_kernel(**kw)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = {"gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms,
+                     "fd_order": w.fd_order, "nt": w.nt, "shots": w.n_shots}
+    return out
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,253 @@
+"""Host-side driver of the C ABI: plans, workspaces, checkpoint storage and
+the autograd Function around the hand-written adjoint.
+
+Everything here runs the CUDA library; there is no CPU path.  A call on a
+non-CUDA device, in a dtype other than float32, or without the built
+library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from collections import OrderedDict
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from .. import _lib
+
+FD_ORDERS = {4: 2, 8: 4}          # fd_order -> stencil half-width
+_PLAN_CACHE: "OrderedDict[tuple, Plan]" = OrderedDict()
+_PLAN_CACHE_SIZE = 32
+
+
+def _i64(a) -> np.ndarray:
+    if torch.is_tensor(a):
+        a = a.detach().cpu().numpy()
+    return np.ascontiguousarray(np.atleast_1d(np.asarray(a)).astype(np.int64))
+
+
+@dataclass(frozen=True)
+class Geometry:
+    nz: int
+    nx: int
+    nabc: int
+    nt: int
+    dt: float
+    dx: float
+    half: int
+    free_surface: bool
+
+
+class Plan:
+    """A gb_plan: validated geometry, receiver binning and workspace sizes."""
+
+    def __init__(self, geo: Geometry, src_x, src_z, rcv_x, rcv_z):
+        self.geo = geo
+        self.src_x, self.src_z = _i64(src_x), _i64(src_z)
+        self.rcv_x, self.rcv_z = _i64(rcv_x), _i64(rcv_z)
+        if self.src_x.shape != self.src_z.shape or self.rcv_x.shape != self.rcv_z.shape:
+            raise ValueError("position arrays must pair up (x and z of equal length)")
+        self.n_shots = int(self.src_x.size)
+        self.n_rcv = int(self.rcv_x.size)
+        self.desc = _lib.ModelDesc(geo.nz, geo.nx, geo.nabc, geo.nt, self.n_shots, self.n_rcv, geo.half,
+                                   int(geo.free_surface), geo.dt, geo.dx)
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self._lib.gb_plan_create(ctypes.byref(self.desc), self.src_x.ctypes.data, self.src_z.ctypes.data,
+                                      self.rcv_x.ctypes.data, self.rcv_z.ctypes.data, ctypes.byref(h))
+        if rc != _lib.GB_OK:
+            msg = self._lib.gb_last_error().decode()
+            raise ValueError(msg) if rc == _lib.GB_E_ARG else _lib.GbError(rc, msg)
+        self.h = h
+        self.tiling = (0, 0)
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value:
+            self._lib.gb_plan_destroy(h)
+            self.h = None
+
+    def set_tiling(self, tile_rows: int = 0, shots_per_cta: int = 0) -> None:
+        _lib.check(self._lib.gb_plan_set_tiling(self.h, int(tile_rows), int(shots_per_cta)))
+        self.tiling = (tile_rows, shots_per_cta)
+
+    def set_profiling(self, enable: bool) -> None:
+        _lib.check(self._lib.gb_plan_set_profiling(self.h, int(enable)))
+
+    def profile(self) -> dict:
+        """Milliseconds per phase (forward loop, recompute, adjoint) and kernel
+        launches since the last call (needs set_profiling(True))."""
+        f, r, a = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        n = ctypes.c_longlong()
+        _lib.check(self._lib.gb_plan_profile(self.h, ctypes.byref(f), ctypes.byref(r), ctypes.byref(a),
+                                             ctypes.byref(n)))
+        return {"forward_ms": f.value, "recompute_ms": r.value, "adjoint_ms": a.value, "launches": n.value}
+
+    def workspace_bytes(self, with_gradient: bool = False, checkpoint_every: int = 0) -> int:
+        return int(self._lib.gb_plan_workspace_bytes(self.h, int(with_gradient), int(checkpoint_every)))
+
+    def checkpoint_bytes(self, checkpoint_every: int, fmt: str) -> int:
+        return int(self._lib.gb_plan_checkpoint_bytes(self.h, int(checkpoint_every), _lib.CKPT_FORMATS[fmt]))
+
+
+def get_plan(geo: Geometry, src_x, src_z, rcv_x, rcv_z) -> Plan:
+    sx, sz, rx, rz = _i64(src_x), _i64(src_z), _i64(rcv_x), _i64(rcv_z)
+    key = (geo, sx.tobytes(), sz.tobytes(), rx.tobytes(), rz.tobytes())
+    plan = _PLAN_CACHE.get(key)
+    if plan is None:
+        plan = Plan(geo, sx, sz, rx, rz)
+        _PLAN_CACHE[key] = plan
+        if len(_PLAN_CACHE) > _PLAN_CACHE_SIZE:
+            _PLAN_CACHE.popitem(last=False)
+    else:
+        _PLAN_CACHE.move_to_end(key)
+    return plan
+
+
+def require_cuda(t: torch.Tensor, name: str) -> None:
+    if not t.is_cuda:
+        raise ValueError(f"geobrain_b200 runs on CUDA devices only ({name} is on {t.device})")
+
+
+def workspace(nbytes: int, device) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+
+
+def stream_handle(device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+def run_forward(plan: Plan, vp: torch.Tensor, rho: torch.Tensor, damp: torch.Tensor, src_v: torch.Tensor, *,
+                want_energy: bool = True, snapshot_every: int = 0, checkpoints: Optional[torch.Tensor] = None,
+                checkpoint_every: int = 0, ckpt_format: str = "fp32"):
+    """One gb_forward call.  Returns (p, vx, vz, energies or None, snapshots or None)."""
+    g = plan.geo
+    dev = vp.device
+    S, NR, nt = plan.n_shots, plan.n_rcv, g.nt
+    f32 = dict(device=dev, dtype=torch.float32)
+    traces = [torch.empty((S, nt, NR), **f32) for _ in range(3)]
+    energies = [torch.empty((g.nz, g.nx), **f32) for _ in range(3)] if want_energy else None
+    nsnap = (nt + snapshot_every - 1) // snapshot_every if snapshot_every > 0 else 0
+    snaps = torch.empty((nsnap, g.nz, g.nx), **f32) if nsnap else None
+    ws = workspace(plan.workspace_bytes(False, checkpoint_every), dev)
+    L = plan._lib
+    with torch.cuda.device(dev):
+        rc = L.gb_forward(plan.h, vp.data_ptr(), rho.data_ptr(), damp.data_ptr(), src_v.data_ptr(),
+                          *[t.data_ptr() for t in traces],
+                          *([e.data_ptr() for e in energies] if energies else [None, None, None]),
+                          int(snapshot_every), _lib.ptr(snaps), _lib.ptr(checkpoints), int(checkpoint_every),
+                          _lib.CKPT_FORMATS[ckpt_format], ws.data_ptr(), ws.numel(), stream_handle(dev))
+    _lib.check(rc)
+    return traces[0], traces[1], traces[2], energies, snaps
+
+
+def pack_output(plan: Plan, p, vx, vz, energies, snaps) -> dict:
+    """The dict acoustic_forward_kernel returns (snapshots go to the CPU, as
+    in the reference, acoustic_2d.py:484-487)."""
+    g = plan.geo
+    if energies is None:
+        energies = [torch.zeros((g.nz, g.nx), device=p.device, dtype=torch.float32) for _ in range(3)]
+    out = {"p": p, "vx": vx, "vz": vz, "forward_wavefield_p": energies[0],
+           "forward_wavefield_vx": energies[1], "forward_wavefield_vz": energies[2]}
+    if snaps is not None:
+        out["snapshots"] = snaps.cpu()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Gradient: checkpointed forward + hand-written adjoint behind autograd
+# ---------------------------------------------------------------------------
+def choose_checkpoint_every(plan: Plan, checkpoint_segments: int = 1, checkpoint_every: int = 0,
+                            fmt: str = "fp32", with_rho: bool = False) -> int:
+    """Segment length K: explicit checkpoint_every wins; otherwise the K that
+    minimises checkpoint storage + one segment of imaging fields
+    (K ~ sqrt(nt * state_bytes / imaging_bytes_per_step)), and never fewer
+    segments than the caller's checkpoint_segments asks for."""
+    nt = plan.geo.nt
+    if checkpoint_every > 0:
+        return min(int(checkpoint_every), nt)
+    state = plan.checkpoint_bytes(1, fmt)                              # one stored state
+    img_step = plan.checkpoint_bytes(1, "fp32") / 3 * (3 if with_rho else 1)   # imaging fields of one step
+    k = int(max(1, round(math.sqrt(nt * state / max(img_step, 1.0)))))
+    k = min(k, max(1, -(-nt // max(1, checkpoint_segments))))
+    return max(1, min(k, nt))
+
+
+def run_backward(plan: Plan, vp, rho, damp, src_v, res_p, res_vx, res_vz, checkpoints, checkpoint_every: int,
+                 fmt: str, want_rho: bool):
+    g = plan.geo
+    dev = vp.device
+    grad_vp = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32)
+    grad_rho = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32) if want_rho else None
+    ws = workspace(plan.workspace_bytes(2 if want_rho else 1, checkpoint_every), dev)
+    with torch.cuda.device(dev):
+        rc = plan._lib.gb_backward(plan.h, vp.data_ptr(), rho.data_ptr(), damp.data_ptr(), src_v.data_ptr(),
+                                   _lib.ptr(res_p), _lib.ptr(res_vx), _lib.ptr(res_vz), checkpoints.data_ptr(),
+                                   int(checkpoint_every), _lib.CKPT_FORMATS[fmt], grad_vp.data_ptr(),
+                                   _lib.ptr(grad_rho), ws.data_ptr(), ws.numel(), stream_handle(dev))
+    _lib.check(rc)
+    return grad_vp, grad_rho
+
+
+class AcousticFunction(torch.autograd.Function):
+    """Traces (p, vx, vz) as a differentiable function of (vp, rho).
+
+    forward: gb_forward keeping checkpoints every K steps (fp32, or bf16 /
+    fp16 with per-snapshot scales); backward: gb_backward (recompute +
+    adjoint + imaging), in place of autograd through ~40 ops per step
+    (geobrain/physics/wave/kernels/acoustic_2d.py:448-460)."""
+
+    @staticmethod
+    def forward(ctx, vp, rho, plan, damp, src_v, opts):
+        vp32 = vp.detach().to(torch.float32).contiguous()
+        rho32 = rho.detach().to(torch.float32).contiguous()
+        K = opts["checkpoint_every"]
+        ckpt = torch.empty(plan.checkpoint_bytes(K, opts["fmt"]), dtype=torch.uint8, device=vp.device)
+        p, vx, vz, en, snaps = run_forward(plan, vp32, rho32, damp, src_v, want_energy=opts["want_energy"],
+                                           snapshot_every=opts["snapshot_every"], checkpoints=ckpt,
+                                           checkpoint_every=K, ckpt_format=opts["fmt"])
+        ctx.plan, ctx.opts = plan, opts
+        ctx.save_for_backward(vp32, rho32, damp, src_v, ckpt)
+        if en is None:
+            en = [torch.zeros((plan.geo.nz, plan.geo.nx), device=vp.device) for _ in range(3)]
+        snaps = snaps if snaps is not None else torch.empty(0, device=vp.device)
+        ctx.mark_non_differentiable(*en, snaps)
+        return p, vx, vz, en[0], en[1], en[2], snaps
+
+    @staticmethod
+    def backward(ctx, gp, gvx, gvz, *unused):
+        vp32, rho32, damp, src_v, ckpt = ctx.saved_tensors
+        need_vp, need_rho = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        if not (need_vp or need_rho):
+            return None, None, None, None, None, None
+        res = [None if t is None else t.to(torch.float32).contiguous() for t in (gp, gvx, gvz)]
+        if all(r is None for r in res):
+            z = torch.zeros_like(vp32)
+            return (z if need_vp else None), (z.clone() if need_rho else None), None, None, None, None
+        gvp, grho = run_backward(ctx.plan, vp32, rho32, damp, src_v, *res, ckpt, ctx.opts["checkpoint_every"],
+                                 ctx.opts["fmt"], need_rho)
+        return (gvp if need_vp else None), (grho if need_rho else None), None, None, None, None
+
+
+def differentiable_forward(plan: Plan, vp, rho, damp, src_v, *, device, snapshot_every: int = 0,
+                           checkpoint_segments: int = 1, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
+                           want_energy: bool = True) -> dict:
+    if snapshot_dtype not in _lib.CKPT_FORMATS:
+        raise ValueError(f"snapshot_dtype must be one of {sorted(_lib.CKPT_FORMATS)}")
+    need_rho = bool(getattr(rho, "requires_grad", False))
+    vp_t = vp if torch.is_tensor(vp) else torch.as_tensor(vp)
+    rho_t = rho if torch.is_tensor(rho) else torch.as_tensor(rho)
+    for name, t in (("vp", vp_t), ("rho", rho_t)):
+        if t.device != device:
+            raise ValueError(f"{name} is on {t.device}, expected {device}")
+    K = choose_checkpoint_every(plan, checkpoint_segments, checkpoint_every, snapshot_dtype, need_rho)
+    opts = dict(checkpoint_every=K, fmt=snapshot_dtype, want_energy=want_energy, snapshot_every=snapshot_every)
+    p, vx, vz, e0, e1, e2, snaps = AcousticFunction.apply(vp_t, rho_t, plan, damp, src_v, opts)
+    out = {"p": p, "vx": vx, "vz": vz, "forward_wavefield_p": e0, "forward_wavefield_vx": e1,
+           "forward_wavefield_vz": e2}
+    if snapshot_every > 0:
+        out["snapshots"] = snaps.detach().cpu()
+    return out

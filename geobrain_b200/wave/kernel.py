@@ -1,0 +1,94 @@
+"""Kernel-level entry points with the reference's call signatures.
+
+``acoustic_forward_kernel`` is a drop-in for
+geobrain/physics/wave/kernels/acoustic_2d.py:294-501: same positional and
+keyword arguments, same output dict (p/vx/vz traces (src_n, nt, rcv_n),
+forward_wavefield_{p,vx,vz} (nz, nx), and 'snapshots' (n, nz, nx) on the CPU
+when snapshot_every > 0), computed by the CUDA library.  When vp or rho
+requires grad, the traces are differentiable through the hand-written
+adjoint (engine.AcousticFunction); the energy maps are detached, as in the
+reference.
+
+Additions, all keyword-only with defaults that keep the reference's
+behaviour: fd_order (4 or 8), checkpoint_every / snapshot_dtype (gradient
+memory), want_energy (skip the energy sums).
+"""
+from __future__ import annotations
+
+import torch
+from torch import Tensor
+
+from . import engine
+
+
+def pad_model(v: Tensor, pml: int, nz: int, nx: int, device: torch.device = torch.device("cpu")) -> Tensor:
+    """Edge-replicating pad of an (nz, nx) model to (nz + 2 pml, nx + 2 pml)
+    (acoustic_2d.py:18-66).  The CUDA path pads inside its coefficient kernel;
+    this host version is kept for API parity."""
+    iz = torch.clamp(torch.arange(nz + 2 * pml, device=v.device) - pml, 0, nz - 1)
+    ix = torch.clamp(torch.arange(nx + 2 * pml, device=v.device) - pml, 0, nx - 1)
+    return v[iz][:, ix].to(device)
+
+
+def _as_f32(t, device, name):
+    if not torch.is_tensor(t):
+        t = torch.as_tensor(t)
+    if t.dtype not in (torch.float32, torch.float64, torch.float16, torch.bfloat16):
+        raise TypeError(f"{name} must be a floating tensor")
+    return t.to(device=device, dtype=torch.float32).contiguous()
+
+
+def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt: float, nabc: int,
+                            free_surface: bool, src_x: Tensor, src_z: Tensor, src_n: int, src_v: Tensor,
+                            rcv_x: Tensor, rcv_z: Tensor, rcv_n: int, damp: Tensor, vp: Tensor, rho: Tensor,
+                            checkpoint_segments: int = 1, device: torch.device = torch.device("cpu"),
+                            dtype: torch.dtype = torch.float32, snapshot_every: int = 0, *,
+                            fd_order: int = 4, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
+                            want_energy: bool = True):
+    device = torch.device(device)
+    if device.type != "cuda":
+        raise ValueError(f"geobrain_b200 runs on CUDA devices only (device={device})")
+    if dtype != torch.float32:
+        raise TypeError(f"geobrain_b200 computes in float32 (dtype={dtype})")
+    if float(dx) != float(dz):
+        raise ValueError(f"Grid spacing must be equal: dx={dx}, dz={dz}")
+    if fd_order not in engine.FD_ORDERS:
+        raise ValueError(f"fd_order must be one of {sorted(engine.FD_ORDERS)}, got {fd_order}")
+    if checkpoint_segments < 1:
+        raise ValueError(f"checkpoint_segments must be >= 1, got {checkpoint_segments}")
+    src_n, rcv_n = int(src_n), int(rcv_n)
+    geo = engine.Geometry(int(nz), int(nx), int(nabc), int(nt), float(dt), float(dx), engine.FD_ORDERS[fd_order],
+                          bool(free_surface))
+    sx, sz = engine._i64(src_x)[:src_n], engine._i64(src_z)[:src_n]
+    rx, rz = engine._i64(rcv_x)[:rcv_n], engine._i64(rcv_z)[:rcv_n]
+    if sx.size != src_n or rx.size != rcv_n:
+        raise ValueError("src_n / rcv_n exceed the position arrays")
+    plan = engine.get_plan(geo, sx, sz, rx, rz)
+
+    w = _as_f32(src_v, device, "src_v")
+    if w.dim() == 1:
+        w = w.unsqueeze(0).expand(src_n, -1)
+    if w.shape[-1] != nt:
+        raise ValueError(f"src_v has {w.shape[-1]} samples, nt={nt}")
+    w = w.contiguous()
+    damp_t = _as_f32(damp, device, "damp")
+    Nz, Nx = int(nz) + 2 * int(nabc), int(nx) + 2 * int(nabc)
+    if tuple(damp_t.shape) != (Nz, Nx):
+        raise ValueError(f"damp must have shape {(Nz, Nx)}, got {tuple(damp_t.shape)}")
+    for name, t in (("vp", vp), ("rho", rho)):
+        if tuple(t.shape) != (int(nz), int(nx)):
+            raise ValueError(f"{name} must have shape {(int(nz), int(nx))}, got {tuple(t.shape)}")
+
+    needs_grad = torch.is_grad_enabled() and (getattr(vp, "requires_grad", False) or
+                                              getattr(rho, "requires_grad", False))
+    if needs_grad:
+        return engine.differentiable_forward(plan, vp, rho, damp_t, w, device=device,
+                                             snapshot_every=int(snapshot_every),
+                                             checkpoint_segments=int(checkpoint_segments),
+                                             checkpoint_every=int(checkpoint_every),
+                                             snapshot_dtype=snapshot_dtype, want_energy=want_energy)
+    vp_t = _as_f32(vp.detach() if torch.is_tensor(vp) else vp, device, "vp")
+    rho_t = _as_f32(rho.detach() if torch.is_tensor(rho) else rho, device, "rho")
+    p, vx, vz, en, snaps = engine.run_forward(plan, vp_t, rho_t, damp_t, w, want_energy=want_energy,
+                                              snapshot_every=int(snapshot_every))
+    return engine.pack_output(plan, p, vx, vz, en, snaps)

@@ -1,0 +1,140 @@
+/*
+ * geobrain_b200 — C ABI of the B200 (sm_100a) 2D acoustic propagator.
+ *
+ * Plain pointers, sizes and a CUDA stream; no framework types.  Every entry
+ * point returns 0 on success or a negative GB_E* code; gb_last_error() gives
+ * the message of the last failure on the calling thread.
+ *
+ * Reference interfaces these replace (paths inside the GeoBrain source tree):
+ *   geobrain/physics/wave/kernels/acoustic_2d.py:294-317  acoustic_forward_kernel(...)
+ *       -> gb_plan_create + gb_forward (traces, energy maps, snapshots)
+ *   geobrain/physics/wave/kernels/acoustic_2d.py:448-460  torch.utils.checkpoint
+ *       segments + autograd backward through acoustic_step_forward (:123-291)
+ *       -> gb_forward with checkpoints + gb_backward (hand-written adjoint)
+ *   geobrain/physics/wave/kernels/acoustic_2d.py:18-66     pad_model and its
+ *       autograd adjoint -> done inside gb_forward / gb_backward
+ *   geobrain/core/inverse.py:104-110 serial per-particle forward_fn loop
+ *       -> gb_batch_* (many models, one launch per step)
+ *
+ * Grid conventions follow the reference: models are (nz, nx) row-major,
+ * padded by nabc cells on every side to (Nz, Nx) = (nz + 2 nabc, nx + 2 nabc);
+ * source and receiver positions are unpadded integer grid indices; traces are
+ * (n_shots, nt, n_rcv); energy maps are (nz, nx).
+ */
+#ifndef GEOBRAIN_B200_H
+#define GEOBRAIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GB_OK              0
+#define GB_E_ARG          -1   /* invalid argument (sizes, positions, CFL, ...) */
+#define GB_E_CUDA         -2   /* a CUDA runtime call failed */
+#define GB_E_WORKSPACE    -3   /* workspace too small */
+#define GB_E_TIMEOUT      -4   /* a device-side bounded wait gave up */
+#define GB_E_UNSUPPORTED  -5   /* option not built into this library */
+
+/* One velocity model and its acquisition (acoustic_forward_kernel arguments
+ * nx, nz, dx, dz, nt, dt, nabc, free_surface, src_n, rcv_n; half = stencil
+ * half-width: 2 for the reference's 4th-order scheme, 4 for 8th order). */
+typedef struct gb_model_desc {
+    int32_t nz, nx, nabc, nt;
+    int32_t n_shots, n_rcv, half, free_surface;
+    float dt, dx;
+} gb_model_desc;
+
+/* Snapshot (checkpoint) storage formats for the gradient. */
+#define GB_CKPT_F32   0
+#define GB_CKPT_BF16  1   /* bf16 with one fp32 scale per (checkpoint, shot, field) */
+#define GB_CKPT_F16   2   /* fp16 with one fp32 scale per (checkpoint, shot, field) */
+
+typedef struct gb_plan gb_plan;   /* opaque */
+
+/* Build a plan for one model: validates sizes and positions (host arrays of
+ * unpadded indices, like the reference's src_x/src_z/rcv_x/rcv_z), bins the
+ * receivers by tile and sizes the device workspace.  Replaces the set-up half
+ * of acoustic_forward_kernel (acoustic_2d.py:365-420). */
+int gb_plan_create(const gb_model_desc *desc,
+                   const int64_t *src_x, const int64_t *src_z,
+                   const int64_t *rcv_x, const int64_t *rcv_z,
+                   gb_plan **out);
+void gb_plan_destroy(gb_plan *plan);
+
+/* Tile height (rows per CTA, 16 or 32) and shots per CTA; 0 keeps the
+ * default.  Used by the autotuner. */
+int gb_plan_set_tiling(gb_plan *plan, int tile_rows, int shots_per_cta);
+
+/* Bytes of device workspace gb_forward / gb_backward need.  with_gradient:
+ * 0 forward only; 1 adds the adjoint state, the imaging buffer of one
+ * checkpoint segment and the velocity-gradient sums; 2 also the density
+ * gradient's.  The workspace is used from its first 256-byte boundary. */
+size_t gb_plan_workspace_bytes(const gb_plan *plan, int with_gradient, int checkpoint_every);
+
+/* Bytes of checkpoint storage for a given segment length and format. */
+size_t gb_plan_checkpoint_bytes(const gb_plan *plan, int checkpoint_every, int ckpt_format);
+
+/* Forward modelling, all nt steps, on `stream` (acoustic_forward_kernel,
+ * acoustic_2d.py:294-501).  Device pointers:
+ *   vp, rho   (nz, nx) float32       damp (Nz, Nx) float32
+ *   wavelet   (n_shots, nt) float32  (the source adds dt * wavelet[s, it])
+ *   trace_p / trace_vx / trace_vz (n_shots, nt, n_rcv) float32, each may be NULL
+ *   energy_p / energy_vx / energy_vz (nz, nx) float32, NULL skips the energy sums
+ *   snapshots ((nt + snapshot_every - 1) / snapshot_every, nz, nx) float32,
+ *             pressure of shot 0 at the end of each snapshot chunk, or NULL
+ *   checkpoints: NULL, or storage of gb_plan_checkpoint_bytes(checkpoint_every,
+ *             ckpt_format) that receives the states gb_backward restarts from.
+ */
+int gb_forward(gb_plan *plan, const float *vp, const float *rho, const float *damp,
+               const float *wavelet,
+               float *trace_p, float *trace_vx, float *trace_vz,
+               float *energy_p, float *energy_vx, float *energy_vz,
+               int32_t snapshot_every, float *snapshots,
+               void *checkpoints, int32_t checkpoint_every, int32_t ckpt_format,
+               void *workspace, size_t workspace_bytes, void *stream);
+
+/* Gradient of a loss L with respect to vp and rho, given the adjoint sources
+ * res_* = dL/d(trace_*) (n_shots, nt, n_rcv) float32 (any may be NULL), and
+ * the checkpoints a gb_forward call with the same plan, model and
+ * checkpoint_every wrote.  Recomputes each segment forward in fp32 from its
+ * checkpoint, runs the hand-written adjoint backwards through it with the
+ * zero-lag imaging condition fused in, sums over shots and time with
+ * compensated fp32 summation and folds the padding back into the edge cells
+ * (the adjoint of pad_model).  grad_vp / grad_rho are (nz, nx) float32 and
+ * are overwritten; grad_rho may be NULL. */
+int gb_backward(gb_plan *plan, const float *vp, const float *rho, const float *damp,
+                const float *wavelet,
+                const float *res_p, const float *res_vx, const float *res_vz,
+                const void *checkpoints, int32_t checkpoint_every, int32_t ckpt_format,
+                float *grad_vp, float *grad_rho,
+                void *workspace, size_t workspace_bytes, void *stream);
+
+/* Profiling (used by the benchmark): when enabled, gb_forward and
+ * gb_backward record CUDA events on their stream around the forward loop,
+ * each segment's fp32 recompute and each segment's adjoint sweep, and count
+ * their kernel launches.  gb_plan_profile waits for those events, returns
+ * the summed milliseconds per phase and the launch count since the last
+ * call, and resets them.  Any output pointer may be NULL. */
+int gb_plan_set_profiling(gb_plan *plan, int enable);
+int gb_plan_profile(gb_plan *plan, double *ms_forward, double *ms_recompute, double *ms_adjoint,
+                    long long *launches);
+
+/* Synchronises `stream` and reports the device-side status word of a
+ * workspace after gb_forward / gb_backward: GB_OK, or GB_E_TIMEOUT if a
+ * bounded wait inside a kernel gave up. */
+int gb_workspace_status(const void *workspace, void *stream);
+
+/* Message of the last failure on this thread ("" if none). */
+const char *gb_last_error(void);
+
+/* Library version string. */
+const char *gb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GEOBRAIN_B200_H */

@@ -1,0 +1,155 @@
+"""Forward parity of the CUDA path (through the C ABI) against the reference's
+golden outputs and the CPU oracle.  Tolerance: 1e-5 relative L2 in fp32."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_case, oracle_kwargs
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-5
+
+
+def run_cuda(c, device, fd_order=4, **kw):
+    from geobrain_b200.wave import acoustic_forward_kernel
+    S = len(c["src_x"])
+    out = acoustic_forward_kernel(
+        nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+        free_surface=c["free_surface"], src_x=torch.as_tensor(c["src_x"]), src_z=torch.as_tensor(c["src_z"]),
+        src_n=S, src_v=torch.as_tensor(c["src_v"], device=device), rcv_x=torch.as_tensor(c["rcv_x"]),
+        rcv_z=torch.as_tensor(c["rcv_z"]), rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=device),
+        vp=torch.as_tensor(c["vp"], device=device), rho=torch.as_tensor(c["rho"], device=device),
+        device=device, fd_order=fd_order, **kw)
+    torch.cuda.synchronize()
+    return {k: (v.cpu().numpy() if torch.is_tensor(v) else v) for k, v in out.items()}
+
+
+@pytest.mark.parametrize("name", ["small_nofs", "small_fs", "layered_100x200"])
+def test_forward_matches_reference(cuda_device, name):
+    c = load_case(name)
+    out = run_cuda(c, cuda_device)
+    for k in ("p", "vx", "vz", "forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vz"):
+        err = orc.rel_l2(out[k], c[f"ref32_{k}"])
+        assert err < TOL, (k, err)
+        if f"ref64_{k}" in c:
+            assert orc.rel_l2(out[k], c[f"ref64_{k}"]) < TOL, k
+
+
+@pytest.mark.parametrize("name", ["small_nofs", "small_fs"])
+def test_snapshots_match_reference(cuda_device, name):
+    c = load_case(name)
+    out = run_cuda(c, cuda_device, snapshot_every=int(c["snapshot_every"]))
+    assert out["snapshots"].shape == c["ref32_snapshots"].shape
+    assert orc.rel_l2(out["snapshots"], c["ref32_snapshots"]) < TOL
+
+
+@pytest.mark.parametrize("free_surface", [False, True])
+def test_eighth_order_matches_oracle(cuda_device, free_surface):
+    c = load_case("small_fs" if free_surface else "small_nofs")
+    ref = orc.forward(**oracle_kwargs(c), half=4, dtype=np.float64)
+    out = run_cuda(c, cuda_device, fd_order=8)
+    for k in ("p", "vx", "vz", "forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vz"):
+        assert orc.rel_l2(out[k], ref[k]) < TOL, k
+
+
+def synthetic_case(nz, nx, nabc, nt, n_shots, seed, free_surface=False, edge_rcv=True):
+    rng = np.random.default_rng(seed)
+    vp = (1800 + 1200 * rng.random((nz, nx))).astype(np.float32)
+    rho = (1800 + 400 * rng.random((nz, nx))).astype(np.float32)
+    from geobrain_b200.wave import bc_pml, RickerWavelet
+    damp = bc_pml(nx, nz, 10.0, 10.0, nabc, float(vp.max()), free_surface=False).astype(np.float32)
+    w, _ = RickerWavelet()(f0=20.0, dt=1e-3)
+    w = np.pad(w.numpy(), (0, max(0, nt - w.shape[0])))[:nt]
+    sx = rng.integers(-nabc, nx + nabc, n_shots)      # sources anywhere in the padded grid, PML included
+    sz = rng.integers(-nabc, nz + nabc, n_shots)
+    sz[0], sx[0] = -nabc, -nabc                       # a border cell outside every update mask
+    rx = np.concatenate([np.arange(0, nx, 3), rng.integers(-nabc, nx + nabc - 1, 40)])
+    rz = np.concatenate([np.ones_like(np.arange(0, nx, 3)), rng.integers(-nabc, nz + nabc - 1, 40)])
+    if edge_rcv:
+        rx = np.concatenate([rx, [-nabc, nx + nabc - 2, 0]])
+        rz = np.concatenate([rz, [nz + nabc - 2, -nabc, nz - 1]])
+    src_v = (w[None, :] * (1 + rng.random((n_shots, 1)))).astype(np.float32)
+    return dict(nz=nz, nx=nx, nabc=nabc, nt=nt, dt=1e-3, dx=10.0, free_surface=free_surface, vp=vp, rho=rho,
+                damp=damp, src_x=sx.astype(np.int64), src_z=sz.astype(np.int64), src_v=src_v,
+                rcv_x=rx.astype(np.int64), rcv_z=rz.astype(np.int64))
+
+
+@pytest.mark.parametrize("shape", [(37, 53, 4), (70, 245, 8), (33, 121, 5)])
+@pytest.mark.parametrize("fd_order", [4, 8])
+def test_ragged_grids_against_oracle(cuda_device, shape, fd_order):
+    nz, nx, nabc = shape
+    c = synthetic_case(nz, nx, nabc, 90, 3, seed=nz * nx)
+    ref = orc.forward(**oracle_kwargs(c), half=fd_order // 2, dtype=np.float64)
+    out = run_cuda(c, cuda_device, fd_order=fd_order)
+    for k in ("p", "vx", "vz", "forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vz"):
+        assert orc.rel_l2(out[k], ref[k]) < TOL, k
+
+
+@pytest.mark.parametrize("tiling", [(16, 1), (32, 1), (16, 3), (32, 5), (32, 0)])
+def test_tilings_are_bit_identical(cuda_device, tiling):
+    """Tile height and shots-per-CTA change the schedule, never the numbers
+    (except the energy sums' association order)."""
+    from geobrain_b200.wave import engine
+    from geobrain_b200.wave.kernel import acoustic_forward_kernel
+    c = synthetic_case(90, 250, 10, 60, 7, seed=11)
+    base = run_cuda(c, cuda_device, fd_order=8)
+    geo = engine.Geometry(c["nz"], c["nx"], c["nabc"], c["nt"], c["dt"], c["dx"], 4, False)
+    plan = engine.get_plan(geo, c["src_x"], c["src_z"], c["rcv_x"], c["rcv_z"])
+    plan.set_tiling(*tiling)
+    try:
+        out = run_cuda(c, cuda_device, fd_order=8)
+    finally:
+        plan.set_tiling(32, 0)
+    for k in ("p", "vx", "vz"):
+        np.testing.assert_array_equal(out[k], base[k])
+    for k in ("forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vz"):
+        assert orc.rel_l2(out[k], base[k]) < 1e-6
+
+
+def test_wavelet_scaling_is_linear(cuda_device):
+    """Linearity in the source at a large grid (a size-independent check):
+    doubling the wavelet doubles every trace to fp32 rounding.  Bit-exact
+    doubling does not hold for this scheme in fp32 even on the CPU oracle
+    (about one sample in thirty moves by one ulp), so the bar is the
+    rounding level, 1e-6 relative L2."""
+    c = synthetic_case(300, 900, 20, 200, 4, seed=5)
+    a = run_cuda(c, cuda_device, fd_order=8)
+    c2 = dict(c, src_v=c["src_v"] * 2)
+    b = run_cuda(c2, cuda_device, fd_order=8)
+    for k in ("p", "vx", "vz"):
+        assert np.abs(a[k]).max() > 0
+        assert orc.rel_l2(b[k], 2 * a[k]) < 1e-6, k
+
+
+def test_shots_are_independent(cuda_device):
+    """Each shot's traces do not depend on which other shots share the launch."""
+    c = synthetic_case(120, 300, 12, 80, 5, seed=9)
+    allr = run_cuda(c, cuda_device)
+    for s in (0, 3):
+        one = dict(c, src_x=c["src_x"][s:s + 1], src_z=c["src_z"][s:s + 1], src_v=c["src_v"][s:s + 1])
+        o = run_cuda(one, cuda_device)
+        for k in ("p", "vx", "vz"):
+            np.testing.assert_array_equal(o[k][0], allr[k][s])
+
+
+def test_invalid_positions_raise(cuda_device):
+    c = synthetic_case(40, 60, 5, 10, 2, seed=1)
+    bad = dict(c, rcv_x=np.array([c["nx"] + c["nabc"] - 1]), rcv_z=np.array([0]))
+    with pytest.raises(ValueError):
+        run_cuda(bad, cuda_device)
+    bad = dict(c, src_x=np.array([0, -c["nabc"] - 1]))
+    with pytest.raises(ValueError):
+        run_cuda(bad, cuda_device)
+
+
+def test_cpu_device_is_rejected():
+    from geobrain_b200.wave import acoustic_forward_kernel
+    c = load_case("small_nofs")
+    with pytest.raises(ValueError):
+        acoustic_forward_kernel(nx=c["nx"], nz=c["nz"], dx=10.0, dz=10.0, nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+                                free_surface=False, src_x=c["src_x"], src_z=c["src_z"], src_n=3,
+                                src_v=torch.as_tensor(c["src_v"]), rcv_x=c["rcv_x"], rcv_z=c["rcv_z"],
+                                rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"]),
+                                vp=torch.as_tensor(c["vp"]), rho=torch.as_tensor(c["rho"]),
+                                device=torch.device("cpu"))
