@@ -675,3 +675,62 @@ int gb_workspace_status(const void *workspace, void *stream)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Forward modelling for callers that cannot allocate device memory.
+//
+// Some hosts cannot call cudaMalloc or hand the library a workspace: plugins
+// embedded in an application whose memory pool owns all device memory and
+// exposes no allocation hook, or code paths where the caller's allocator must
+// not be re-entered.  For them the scratch gb_forward needs (coefficient
+// planes, the two time levels of the wavefield, the energy sums and the
+// receiver tables) lives in one file-scope device array of fixed size, which
+// every GPU that loads this library keeps for the life of the process.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(64) << 20;   // 64 MiB per device
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_scratch_mutex;
+void *g_static_scratch_addr[kMaxDevices] = {};
+
+}  // namespace
+
+extern "C" size_t gb_static_scratch_bytes(void) { return kStaticScratchBytes; }
+
+extern "C" int gb_forward_static_scratch(gb_plan *P, const float *vp, const float *rho, const float *damp,
+                                         const float *wavelet, float *trace_p, float *trace_vx, float *trace_vz,
+                                         float *energy_p, float *energy_vx, float *energy_vz,
+                                         int32_t snapshot_every, float *snapshots, void *stream)
+{
+    g_last_error.clear();
+    if (!P) return fail(GB_E_ARG, "null plan");
+    const size_t need = gb_plan_workspace_bytes(P, 0, 0);
+    if (need > kStaticScratchBytes)
+        return fail(GB_E_WORKSPACE, "this model needs " + std::to_string(need) +
+                                        " bytes of scratch; the static scratch holds " +
+                                        std::to_string(kStaticScratchBytes) + " bytes (use gb_forward with a workspace)");
+    int dev = -1;
+    GB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(GB_E_ARG, "device ordinal out of range");
+    void *scratch = nullptr;
+    {
+        // first call on this device: look the array's device address up once,
+        // with this device current (the host-side symbol is not a device address)
+        std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
+        if (!g_static_scratch_addr[dev]) {
+            void *addr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&addr, g_static_scratch);
+            if (e != cudaSuccess)
+                return fail(GB_E_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+            g_static_scratch_addr[dev] = addr;
+        }
+        scratch = g_static_scratch_addr[dev];
+    }
+    // gb_forward clears every part of the scratch that must start at zero
+    // (both wavefield time levels, the energy sums, the status word)
+    return gb_forward(P, vp, rho, damp, wavelet, trace_p, trace_vx, trace_vz, energy_p, energy_vx, energy_vz,
+                      snapshot_every, snapshots, nullptr, 0, GB_CKPT_F32, scratch, kStaticScratchBytes, stream);
+}

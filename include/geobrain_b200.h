@@ -127,6 +127,29 @@ int gb_plan_profile(gb_plan *plan, double *ms_forward, double *ms_recompute, dou
  * bounded wait inside a kernel gave up. */
 int gb_workspace_status(const void *workspace, void *stream);
 
+/* Forward modelling without any device allocation: the same computation and
+ * outputs as gb_forward (no checkpoints), with the scratch held in a static
+ * device array inside this library instead of a caller workspace.
+ * No counterpart in the reference.  It is meant for callers that cannot
+ * allocate device memory (a host whose memory pool owns the GPU and offers
+ * no allocation hook).  Limits and behaviour:
+ *   - the array is gb_static_scratch_bytes() (64 MiB) on every GPU that
+ *     loads the library, held until the process exits; a model whose
+ *     gb_plan_workspace_bytes(plan, 0, 0) exceeds it is rejected with
+ *     GB_E_WORKSPACE;
+ *   - the first call on each device looks the array's device address up
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture;
+ *   - every call shares the one array per device: calls whose work overlaps
+ *     on the GPU (other streams, other threads) race and corrupt each other;
+ *   - it calls no cudaMalloc / cudaFree; inputs and outputs are the caller's. */
+size_t gb_static_scratch_bytes(void);
+int gb_forward_static_scratch(gb_plan *plan, const float *vp, const float *rho, const float *damp,
+                              const float *wavelet,
+                              float *trace_p, float *trace_vx, float *trace_vz,
+                              float *energy_p, float *energy_vx, float *energy_vz,
+                              int32_t snapshot_every, float *snapshots, void *stream);
+
 /* Message of the last failure on this thread ("" if none). */
 const char *gb_last_error(void);
 
