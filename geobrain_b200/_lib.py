@@ -38,6 +38,11 @@ class ModelDesc(ctypes.Structure):
     ]
 
 
+class GradStore(ctypes.Structure):
+    _fields_ = [("checkpoints", ctypes.c_void_p), ("checkpoint_every", ctypes.c_int32), ("format", ctypes.c_int32),
+                ("imaging", ctypes.c_void_p), ("cached_steps", ctypes.c_int32), ("with_rho", ctypes.c_int32)]
+
+
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _SZ = ctypes.c_size_t
@@ -49,9 +54,10 @@ SIGNATURES = {
     "gb_plan_set_tiling": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_workspace_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_checkpoint_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
-    "gb_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P, _I32, _I32,
-                                  _P, _SZ, _P]),
-    "gb_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _SZ, _P]),
+    "gb_plan_imaging_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
+    "gb_plan_set_group_streams": (ctypes.c_int, [_P, ctypes.c_int]),
+    "gb_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P, _P, _SZ, _P]),
+    "gb_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
     "gb_workspace_status": (ctypes.c_int, [_P, _P]),
     "gb_plan_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_plan_profile": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),

@@ -23,7 +23,6 @@
 // dL/dvp and dL/drho follow from G1, G2 in grad_finish_kernel.
 #pragma once
 
-#include "gb_device.cuh"
 #include "gb_fwd.cuh"
 
 namespace gb {
@@ -32,6 +31,7 @@ struct AdjArgs {
     StepGeom g;
     int it;                                  // forward step whose adjoint this is
     const float *a1, *k1, *a2, *k2, *k3;
+    const int *tile_fast;
     float *out;                              // previous adjoint state [S][3][plane]
     const int *rcv_ptr;                      // CSR over tiles, receivers within the loaded rectangles
     const int4 *rcv_ent;                     // (padded z, padded x, receiver, 0)
@@ -39,6 +39,7 @@ struct AdjArgs {
     const float *img;                        // [S][plane] I_n (and Jx, Jz planes after it when RHO)
     long long img_field_stride;              // distance between the I, Jx, Jz blocks
     float *G1, *C1, *G2, *C2;                // [n_groups][plane] sums and compensations
+    int grp0, grp_count;             // shot groups this launch covers
     int *err;
 };
 
@@ -53,38 +54,61 @@ __device__ __forceinline__ void neumaier_add(float &s, float &c, float x)
 }
 
 template <int R, int TZ, bool FS, bool RHO>
-__global__ void __launch_bounds__(NTHR, 1)
+__global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
 adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mVX,
-                const __grid_constant__ CUtensorMap mVZ, const AdjArgs A)
+                const __grid_constant__ CUtensorMap mVZ, const __grid_constant__ CUtensorMap mA1,
+                const __grid_constant__ CUtensorMap mA2, const AdjArgs A)
 {
     using G = Geo<R, TZ>;
+    using SM = StepSmem<R, TZ>;
     const StepGeom &g = A.g;
     extern __shared__ __align__(128) float smem[];
-    float *stage[2] = {smem, smem + G::STAGE_FL};
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * G::STAGE_FL);
+    float *sA1 = smem + 2 * G::STAGE_FL;
+    float *sA2 = sA1 + SM::A1_FL;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sA1 + SM::COEF_FL);
 
-    const int group = blockIdx.x % g.n_groups;
-    const int tile = blockIdx.x / g.n_groups;
+    // launch covers shot groups [grp0, grp0 + grp_count): one launch for all
+    // groups, or one launch per group when groups run on their own streams
+    const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
+    const int tile = (int)(blockIdx.x / A.grp_count);
     const int z0 = (tile / g.tiles_x) * TZ;
     const int x0 = (tile % g.tiles_x) * TX;
     const int s0 = group * g.shots_per_cta;
     const int ns = min(g.n_shots - s0, g.shots_per_cta);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool fast = A.tile_fast[tile] != 0;
+    const int rcv0 = A.rcv_ptr[tile], rcv1 = A.rcv_ptr[tile + 1];
+    const bool has_rcv = rcv1 > rcv0 && (A.res_p || A.res_vx || A.res_vz);
 
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
         fence_mbar_init();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&bars[2], SM::COEF_BYTES);
+        tma_load_2d(sA1, &mA1, &bars[2], x0 - 4, z0 - R);
+        tma_load_2d(sA2, &mA2, &bars[2], x0 - 4, z0);
         for (int k = 0; k < 2 && k < ns; ++k)
-            stage_loads<R>(&mP, &mVX, &mVZ, stage[k], &bars[k], G::STAGE_BYTES, x0, z0, s0 + k, G::P_FL,
-                           G::VX_FL);
+            stage_loads<R>(&mP, &mVX, &mVZ, smem + k * G::STAGE_FL, &bars[k], G::STAGE_BYTES, x0, z0, s0 + k,
+                           G::P_FL, G::VX_FL);
     }
-    const int gx0 = x0 - 4 + 4 * lane;
+    if (!__syncthreads_and(mbar_wait_bounded(&bars[2], 0))) {
+        if (threadIdx.x == 0) {
+            atomicExch(A.err, -4);
+            for (int k = 0; k < 2 && k < ns; ++k) mbar_wait_bounded(&bars[k], 0);
+        }
+        return;
+    }
 
-    // per-thread partial sums over this CTA's shots (v-stage cells)
+    const int gx0 = x0 - 4 + 4 * lane;
+    const int rb = warp * G::LP, rc = min(G::LP, G::PR - rb);
+    const int vb = warp * G::LV, vcnt = min(G::LV, TZ - vb);
+    const bool vlane = lane >= 1 && lane <= 30;
+
+    // per-thread partial sums over this CTA's shots (tile cells)
     float4 acc1[G::LV], acc2[G::LV];
 #pragma unroll
     for (int u = 0; u < G::LV; ++u) {
@@ -95,6 +119,19 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
     for (int k = 0; k < ns; ++k) {
         const int s = s0 + k;
         const int b = k & 1;
+        // imaging fields of this shot's tile cells: issued now, used in stage B
+        float4 im[G::LV], jx[G::LV], jz[G::LV];
+#pragma unroll
+        for (int u = 0; u < G::LV; ++u) {
+            const int gz = z0 + vb + u;
+            const bool ok = vlane && u < vcnt && gz < g.Nz && gx0 < g.Nx;
+            const float *imp = A.img + (long long)s * g.plane + (long long)gz * g.pitch + gx0;
+            im[u] = ok ? ldg4(imp) : zero4();
+            if (RHO) {
+                jx[u] = ok ? ldg4(imp + A.img_field_stride) : zero4();
+                jz[u] = ok ? ldg4(imp + 2 * A.img_field_stride) : zero4();
+            }
+        }
         if (!__syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1))) {
             if (threadIdx.x == 0) {
                 atomicExch(A.err, -4);
@@ -102,14 +139,16 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
             }
             return;
         }
-        float *sP = stage[b];
+        if (threadIdx.x == 0 && k >= 1 && k + 1 < ns)   // refill shot k-1's buffer with shot k+1
+            stage_loads<R>(&mP, &mVX, &mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
+                           s + 1, G::P_FL, G::VX_FL);
+        float *sP = smem + b * G::STAGE_FL;
         float *sVX = sP + G::P_FL;
         float *sVZ = sVX + G::VX_FL;
 
         // ---------------- adjoint sources at the receivers ------------------
-        if (A.res_p || A.res_vx || A.res_vz) {
-            const int e0 = A.rcv_ptr[tile], e1 = A.rcv_ptr[tile + 1];
-            for (int e = e0 + threadIdx.x; e < e1; e += NTHR) {
+        if (has_rcv) {
+            for (int e = rcv0 + threadIdx.x; e < rcv1; e += NTHR) {
                 const int4 en = A.rcv_ent[e];
                 const int gz = en.x, gx = en.y;
                 const long long t = ((long long)s * g.nt + A.it) * g.n_rcv + en.z;
@@ -134,8 +173,6 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
 
         // ---------------- stage A: mu_p on the whole sP rectangle ----------
         {
-            const int rb = warp * G::LP;
-            const int rc = min(G::LP, G::PR - rb);
             float4 wz[G::LP + 2 * R - 1];
 #pragma unroll
             for (int t = 0; t < G::LP + 2 * R - 1; ++t)
@@ -146,37 +183,32 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                     const int r = rb + u;
                     const int gz = z0 - R + r;
                     float4 pv = lds4(sP + r * RW + 4 * lane);
-                    const bool row_in = gz >= g.p_r0 && gz <= g.p_r1;
-                    if (row_in && (gx0 + 3 >= g.p_c0) && (gx0 <= g.p_c1)) {
-                        float e[12];
-                        {
-                            const float4 e0 = lds4(sVX + r * VXW + 4 * lane);
-                            const float4 e1 = lds4(sVX + r * VXW + 4 * lane + 4);
-                            const float4 e2 = lds4(sVX + r * VXW + 4 * lane + 8);
-                            e[0] = e0.x; e[1] = e0.y; e[2] = e0.z; e[3] = e0.w;
-                            e[4] = e1.x; e[5] = e1.y; e[6] = e1.z; e[7] = e1.w;
-                            e[8] = e2.x; e[9] = e2.y; e[10] = e2.z; e[11] = e2.w;
-                        }
-                        const float4 a1 = ldg4(A.a1 + (long long)gz * g.pitch + gx0);
+                    const float4 a1 = lds4(sA1 + r * RW + 4 * lane);
+                    float D[4];
+                    if (fast) {
+                        divergence4<R>(sVX + r * VXW, lane, wz, u, g.c, D);
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            float D = 0.f;
-#pragma unroll
-                            for (int kk = 0; kk < R; ++kk)
-                                D += g.c[kk] * (((e[q + 4 + kk] - e[q + 3 - kk]) + at(wz[u + R + kk], q)) -
-                                                at(wz[u + R - 1 - kk], q));
-                            if (FS && gz == g.fs + 1) {
-                                // share of the mirror row p[fs-1] = -p[fs+1]
-                                float M = 0.f;
-#pragma unroll
-                                for (int kk = 0; kk < R; ++kk) M += g.c[kk] * at(wz[u + R - 2 + kk], q);
-                                D -= M;
-                            }
-                            const int gx = gx0 + q;
-                            at(pv, q) = (gx >= g.p_c0 && gx <= g.p_c1) ? at(pv, q) + at(a1, q) * D : 0.f;
-                        }
+                        for (int q = 0; q < 4; ++q) at(pv, q) = __fmaf_rn(at(a1, q), D[q], at(pv, q));
                     } else {
-                        pv = zero4();
+                        const bool row_in = gz >= g.p_r0 && gz <= g.p_r1;
+                        if (row_in && (gx0 + 3 >= g.p_c0) && (gx0 <= g.p_c1)) {
+                            divergence4<R>(sVX + r * VXW, lane, wz, u, g.c, D);
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                float d = D[q];
+                                if (FS && gz == g.fs + 1) {
+                                    // share of the mirror row p[fs-1] = -p[fs+1]
+                                    float M = 0.f;
+#pragma unroll
+                                    for (int kk = 0; kk < R; ++kk) M += g.c[kk] * at(wz[u + R - 2 + kk], q);
+                                    d -= M;
+                                }
+                                const int gx = gx0 + q;
+                                at(pv, q) = (gx >= g.p_c0 && gx <= g.p_c1) ? __fmaf_rn(at(a1, q), d, at(pv, q)) : 0.f;
+                            }
+                        } else {
+                            pv = zero4();
+                        }
                     }
                     sts4(sP + r * RW + 4 * lane, pv);
                 }
@@ -185,84 +217,81 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
         __syncthreads();
 
         // ---------------- stage B: tile --------------------------------------
-        if (lane >= 1 && lane <= 30) {
-            const int vb = warp * G::LV;
-            const int vc = min(G::LV, TZ - vb);
+        if (vlane) {
             float4 wp[G::LV + 2 * R - 1];
 #pragma unroll
             for (int t = 0; t < G::LV + 2 * R - 1; ++t)
-                wp[t] = (t < vc + 2 * R - 1) ? lds4(sP + (vb + 1 + t) * RW + 4 * lane) : zero4();
+                wp[t] = (t < vcnt + 2 * R - 1) ? lds4(sP + (vb + 1 + t) * RW + 4 * lane) : zero4();
 #pragma unroll
             for (int u = 0; u < G::LV; ++u) {
-                if (u < vc) {
+                if (u < vcnt) {
                     const int rv = vb + u;
                     const int rr = rv + R;
                     const int gz = z0 + rv;
-                    if (gz < g.Nz && gx0 < g.Nx) {
-                        float f[12];
-                        {
-                            const float4 f0 = lds4(sP + rr * RW + 4 * lane - 4);
-                            const float4 f1 = lds4(sP + rr * RW + 4 * lane);
-                            const float4 f2 = lds4(sP + rr * RW + 4 * lane + 4);
-                            f[0] = f0.x; f[1] = f0.y; f[2] = f0.z; f[3] = f0.w;
-                            f[4] = f1.x; f[5] = f1.y; f[6] = f1.z; f[7] = f1.w;
-                            f[8] = f2.x; f[9] = f2.y; f[10] = f2.z; f[11] = f2.w;
-                        }
+                    if (fast || (gz < g.Nz && gx0 < g.Nx)) {
+                        float Dx[4], Dz[4];
+                        float4 mp1;
+                        grad_x4<R>(sP + rr * RW, lane, g.c, Dx, mp1);
+                        grad_z4<R>(wp, u, g.c, Dz);
                         const float4 vx1 = lds4(sVX + rr * VXW + 4 * lane + 4);
                         const float4 vz1 = lds4(sVZ + (rv + 2 * R) * RW + 4 * lane);
-                        const float4 mp1 = make_float4(f[4], f[5], f[6], f[7]);
-                        float4 vx = zero4(), vz = zero4(), pp = zero4();
+                        const float4 a2 = lds4(sA2 + rv * RW + 4 * lane);
                         const long long o = (long long)gz * g.pitch + gx0;
-                        const bool vx_row = gz >= g.vx_r0 && gz <= g.vx_r1;
-                        const bool vz_row = gz >= g.vz_r0 && gz <= g.vz_r1;
-                        const bool p_row = gz >= g.p_r0 && gz <= g.p_r1;
-                        const bool any_v = (vx_row && gx0 + 3 >= g.vx_c0 && gx0 <= g.vx_c1) ||
-                                           (vz_row && gx0 + 3 >= g.vz_c0 && gx0 <= g.vz_c1);
-                        const bool any_p = p_row && gx0 + 3 >= g.p_c0 && gx0 <= g.p_c1;
-                        if (any_v) {
-                            const float4 a2 = ldg4(A.a2 + o);
-                            const float4 k2 = ldg4(A.k2 + o);
-                            const float4 k3 = ldg4(A.k3 + o);
-                            float4 jx, jz;
+                        float4 vx, vz, pp;
+                        if (fast) {
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                at(vx, q) = __fmaf_rn(at(a2, q), Dx[q], at(vx1, q));
+                                at(vz, q) = __fmaf_rn(at(a2, q), Dz[q], at(vz1, q));
+                                at(acc1[u], q) += at(mp1, q) * at(im[u], q);
+                            }
+                            pp = mp1;
                             if (RHO) {
-                                jx = ldg4(A.img + (long long)s * g.plane + A.img_field_stride + o);
-                                jz = ldg4(A.img + (long long)s * g.plane + 2 * A.img_field_stride + o);
-                            }
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                const int gx = gx0 + q;
-                                if (vx_row && gx >= g.vx_c0 && gx <= g.vx_c1) {
-                                    float D = 0.f;
-#pragma unroll
-                                    for (int kk = 0; kk < R; ++kk)
-                                        D += g.c[kk] * (f[q + 5 + kk] - f[q + 4 - kk]);
-                                    at(vx, q) = (1.f - at(k2, q)) * at(vx1, q) + at(a2, q) * D;
-                                    if (RHO) at(acc2[u], q) += at(vx1, q) * at(jx, q);
+                                for (int q = 0; q < 4; ++q) {
+                                    at(acc2[u], q) += at(vx1, q) * at(jx[u], q);
+                                    at(acc2[u], q) += at(vz1, q) * at(jz[u], q);
                                 }
-                                if (vz_row && gx >= g.vz_c0 && gx <= g.vz_c1) {
-                                    float D = 0.f;
+                            }
+                        } else {
+                            vx = zero4(); vz = zero4(); pp = zero4();
+                            const bool vx_row = gz >= g.vx_r0 && gz <= g.vx_r1;
+                            const bool vz_row = gz >= g.vz_r0 && gz <= g.vz_r1;
+                            const bool p_row = gz >= g.p_r0 && gz <= g.p_r1;
+                            const bool any_v = (vx_row && gx0 + 3 >= g.vx_c0 && gx0 <= g.vx_c1) ||
+                                               (vz_row && gx0 + 3 >= g.vz_c0 && gx0 <= g.vz_c1);
+                            const bool any_p = p_row && gx0 + 3 >= g.p_c0 && gx0 <= g.p_c1;
+                            if (any_v) {
+                                const float4 k2 = ldg4(A.k2 + o);
+                                const float4 k3 = ldg4(A.k3 + o);
 #pragma unroll
-                                    for (int kk = 0; kk < R; ++kk)
-                                        D += g.c[kk] * (at(wp[u + R + kk], q) - at(wp[u + R - 1 - kk], q));
-                                    if (FS && gz == g.fs) {
-                                        // the p update reads vz[fs-1] as vz[fs]
-#pragma unroll
-                                        for (int kk = 0; kk < R; ++kk) D += g.c[kk] * at(wp[u + R - 1 + kk], q);
+                                for (int q = 0; q < 4; ++q) {
+                                    const int gx = gx0 + q;
+                                    if (vx_row && gx >= g.vx_c0 && gx <= g.vx_c1) {
+                                        at(vx, q) = __fmaf_rn(at(a2, q), Dx[q], (1.f - at(k2, q)) * at(vx1, q));
+                                        if (RHO) at(acc2[u], q) += at(vx1, q) * at(jx[u], q);
                                     }
-                                    at(vz, q) = (1.f - at(k3, q)) * at(vz1, q) + at(a2, q) * D;
-                                    if (RHO) at(acc2[u], q) += at(vz1, q) * at(jz, q);
+                                    if (vz_row && gx >= g.vz_c0 && gx <= g.vz_c1) {
+                                        float d = Dz[q];
+                                        if (FS && gz == g.fs) {
+                                            // the p update reads vz[fs-1] as vz[fs]
+#pragma unroll
+                                            for (int kk = 0; kk < R; ++kk) d += g.c[kk] * at(wp[u + R - 1 + kk], q);
+                                        }
+                                        at(vz, q) = __fmaf_rn(at(a2, q), d, (1.f - at(k3, q)) * at(vz1, q));
+                                        if (RHO) at(acc2[u], q) += at(vz1, q) * at(jz[u], q);
+                                    }
                                 }
                             }
-                        }
-                        if (any_p) {
-                            const float4 k1 = ldg4(A.k1 + o);
-                            const float4 im = ldg4(A.img + (long long)s * g.plane + o);
+                            if (any_p) {
+                                const float4 k1 = ldg4(A.k1 + o);
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                const int gx = gx0 + q;
-                                if (gx >= g.p_c0 && gx <= g.p_c1) {
-                                    at(pp, q) = (1.f - at(k1, q)) * at(mp1, q);
-                                    at(acc1[u], q) += at(mp1, q) * at(im, q);
+                                for (int q = 0; q < 4; ++q) {
+                                    const int gx = gx0 + q;
+                                    if (gx >= g.p_c0 && gx <= g.p_c1) {
+                                        at(pp, q) = (1.f - at(k1, q)) * at(mp1, q);
+                                        at(acc1[u], q) += at(mp1, q) * at(im[u], q);
+                                    }
                                 }
                             }
                         }
@@ -275,22 +304,15 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
             }
         }
         fence_proxy_async_smem();
-        __syncthreads();
-        if (threadIdx.x == 0 && k + 2 < ns) {
-            stage_loads<R>(&mP, &mVX, &mVZ, stage[b], &bars[b], G::STAGE_BYTES, x0, z0, s + 2, G::P_FL,
-                           G::VX_FL);
-        }
     }
 
     // compensated accumulation of this step's partial sums into the group's
     // running totals (this CTA is their only writer for this tile)
-    if (lane >= 1 && lane <= 30) {
-        const int vb = warp * G::LV;
-        const int vc = min(G::LV, TZ - vb);
+    if (vlane) {
 #pragma unroll
         for (int u = 0; u < G::LV; ++u) {
             const int gz = z0 + vb + u;
-            if (u < vc && gz >= g.p_r0 && gz <= g.p_r1 && gx0 < g.Nx) {
+            if (u < vcnt && gz >= g.p_r0 && gz <= g.p_r1 && gx0 < g.Nx) {
                 const long long o = (long long)group * g.plane + (long long)gz * g.pitch + gx0;
                 float4 s1 = *reinterpret_cast<float4 *>(A.G1 + o), c1 = *reinterpret_cast<float4 *>(A.C1 + o);
 #pragma unroll
@@ -298,7 +320,7 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                 stg4(A.G1 + o, s1);
                 stg4(A.C1 + o, c1);
             }
-            if (RHO && u < vc && gz < g.Nz && gx0 < g.Nx) {
+            if (RHO && u < vcnt && gz < g.Nz && gx0 < g.Nx) {
                 const long long o = (long long)group * g.plane + (long long)gz * g.pitch + gx0;
                 float4 s2 = *reinterpret_cast<float4 *>(A.G2 + o), c2 = *reinterpret_cast<float4 *>(A.C2 + o);
 #pragma unroll
@@ -313,7 +335,7 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
 template <int R, int TZ>
 constexpr size_t adj_smem_bytes()
 {
-    return 2 * Geo<R, TZ>::STAGE_BYTES + 16;
+    return StepSmem<R, TZ>::BYTES;
 }
 
 // dL/dvp and dL/drho on the (nz, nx) model: per padded cell

@@ -54,3 +54,68 @@ __global__ void extract_interior_kernel(const float *__restrict__ src, int nz, i
 }
 
 }  // namespace gb
+
+namespace gb {
+
+// ---------------------------------------------------------------------------
+// Checkpoint snapshots in 16 bits with one fp32 scale per (checkpoint, shot,
+// field) plane.  Pass 1 takes |x|max of each plane; pass 2 stores x / scale
+// (scale = absmax / 2^15, so every plane spans about +-32768, well inside the
+// range of either format); unpacking multiplies back.  bf16 keeps 8
+// significant bits, fp16 11; the recompute that restarts from a snapshot runs
+// in fp32.
+// ---------------------------------------------------------------------------
+__global__ void plane_absmax_kernel(const float *__restrict__ x, long long plane, unsigned int *amax_bits)
+{
+    const int pl = blockIdx.y;
+    const float *p = x + pl * plane;
+    float m = 0.f;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane;
+         i += (long long)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(p[i]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&amax_bits[pl], __float_as_uint(m));   // |x| >= 0 orders as unsigned
+}
+
+template <class H>
+__device__ __forceinline__ H to_h(float v);
+template <>
+__device__ __forceinline__ __nv_bfloat16 to_h<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+template <>
+__device__ __forceinline__ __half to_h<__half>(float v) { return __float2half_rn(v); }
+__device__ __forceinline__ float from_h(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float from_h(__half v) { return __half2float(v); }
+
+constexpr float kSnapshotRange = 32768.f;
+
+template <class H>
+__global__ void pack16_kernel(const float *__restrict__ x, long long plane, const unsigned int *__restrict__ amax_bits,
+                              H *__restrict__ out, float *__restrict__ scales)
+{
+    const int pl = blockIdx.y;
+    const float amax = __uint_as_float(amax_bits[pl]);
+    // the floor keeps all-zero and subnormal-only planes finite
+    const float scale = fmaxf(amax / kSnapshotRange, 1.17549435e-38f);
+    const float inv = 1.f / scale;
+    if (blockIdx.x == 0 && threadIdx.x == 0) scales[pl] = scale;
+    const float *p = x + pl * plane;
+    H *o = out + pl * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane;
+         i += (long long)gridDim.x * blockDim.x)
+        o[i] = to_h<H>(p[i] * inv);
+}
+
+template <class H>
+__global__ void unpack16_kernel(const H *__restrict__ in, const float *__restrict__ scales, long long plane,
+                                float *__restrict__ x)
+{
+    const int pl = blockIdx.y;
+    const float scale = scales[pl];
+    const H *p = in + pl * plane;
+    float *o = x + pl * plane;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < plane;
+         i += (long long)gridDim.x * blockDim.x)
+        o[i] = from_h(p[i]) * scale;
+}
+
+}  // namespace gb

@@ -76,6 +76,23 @@ int make_map(CUtensorMap *map, const float *base, int Nx, int Nz, int pitch, int
     return GB_OK;
 }
 
+// 2-D map over one coefficient plane [Nz][pitch] fp32 (valid extent Nx).
+int make_map2d(CUtensorMap *map, const float *base, int Nx, int Nz, int pitch, int box_x, int box_z)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc;
+    if (int rc = get_encoder(&enc)) return rc;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || (pitch % 4)) return fail(GB_E_ARG, "coefficient plane not aligned");
+    cuuint64_t dims[2] = {(cuuint64_t)Nx, (cuuint64_t)Nz};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
+    cuuint32_t box[2] = {(cuuint32_t)box_x, (cuuint32_t)box_z};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(GB_E_CUDA, "cuTensorMapEncodeTiled (2-D) failed (" + std::to_string((int)r) + ")");
+    return GB_OK;
+}
+
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
 }  // namespace
@@ -88,20 +105,40 @@ struct gb_plan {
     int R = 2, fs = 1;
     int Nz = 0, Nx = 0, pitch = 0;
     long long plane = 0;
-    int tz = 32, spc = 0;   // tile rows, shots per CTA
+    int tz = 16, spc = 0;   // tile rows, shots per CTA (0 = automatic)
     int tiles_x = 0, tiles_z = 0, n_tiles = 0, n_groups = 0;
+    bool group_streams = true;                     // run shot groups on their own streams
     float c[4] = {0, 0, 0, 0};
     std::vector<int> src_z, src_x, rcv_z, rcv_x;   // padded
     std::vector<int> rcv_ptr;                      // CSR over tiles (own receivers)
     std::vector<int4> rcv_ent;
     std::vector<int> arcv_ptr;                     // CSR over tiles: receivers inside the
     std::vector<int4> arcv_ent;                    // loaded halo rectangles (adjoint)
-    // optional phase profiling: event pairs recorded on the launching stream
+    // one stream per shot group (created on first use, per device)
+    int stream_dev = -1;
+    std::vector<cudaStream_t> gstream;
+    std::vector<cudaEvent_t> gjoin;
+    cudaEvent_t gfork = nullptr;
+    // optional phase profiling: event pairs recorded on the caller's stream
     bool prof = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[3];   // forward, recompute, adjoint
     long long launches = 0;
 
-    ~gb_plan() { clear_events(); }
+    ~gb_plan()
+    {
+        clear_events();
+        release_streams();
+    }
+    void release_streams()
+    {
+        for (auto s : gstream) cudaStreamDestroy(s);
+        for (auto e : gjoin) cudaEventDestroy(e);
+        if (gfork) cudaEventDestroy(gfork);
+        gstream.clear();
+        gjoin.clear();
+        gfork = nullptr;
+        stream_dev = -1;
+    }
     void clear_events()
     {
         for (auto &v : ev) {
@@ -112,7 +149,7 @@ struct gb_plan {
             v.clear();
         }
     }
-    // record the start (end) of a phase; returns the index of the pair
+    // record the start (end) of a phase on the caller's stream
     void mark(int phase, bool start, cudaStream_t st)
     {
         if (!prof) return;
@@ -132,8 +169,9 @@ struct gb_plan {
         tiles_x = (Nx + TX - 1) / TX;
         tiles_z = (Nz + tz - 1) / tz;
         n_tiles = tiles_x * tiles_z;
-        if (spc <= 0) spc = default_spc();
-        n_groups = (d.n_shots + spc - 1) / spc;
+        const int use_spc = spc > 0 ? spc : default_spc();
+        n_groups = (d.n_shots + use_spc - 1) / use_spc;
+        spc_eff = use_spc;
         rcv_ptr.assign(n_tiles + 1, 0);
         for (int r = 0; r < d.n_rcv; ++r) rcv_ptr[(rcv_z[r] / tz) * tiles_x + rcv_x[r] / TX + 1]++;
         for (int t = 0; t < n_tiles; ++t) rcv_ptr[t + 1] += rcv_ptr[t];
@@ -165,10 +203,11 @@ struct gb_plan {
             arcv_ent.insert(arcv_ent.end(), per[t].begin(), per[t].end());
         }
     }
+    int spc_eff = 1;
 
     // Enough CTAs to fill the GPU several times over, as few groups as that
     // allows (each group re-reads the coefficient tiles and adds its own
-    // energy partial sums).
+    // energy / gradient partial sums); at most 8 shots per CTA.
     int default_spc() const
     {
         const int S = d.n_shots;
@@ -190,20 +229,23 @@ struct gb_plan {
         g.vx_r0 = fs; g.vx_r1 = Nz - 2; g.vx_c0 = R - 1; g.vx_c1 = Nx - 1 - R;
         g.vz_r0 = std::max(fs, R - 1); g.vz_r1 = Nz - 1 - R; g.vz_c0 = 1; g.vz_c1 = Nx - 2;
         g.tiles_x = tiles_x; g.n_tiles = n_tiles;
-        g.n_shots = d.n_shots; g.shots_per_cta = spc; g.n_groups = n_groups;
+        g.n_shots = d.n_shots; g.shots_per_cta = spc_eff; g.n_groups = n_groups;
         g.nt = d.nt; g.n_rcv = d.n_rcv;
         g.dt = d.dt;
         for (int k = 0; k < 4; ++k) g.c[k] = c[k];
         g.plane = plane;
         return g;
     }
+
+    int group_first(int grp) const { return grp * spc_eff; }
+    int group_shots(int grp) const { return std::min(d.n_shots - grp * spc_eff, spc_eff); }
 };
 
 namespace {
 
 // Workspace layout (offsets in bytes from the 256-aligned base).
 struct Layout {
-    size_t err, coef, fields, energy, src, rcv_ptr, rcv_ent, total;
+    size_t err, coef, fields, energy, src, rcv_ptr, rcv_ent, tile_fast, amax, total;
     // gradient only
     size_t mu, img, g1, c1, g2, c2, arcv_ptr, arcv_ent;
     int n_img;
@@ -222,6 +264,8 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0)
     L.src = o; o = align256(o + 2 * S * 4);
     L.rcv_ptr = o; o = align256(o + (p->n_tiles + 1) * 4);
     L.rcv_ent = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 16);
+    L.tile_fast = o; o = align256(o + (size_t)p->n_tiles * 4);
+    L.amax = o; o = align256(o + S * 3 * 4);
     L.n_img = with_gradient >= 2 ? 3 : 1;
     if (with_gradient > 0) {
         const size_t K = std::max(1, std::min(checkpoint_every, p->d.nt));
@@ -247,33 +291,32 @@ void *fwd_fn()
     return reinterpret_cast<void *>(&fwd_step_kernel<R, TZ, FS, EN, IMG>);
 }
 
-// Energy sums are only taken by the plain forward; the imaging fields only by
-// the gradient's recompute (which takes no energy).
+template <int R, int TZ, bool FS>
+void *fwd_pick_fs(bool en, int img)
+{
+    if (img == 1) return en ? fwd_fn<R, TZ, FS, true, 1>() : fwd_fn<R, TZ, FS, false, 1>();
+    if (img == 2) return en ? fwd_fn<R, TZ, FS, true, 2>() : fwd_fn<R, TZ, FS, false, 2>();
+    return en ? fwd_fn<R, TZ, FS, true, 0>() : fwd_fn<R, TZ, FS, false, 0>();
+}
+
 template <int R, int TZ>
 void *fwd_pick3(bool fs, bool en, int img)
 {
-    if (fs) {
-        if (img == 1) return fwd_fn<R, TZ, true, false, 1>();
-        if (img == 2) return fwd_fn<R, TZ, true, false, 2>();
-        return en ? fwd_fn<R, TZ, true, true, 0>() : fwd_fn<R, TZ, true, false, 0>();
-    }
-    if (img == 1) return fwd_fn<R, TZ, false, false, 1>();
-    if (img == 2) return fwd_fn<R, TZ, false, false, 2>();
-    return en ? fwd_fn<R, TZ, false, true, 0>() : fwd_fn<R, TZ, false, false, 0>();
+    return fs ? fwd_pick_fs<R, TZ, true>(en, img) : fwd_pick_fs<R, TZ, false>(en, img);
 }
 
-struct FwdKernel {
+struct StepKernel {
     void *fn;
     size_t smem;
 };
 
-FwdKernel fwd_kernel(int R, int tz, bool fs, bool en, int im)
+StepKernel fwd_kernel(int R, int tz, bool fs, bool en, int im)
 {
-    FwdKernel k{nullptr, 0};
-    if (R == 2 && tz == 32) { k.fn = fwd_pick3<2, 32>(fs, en, im); k.smem = en ? fwd_smem_bytes<2, 32, true>() : fwd_smem_bytes<2, 32, false>(); }
-    if (R == 2 && tz == 16) { k.fn = fwd_pick3<2, 16>(fs, en, im); k.smem = en ? fwd_smem_bytes<2, 16, true>() : fwd_smem_bytes<2, 16, false>(); }
-    if (R == 4 && tz == 32) { k.fn = fwd_pick3<4, 32>(fs, en, im); k.smem = en ? fwd_smem_bytes<4, 32, true>() : fwd_smem_bytes<4, 32, false>(); }
-    if (R == 4 && tz == 16) { k.fn = fwd_pick3<4, 16>(fs, en, im); k.smem = en ? fwd_smem_bytes<4, 16, true>() : fwd_smem_bytes<4, 16, false>(); }
+    StepKernel k{nullptr, 0};
+    if (R == 2 && tz == 32) { k.fn = fwd_pick3<2, 32>(fs, en, im); k.smem = fwd_smem_bytes<2, 32>(); }
+    if (R == 2 && tz == 16) { k.fn = fwd_pick3<2, 16>(fs, en, im); k.smem = fwd_smem_bytes<2, 16>(); }
+    if (R == 4 && tz == 32) { k.fn = fwd_pick3<4, 32>(fs, en, im); k.smem = fwd_smem_bytes<4, 32>(); }
+    if (R == 4 && tz == 16) { k.fn = fwd_pick3<4, 16>(fs, en, im); k.smem = fwd_smem_bytes<4, 16>(); }
     return k;
 }
 
@@ -286,9 +329,9 @@ void *adj_pick(bool fs, bool rho)
                : reinterpret_cast<void *>(&adj_step_kernel<R, TZ, false, false>);
 }
 
-FwdKernel adj_kernel(int R, int tz, bool fs, bool rho)
+StepKernel adj_kernel(int R, int tz, bool fs, bool rho)
 {
-    FwdKernel k{nullptr, 0};
+    StepKernel k{nullptr, 0};
     if (R == 2 && tz == 32) { k.fn = adj_pick<2, 32>(fs, rho); k.smem = adj_smem_bytes<2, 32>(); }
     if (R == 2 && tz == 16) { k.fn = adj_pick<2, 16>(fs, rho); k.smem = adj_smem_bytes<2, 16>(); }
     if (R == 4 && tz == 32) { k.fn = adj_pick<4, 32>(fs, rho); k.smem = adj_smem_bytes<4, 32>(); }
@@ -296,28 +339,228 @@ FwdKernel adj_kernel(int R, int tz, bool fs, bool rho)
     return k;
 }
 
+int prepare_kernel(const StepKernel &k)
+{
+    if (!k.fn) return fail(GB_E_UNSUPPORTED, "no kernel for this configuration");
+    GB_CUDA(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)k.smem));
+    return GB_OK;
+}
+
 int box_rows_p(int R, int tz) { return tz + 2 * R; }
 int box_rows_vz(int R, int tz) { return tz + 4 * R; }
 
 struct Maps {
-    CUtensorMap p, vx, vz;
+    CUtensorMap p, vx, vz, a1, a2;
 };
 
-int make_maps(const gb_plan *P, const float *buf, Maps *m)
+// Field maps over one state buffer plus the a1 / a2 coefficient maps.
+int make_maps(const gb_plan *P, const float *buf, const float *a1, const float *a2, Maps *m)
 {
     const int n_planes = 3 * P->d.n_shots;
     if (int rc = make_map(&m->p, buf, P->Nx, P->Nz, P->pitch, n_planes, RW, box_rows_p(P->R, P->tz))) return rc;
     if (int rc = make_map(&m->vx, buf, P->Nx, P->Nz, P->pitch, n_planes, VXW, box_rows_p(P->R, P->tz))) return rc;
-    return make_map(&m->vz, buf, P->Nx, P->Nz, P->pitch, n_planes, RW, box_rows_vz(P->R, P->tz));
+    if (int rc = make_map(&m->vz, buf, P->Nx, P->Nz, P->pitch, n_planes, RW, box_rows_vz(P->R, P->tz))) return rc;
+    if (int rc = make_map2d(&m->a1, a1, P->Nx, P->Nz, P->pitch, RW, box_rows_p(P->R, P->tz))) return rc;
+    return make_map2d(&m->a2, a2, P->Nx, P->Nz, P->pitch, RW, P->tz);
 }
 
-template <class Args>
-int launch_step(gb_plan *P, const FwdKernel &K, const Maps &maps, const Args &A, cudaStream_t st)
+// Per-tile fast-path flags (needs the coefficient planes).
+int launch_tile_flags(gb_plan *P, const StepGeom &g, const float *k1, const float *k2, const float *k3, int *flags,
+                      cudaStream_t st)
 {
-    void *args[] = {(void *)&maps.p, (void *)&maps.vx, (void *)&maps.vz, (void *)&A};
-    dim3 grid(P->n_tiles * P->n_groups), block(NTHR);
+    if (P->R == 2 && P->tz == 16) tile_fast_kernel<2, 16><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags);
+    if (P->R == 2 && P->tz == 32) tile_fast_kernel<2, 32><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags);
+    if (P->R == 4 && P->tz == 16) tile_fast_kernel<4, 16><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags);
+    if (P->R == 4 && P->tz == 32) tile_fast_kernel<4, 32><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags);
+    GB_CUDA(cudaGetLastError());
+    ++P->launches;
+    return GB_OK;
+}
+
+// One step kernel launch for shot groups [grp0, grp0 + grp_count).
+template <class Args>
+int launch_step(gb_plan *P, const StepKernel &K, const Maps &maps, Args A, int grp0, int grp_count, cudaStream_t st)
+{
+    A.grp0 = grp0;
+    A.grp_count = grp_count;
+    void *args[] = {(void *)&maps.p, (void *)&maps.vx, (void *)&maps.vz, (void *)&maps.a1, (void *)&maps.a2,
+                    (void *)&A};
+    dim3 grid(P->n_tiles * grp_count), block(NTHR);
     GB_CUDA(cudaLaunchKernel(K.fn, grid, block, args, K.smem, st));
     ++P->launches;
+    return GB_OK;
+}
+
+// Streams the shot groups run on: the caller's stream when there is one
+// group (or grouping is off), else one stream per group forked from it.
+struct GroupStreams {
+    gb_plan *P;
+    cudaStream_t main;
+    int n;            // streams in use (1 = the caller's stream only)
+
+    cudaStream_t at(int grp) const { return n == 1 ? main : P->gstream[grp]; }
+};
+
+int group_streams(gb_plan *P, cudaStream_t main, GroupStreams *gs)
+{
+    gs->P = P;
+    gs->main = main;
+    gs->n = (P->group_streams && P->n_groups > 1) ? P->n_groups : 1;
+    if (gs->n == 1) return GB_OK;
+    int dev = -1;
+    GB_CUDA(cudaGetDevice(&dev));
+    if (dev != P->stream_dev || (int)P->gstream.size() < gs->n) {
+        P->release_streams();
+        for (int i = 0; i < gs->n; ++i) {
+            cudaStream_t s;
+            cudaEvent_t e;
+            GB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            GB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            P->gstream.push_back(s);
+            P->gjoin.push_back(e);
+        }
+        GB_CUDA(cudaEventCreateWithFlags(&P->gfork, cudaEventDisableTiming));
+        P->stream_dev = dev;
+    }
+    return GB_OK;
+}
+
+int fork(const GroupStreams &gs)
+{
+    if (gs.n == 1) return GB_OK;
+    GB_CUDA(cudaEventRecord(gs.P->gfork, gs.main));
+    for (int i = 0; i < gs.n; ++i) GB_CUDA(cudaStreamWaitEvent(gs.P->gstream[i], gs.P->gfork, 0));
+    return GB_OK;
+}
+
+int join(const GroupStreams &gs)
+{
+    if (gs.n == 1) return GB_OK;
+    for (int i = 0; i < gs.n; ++i) {
+        GB_CUDA(cudaEventRecord(gs.P->gjoin[i], gs.P->gstream[i]));
+        GB_CUDA(cudaStreamWaitEvent(gs.main, gs.P->gjoin[i], 0));
+    }
+    return GB_OK;
+}
+
+// groups handled by one launch on stream i: all of them on a single stream
+inline void launch_groups(const GroupStreams &gs, int i, int n_groups, int *g0, int *gc)
+{
+    if (gs.n == 1) {
+        *g0 = 0;
+        *gc = n_groups;
+    } else {
+        *g0 = i;
+        *gc = 1;
+    }
+}
+
+// Per-checkpoint sizes of the 16-bit formats.
+size_t ck16_bytes(const gb_plan *p) { return align256((size_t)p->d.n_shots * 3 * p->plane * 2); }
+size_t ck_scale_bytes(const gb_plan *p) { return align256((size_t)p->d.n_shots * 3 * 4); }
+size_t ck_bytes(const gb_plan *p, int fmt)
+{
+    return fmt == GB_CKPT_F32 ? (size_t)p->d.n_shots * 3 * p->plane * 4 : ck16_bytes(p) + ck_scale_bytes(p);
+}
+
+// Save shots [s0, s0 + ns) of `state` into checkpoint k.
+int save_checkpoint(gb_plan *P, const float *state, void *ckpts, int k, int fmt, unsigned int *amax, int s0, int ns,
+                    cudaStream_t st)
+{
+    const long long pl = P->plane;
+    char *base = reinterpret_cast<char *>(ckpts) + (size_t)k * ck_bytes(P, fmt);
+    const float *src = state + (size_t)s0 * 3 * pl;
+    if (fmt == GB_CKPT_F32) {
+        GB_CUDA(cudaMemcpyAsync(base + (size_t)s0 * 3 * pl * 4, src, (size_t)ns * 3 * pl * 4, cudaMemcpyDeviceToDevice,
+                                st));
+        return GB_OK;
+    }
+    float *scales = reinterpret_cast<float *>(base + ck16_bytes(P)) + 3 * s0;
+    unsigned int *am = amax + 3 * s0;
+    GB_CUDA(cudaMemsetAsync(am, 0, (size_t)ns * 3 * 4, st));
+    dim3 grid(64, ns * 3);
+    plane_absmax_kernel<<<grid, 256, 0, st>>>(src, pl, am);
+    if (fmt == GB_CKPT_BF16)
+        pack16_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
+            src, pl, am, reinterpret_cast<__nv_bfloat16 *>(base) + (size_t)s0 * 3 * pl, scales);
+    else
+        pack16_kernel<__half><<<grid, 256, 0, st>>>(src, pl, am, reinterpret_cast<__half *>(base) + (size_t)s0 * 3 * pl,
+                                                   scales);
+    GB_CUDA(cudaGetLastError());
+    P->launches += 2;
+    return GB_OK;
+}
+
+int restore_checkpoint(gb_plan *P, float *state, const void *ckpts, int k, int fmt, int s0, int ns, cudaStream_t st)
+{
+    const long long pl = P->plane;
+    const char *base = reinterpret_cast<const char *>(ckpts) + (size_t)k * ck_bytes(P, fmt);
+    float *dst = state + (size_t)s0 * 3 * pl;
+    if (fmt == GB_CKPT_F32) {
+        GB_CUDA(cudaMemcpyAsync(dst, base + (size_t)s0 * 3 * pl * 4, (size_t)ns * 3 * pl * 4, cudaMemcpyDeviceToDevice,
+                                st));
+        return GB_OK;
+    }
+    const float *scales = reinterpret_cast<const float *>(base + ck16_bytes(P)) + 3 * s0;
+    dim3 grid(64, ns * 3);
+    if (fmt == GB_CKPT_BF16)
+        unpack16_kernel<__nv_bfloat16><<<grid, 256, 0, st>>>(
+            reinterpret_cast<const __nv_bfloat16 *>(base) + (size_t)s0 * 3 * pl, scales, pl, dst);
+    else
+        unpack16_kernel<__half><<<grid, 256, 0, st>>>(reinterpret_cast<const __half *>(base) + (size_t)s0 * 3 * pl,
+                                                     scales, pl, dst);
+    GB_CUDA(cudaGetLastError());
+    ++P->launches;
+    return GB_OK;
+}
+
+// Everything both passes set up: metadata upload, coefficient planes, flags.
+struct Setup {
+    int *err;
+    float *a1, *k1, *a2, *k2, *k3;
+    int *d_src, *d_rptr, *tile_fast;
+    int4 *d_rent;
+    unsigned int *amax;
+};
+
+int common_setup(gb_plan *P, const Layout &L, char *ws, const float *vp, const float *rho, const float *damp,
+                 cudaStream_t st, Setup *S)
+{
+    const gb_model_desc &d = P->d;
+    S->err = reinterpret_cast<int *>(ws + L.err);
+    float *coef = reinterpret_cast<float *>(ws + L.coef);
+    S->a1 = coef;
+    S->k1 = coef + P->plane;
+    S->a2 = coef + 2 * P->plane;
+    S->k2 = coef + 3 * P->plane;
+    S->k3 = coef + 4 * P->plane;
+    S->d_src = reinterpret_cast<int *>(ws + L.src);
+    S->d_rptr = reinterpret_cast<int *>(ws + L.rcv_ptr);
+    S->d_rent = reinterpret_cast<int4 *>(ws + L.rcv_ent);
+    S->tile_fast = reinterpret_cast<int *>(ws + L.tile_fast);
+    S->amax = reinterpret_cast<unsigned int *>(ws + L.amax);
+    GB_CUDA(cudaMemsetAsync(S->err, 0, 4, st));
+    GB_CUDA(cudaMemcpyAsync(S->d_src, P->src_z.data(), d.n_shots * 4, cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(S->d_src + d.n_shots, P->src_x.data(), d.n_shots * 4, cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(S->d_rptr, P->rcv_ptr.data(), (P->n_tiles + 1) * 4, cudaMemcpyHostToDevice, st));
+    if (d.n_rcv) GB_CUDA(cudaMemcpyAsync(S->d_rent, P->rcv_ent.data(), d.n_rcv * 16, cudaMemcpyHostToDevice, st));
+    coef_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, damp, d.nz, d.nx, d.nabc, P->Nz, P->Nx, P->pitch, P->fs, d.dt, d.dx,
+                                         S->a1, S->k1, S->a2, S->k2, S->k3);
+    GB_CUDA(cudaGetLastError());
+    ++P->launches;
+    return launch_tile_flags(P, P->geom(), S->k1, S->k2, S->k3, S->tile_fast, st);
+}
+
+char *aligned_ws(void *workspace) { return reinterpret_cast<char *>(align256(reinterpret_cast<uintptr_t>(workspace))); }
+
+int check_store(const gb_plan *P, const gb_grad_store *store)
+{
+    if (!store) return GB_OK;
+    if (store->checkpoint_every < 1) return fail(GB_E_ARG, "checkpoint_every must be >= 1");
+    if (store->format < GB_CKPT_F32 || store->format > GB_CKPT_F16) return fail(GB_E_ARG, "unknown checkpoint format");
+    if (store->cached_steps < 0 || store->cached_steps > P->d.nt) return fail(GB_E_ARG, "cached_steps out of range");
+    if (store->cached_steps > 0 && !store->imaging) return fail(GB_E_ARG, "cached_steps > 0 needs an imaging buffer");
+    if (store->cached_steps < P->d.nt && !store->checkpoints) return fail(GB_E_ARG, "checkpoint storage missing");
     return GB_OK;
 }
 
@@ -330,7 +573,7 @@ extern "C" {
 
 const char *gb_last_error(void) { return g_last_error.c_str(); }
 
-const char *gb_version(void) { return "geobrain_b200 0.1 (sm_100a)"; }
+const char *gb_version(void) { return "geobrain_b200 0.2 (sm_100a)"; }
 
 int gb_plan_create(const gb_model_desc *desc, const int64_t *src_x, const int64_t *src_z, const int64_t *rcv_x,
                    const int64_t *rcv_z, gb_plan **out)
@@ -400,8 +643,15 @@ int gb_plan_set_tiling(gb_plan *p, int tile_rows, int shots_per_cta)
     if (tile_rows != 0 && tile_rows != 16 && tile_rows != 32) return fail(GB_E_ARG, "tile_rows must be 16 or 32");
     if (shots_per_cta < 0) return fail(GB_E_ARG, "shots_per_cta must be >= 0");
     if (tile_rows) p->tz = tile_rows;
-    p->spc = shots_per_cta ? std::min(shots_per_cta, p->d.n_shots) : 0;
+    p->spc = shots_per_cta ? std::min(std::min(shots_per_cta, p->d.n_shots), kMaxShotsPerCta) : 0;
     p->retile();
+    return GB_OK;
+}
+
+int gb_plan_set_group_streams(gb_plan *p, int enable)
+{
+    if (!p) return fail(GB_E_ARG, "null plan");
+    p->group_streams = enable != 0;
     return GB_OK;
 }
 
@@ -415,91 +665,98 @@ size_t gb_plan_checkpoint_bytes(const gb_plan *p, int checkpoint_every, int ckpt
 {
     if (!p || checkpoint_every < 1) return 0;
     const size_t n_ck = (p->d.nt + checkpoint_every - 1) / checkpoint_every;
-    const size_t per = (size_t)p->d.n_shots * 3 * p->plane;
-    if (ckpt_format == GB_CKPT_F32) return n_ck * per * 4;
-    return n_ck * (align256(per * 2) + align256((size_t)p->d.n_shots * 3 * 4));
+    return n_ck * ck_bytes(p, ckpt_format);
+}
+
+size_t gb_plan_imaging_bytes(const gb_plan *p, int cached_steps, int with_rho)
+{
+    if (!p || cached_steps < 0) return 0;
+    return (size_t)cached_steps * (with_rho ? 3 : 1) * p->d.n_shots * p->plane * 4;
 }
 
 int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp, const float *wavelet,
                float *trace_p, float *trace_vx, float *trace_vz, float *energy_p, float *energy_vx,
-               float *energy_vz, int32_t snapshot_every, float *snapshots, void *checkpoints,
-               int32_t checkpoint_every, int32_t ckpt_format, void *workspace, size_t workspace_bytes,
-               void *stream)
+               float *energy_vz, int32_t snapshot_every, float *snapshots, const gb_grad_store *store,
+               void *workspace, size_t workspace_bytes, void *stream)
 {
     g_last_error.clear();
     if (!P || !vp || !rho || !damp || !wavelet) return fail(GB_E_ARG, "null argument");
-    if (checkpoints && ckpt_format != GB_CKPT_F32) return fail(GB_E_UNSUPPORTED, "checkpoint format not built yet");
+    if (int rc = check_store(P, store)) return rc;
     const Layout L = layout(P);
-    char *ws = reinterpret_cast<char *>(align256(reinterpret_cast<uintptr_t>(workspace)));
+    char *ws = aligned_ws(workspace);
     if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
         return fail(GB_E_WORKSPACE, "workspace too small");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const gb_model_desc &d = P->d;
     const int S = d.n_shots;
     const bool want_energy = energy_p || energy_vx || energy_vz;
+    const int K = store ? std::min<int>(store->checkpoint_every, d.nt) : 0;
+    const int t_cache = store ? d.nt - store->cached_steps : d.nt;   // steps >= t_cache keep their imaging fields
+    const int n_img = store && store->with_rho ? 3 : 1;
 
-    int *err = reinterpret_cast<int *>(ws + L.err);
-    float *coef = reinterpret_cast<float *>(ws + L.coef);
-    float *a1 = coef, *k1 = coef + P->plane, *a2 = coef + 2 * P->plane, *k2 = coef + 3 * P->plane,
-          *k3 = coef + 4 * P->plane;
+    P->mark(0, true, st);
+    Setup Su;
+    if (int rc = common_setup(P, L, ws, vp, rho, damp, st, &Su)) return rc;
     float *buf[2] = {reinterpret_cast<float *>(ws + L.fields),
                      reinterpret_cast<float *>(ws + L.fields) + (size_t)S * 3 * P->plane};
     float *energy = reinterpret_cast<float *>(ws + L.energy);
-    int *d_src = reinterpret_cast<int *>(ws + L.src);
-    int *d_rptr = reinterpret_cast<int *>(ws + L.rcv_ptr);
-    int4 *d_rent = reinterpret_cast<int4 *>(ws + L.rcv_ent);
-
-    GB_CUDA(cudaMemsetAsync(err, 0, 4, st));
-    GB_CUDA(cudaMemcpyAsync(d_src, P->src_z.data(), S * 4, cudaMemcpyHostToDevice, st));
-    GB_CUDA(cudaMemcpyAsync(d_src + S, P->src_x.data(), S * 4, cudaMemcpyHostToDevice, st));
-    GB_CUDA(cudaMemcpyAsync(d_rptr, P->rcv_ptr.data(), (P->n_tiles + 1) * 4, cudaMemcpyHostToDevice, st));
-    if (d.n_rcv)
-        GB_CUDA(cudaMemcpyAsync(d_rent, P->rcv_ent.data(), d.n_rcv * 16, cudaMemcpyHostToDevice, st));
     GB_CUDA(cudaMemsetAsync(buf[0], 0, (size_t)S * 3 * P->plane * 4, st));
     GB_CUDA(cudaMemsetAsync(buf[1], 0, (size_t)S * 3 * P->plane * 4, st));
     if (want_energy) GB_CUDA(cudaMemsetAsync(energy, 0, 3 * P->plane * 4, st));
 
-    P->mark(0, true, st);
-    coef_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, damp, d.nz, d.nx, d.nabc, P->Nz, P->Nx, P->pitch, P->fs, d.dt,
-                                         d.dx, a1, k1, a2, k2, k3);
-    GB_CUDA(cudaGetLastError());
-    ++P->launches;
-
-    FwdKernel K = fwd_kernel(P->R, P->tz, d.free_surface != 0, want_energy, 0);
-    if (!K.fn) return fail(GB_E_UNSUPPORTED, "no kernel for this configuration");
-    GB_CUDA(cudaFuncSetAttribute(K.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem));
+    const bool fs = d.free_surface != 0;
+    const StepKernel K0 = fwd_kernel(P->R, P->tz, fs, want_energy, 0);
+    const StepKernel KI = fwd_kernel(P->R, P->tz, fs, want_energy, n_img == 3 ? 2 : 1);
+    if (int rc = prepare_kernel(K0)) return rc;
+    if (store && store->cached_steps > 0)
+        if (int rc = prepare_kernel(KI)) return rc;
     Maps maps[2];
     for (int b = 0; b < 2; ++b)
-        if (int rc = make_maps(P, buf[b], &maps[b])) return rc;
+        if (int rc = make_maps(P, buf[b], Su.a1, Su.a2, &maps[b])) return rc;
 
     FwdArgs A{};
     A.g = P->geom();
-    A.a1 = a1; A.k1 = k1; A.a2 = a2; A.k2 = k2; A.k3 = k3;
-    A.src_z = d_src; A.src_x = d_src + S;
+    A.tile_fast = Su.tile_fast;
+    A.a1 = Su.a1; A.k1 = Su.k1; A.a2 = Su.a2; A.k2 = Su.k2; A.k3 = Su.k3;
+    A.src_z = Su.d_src; A.src_x = Su.d_src + S;
     A.wavelet = wavelet;
-    A.rcv_ptr = d_rptr; A.rcv_ent = d_rent;
+    A.rcv_ptr = Su.d_rptr; A.rcv_ent = Su.d_rent;
     A.tr_p = trace_p; A.tr_vx = trace_vx; A.tr_vz = trace_vz;
     A.energy = want_energy ? energy : nullptr;
-    A.imaging = nullptr;
-    A.err = err;
+    A.img_field_stride = (long long)S * P->plane;
+    A.err = Su.err;
 
-    const size_t state_bytes = (size_t)S * 3 * P->plane * 4;
+    GroupStreams gs;
+    if (int rc = group_streams(P, st, &gs)) return rc;
+    if (int rc = fork(gs)) return rc;
+    const size_t step_img = (size_t)n_img * S * P->plane;
     int snap_i = 0;
     for (int it = 0; it < d.nt; ++it) {
         const int b = it & 1;
-        if (checkpoints && checkpoint_every > 0 && it % checkpoint_every == 0)
-            GB_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(checkpoints) + (size_t)(it / checkpoint_every) * state_bytes,
-                                    buf[b], state_bytes, cudaMemcpyDeviceToDevice, st));
         A.it = it;
         A.out = buf[b ^ 1];
-        if (int rc = launch_step(P, K, maps[b], A, st)) return rc;
-        if (snapshot_every > 0 && snapshots && ((it + 1) % snapshot_every == 0 || it == d.nt - 1)) {
-            GB_CUDA(cudaMemcpy2DAsync(snapshots + (size_t)snap_i * d.nz * d.nx, (size_t)d.nx * 4,
-                                      buf[b ^ 1] + (size_t)d.nabc * P->pitch + d.nabc, (size_t)P->pitch * 4,
-                                      (size_t)d.nx * 4, d.nz, cudaMemcpyDeviceToDevice, st));
-            ++snap_i;
+        const bool keep = store && it >= t_cache;
+        A.imaging = keep ? reinterpret_cast<float *>(store->imaging) + (size_t)(it - t_cache) * step_img : nullptr;
+        for (int i = 0; i < gs.n; ++i) {
+            int g0, gc;
+            launch_groups(gs, i, P->n_groups, &g0, &gc);
+            const cudaStream_t si = gs.at(i);
+            if (store && it < t_cache && it % K == 0) {
+                const int s0 = P->group_first(g0);
+                const int ns = gs.n == 1 ? S : P->group_shots(g0);
+                if (int rc = save_checkpoint(P, buf[b], store->checkpoints, it / K, store->format, Su.amax, s0, ns, si))
+                    return rc;
+            }
+            if (int rc = launch_step(P, keep ? KI : K0, maps[b], A, g0, gc, si)) return rc;
+            if (snapshot_every > 0 && snapshots && g0 == 0 && ((it + 1) % snapshot_every == 0 || it == d.nt - 1)) {
+                GB_CUDA(cudaMemcpy2DAsync(snapshots + (size_t)snap_i * d.nz * d.nx, (size_t)d.nx * 4,
+                                          buf[b ^ 1] + (size_t)d.nabc * P->pitch + d.nabc, (size_t)P->pitch * 4,
+                                          (size_t)d.nx * 4, d.nz, cudaMemcpyDeviceToDevice, si));
+                ++snap_i;
+            }
         }
     }
+    if (int rc = join(gs)) return rc;
     float *eouts[3] = {energy_p, energy_vx, energy_vz};
     for (int f = 0; f < 3; ++f)
         if (eouts[f]) {
@@ -513,46 +770,35 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
 }
 
 int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp, const float *wavelet,
-                const float *res_p, const float *res_vx, const float *res_vz, const void *checkpoints,
-                int32_t checkpoint_every, int32_t ckpt_format, float *grad_vp, float *grad_rho, void *workspace,
-                size_t workspace_bytes, void *stream)
+                const float *res_p, const float *res_vx, const float *res_vz, const gb_grad_store *store,
+                float *grad_vp, float *grad_rho, void *workspace, size_t workspace_bytes, void *stream)
 {
     g_last_error.clear();
-    if (!P || !vp || !rho || !damp || !wavelet || !checkpoints || !grad_vp) return fail(GB_E_ARG, "null argument");
-    if (checkpoint_every < 1) return fail(GB_E_ARG, "checkpoint_every must be >= 1");
-    if (ckpt_format != GB_CKPT_F32) return fail(GB_E_UNSUPPORTED, "checkpoint format not built yet");
+    if (!P || !vp || !rho || !damp || !wavelet || !store || !grad_vp) return fail(GB_E_ARG, "null argument");
+    if (int rc = check_store(P, store)) return rc;
+    if (grad_rho && !store->with_rho) return fail(GB_E_ARG, "density gradient needs a store made with with_rho");
     const gb_model_desc &d = P->d;
     const int S = d.n_shots;
-    const int K = std::min<int>(checkpoint_every, d.nt);
-    const int with_grad = grad_rho ? 2 : 1;
+    const int K = std::min<int>(store->checkpoint_every, d.nt);
+    const bool rho_fields = store->with_rho != 0;
+    const int with_grad = rho_fields ? 2 : 1;
     const Layout L = layout(P, with_grad, K);
-    char *ws = reinterpret_cast<char *>(align256(reinterpret_cast<uintptr_t>(workspace)));
+    char *ws = aligned_ws(workspace);
     if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
         return fail(GB_E_WORKSPACE, "workspace too small");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
 
-    int *err = reinterpret_cast<int *>(ws + L.err);
-    float *coef = reinterpret_cast<float *>(ws + L.coef);
-    float *a1 = coef, *k1 = coef + P->plane, *a2 = coef + 2 * P->plane, *k2 = coef + 3 * P->plane,
-          *k3 = coef + 4 * P->plane;
+    Setup Su;
+    if (int rc = common_setup(P, L, ws, vp, rho, damp, st, &Su)) return rc;
     const size_t state_fl = (size_t)S * 3 * P->plane;
     float *fb[2] = {reinterpret_cast<float *>(ws + L.fields), reinterpret_cast<float *>(ws + L.fields) + state_fl};
     float *mu[2] = {reinterpret_cast<float *>(ws + L.mu), reinterpret_cast<float *>(ws + L.mu) + state_fl};
-    float *img = reinterpret_cast<float *>(ws + L.img);
+    float *wimg = reinterpret_cast<float *>(ws + L.img);
     float *G1 = reinterpret_cast<float *>(ws + L.g1), *C1 = reinterpret_cast<float *>(ws + L.c1);
-    float *G2 = with_grad >= 2 ? reinterpret_cast<float *>(ws + L.g2) : nullptr;
-    float *C2 = with_grad >= 2 ? reinterpret_cast<float *>(ws + L.c2) : nullptr;
-    int *d_src = reinterpret_cast<int *>(ws + L.src);
-    int *d_rptr = reinterpret_cast<int *>(ws + L.rcv_ptr);
-    int4 *d_rent = reinterpret_cast<int4 *>(ws + L.rcv_ent);
+    float *G2 = rho_fields ? reinterpret_cast<float *>(ws + L.g2) : nullptr;
+    float *C2 = rho_fields ? reinterpret_cast<float *>(ws + L.c2) : nullptr;
     int *d_aptr = reinterpret_cast<int *>(ws + L.arcv_ptr);
     int4 *d_aent = reinterpret_cast<int4 *>(ws + L.arcv_ent);
-
-    GB_CUDA(cudaMemsetAsync(err, 0, 4, st));
-    GB_CUDA(cudaMemcpyAsync(d_src, P->src_z.data(), S * 4, cudaMemcpyHostToDevice, st));
-    GB_CUDA(cudaMemcpyAsync(d_src + S, P->src_x.data(), S * 4, cudaMemcpyHostToDevice, st));
-    GB_CUDA(cudaMemcpyAsync(d_rptr, P->rcv_ptr.data(), (P->n_tiles + 1) * 4, cudaMemcpyHostToDevice, st));
-    if (d.n_rcv) GB_CUDA(cudaMemcpyAsync(d_rent, P->rcv_ent.data(), d.n_rcv * 16, cudaMemcpyHostToDevice, st));
     GB_CUDA(cudaMemcpyAsync(d_aptr, P->arcv_ptr.data(), (P->n_tiles + 1) * 4, cudaMemcpyHostToDevice, st));
     if (!P->arcv_ent.empty())
         GB_CUDA(cudaMemcpyAsync(d_aent, P->arcv_ent.data(), P->arcv_ent.size() * 16, cudaMemcpyHostToDevice, st));
@@ -563,71 +809,114 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
         GB_CUDA(cudaMemsetAsync(G2, 0, (size_t)P->n_groups * P->plane * 4, st));
         GB_CUDA(cudaMemsetAsync(C2, 0, (size_t)P->n_groups * P->plane * 4, st));
     }
-    coef_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, damp, d.nz, d.nx, d.nabc, P->Nz, P->Nx, P->pitch, P->fs, d.dt,
-                                         d.dx, a1, k1, a2, k2, k3);
-    GB_CUDA(cudaGetLastError());
-    ++P->launches;
 
     const bool fs = d.free_surface != 0;
-    FwdKernel KF = fwd_kernel(P->R, P->tz, fs, false, with_grad);
-    FwdKernel KA = adj_kernel(P->R, P->tz, fs, with_grad >= 2);
-    if (!KF.fn || !KA.fn) return fail(GB_E_UNSUPPORTED, "no kernel for this configuration");
-    GB_CUDA(cudaFuncSetAttribute(KF.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KF.smem));
-    GB_CUDA(cudaFuncSetAttribute(KA.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KA.smem));
+    const StepKernel KF = fwd_kernel(P->R, P->tz, fs, false, rho_fields ? 2 : 1);
+    const StepKernel KA = adj_kernel(P->R, P->tz, fs, rho_fields);
+    if (int rc = prepare_kernel(KF)) return rc;
+    if (int rc = prepare_kernel(KA)) return rc;
     Maps fmaps[2], amaps[2];
     for (int b = 0; b < 2; ++b) {
-        if (int rc = make_maps(P, fb[b], &fmaps[b])) return rc;
-        if (int rc = make_maps(P, mu[b], &amaps[b])) return rc;
+        if (int rc = make_maps(P, fb[b], Su.a1, Su.a2, &fmaps[b])) return rc;
+        if (int rc = make_maps(P, mu[b], Su.a1, Su.a2, &amaps[b])) return rc;
     }
 
     const StepGeom g = P->geom();
     FwdArgs F{};
     F.g = g;
-    F.a1 = a1; F.k1 = k1; F.a2 = a2; F.k2 = k2; F.k3 = k3;
-    F.src_z = d_src; F.src_x = d_src + S;
+    F.a1 = Su.a1; F.k1 = Su.k1; F.a2 = Su.a2; F.k2 = Su.k2; F.k3 = Su.k3;
+    F.tile_fast = Su.tile_fast;
+    F.src_z = Su.d_src; F.src_x = Su.d_src + S;
     F.wavelet = wavelet;
-    F.rcv_ptr = d_rptr; F.rcv_ent = d_rent;
-    F.err = err;
+    F.rcv_ptr = Su.d_rptr; F.rcv_ent = Su.d_rent;
+    F.err = Su.err;
     F.img_field_stride = (long long)S * P->plane;
     AdjArgs A{};
     A.g = g;
-    A.a1 = a1; A.k1 = k1; A.a2 = a2; A.k2 = k2; A.k3 = k3;
+    A.a1 = Su.a1; A.k1 = Su.k1; A.a2 = Su.a2; A.k2 = Su.k2; A.k3 = Su.k3;
+    A.tile_fast = Su.tile_fast;
     A.rcv_ptr = d_aptr; A.rcv_ent = d_aent;
     A.res_p = res_p; A.res_vx = res_vx; A.res_vz = res_vz;
     A.img_field_stride = (long long)S * P->plane;
     A.G1 = G1; A.C1 = C1; A.G2 = G2; A.C2 = C2;
-    A.err = err;
+    A.err = Su.err;
 
-    const size_t step_img = (size_t)L.n_img * S * P->plane;
-    const int n_seg = (d.nt + K - 1) / K;
-    int cur = 0;
+    GroupStreams gs;
+    if (int rc = group_streams(P, st, &gs)) return rc;
+    const size_t step_img = (size_t)(rho_fields ? 3 : 1) * S * P->plane;
+    const int t_cache = d.nt - store->cached_steps;
+    int cur = 0;   // adjoint state lives in mu[cur]
+
+    // adjoint sweep over [t0, t1) in reverse, imaging fields at img_base[(it - t0)]
+    auto adjoint_sweep = [&](int t0, int t1, const float *img_base) -> int {
+        P->mark(2, true, st);
+        if (int rc = fork(gs)) return rc;
+        for (int it = t1 - 1; it >= t0; --it) {
+            A.it = it;
+            A.out = mu[cur ^ 1];
+            A.img = img_base + (size_t)(it - t0) * step_img;
+            for (int i = 0; i < gs.n; ++i) {
+                int g0, gc;
+                launch_groups(gs, i, P->n_groups, &g0, &gc);
+                if (int rc = launch_step(P, KA, amaps[cur], A, g0, gc, gs.at(i))) return rc;
+            }
+            cur ^= 1;
+        }
+        if (int rc = join(gs)) return rc;
+        P->mark(2, false, st);
+        return GB_OK;
+    };
+
+    // 1. steps whose imaging fields the forward kept
+    if (store->cached_steps > 0)
+        if (int rc = adjoint_sweep(t_cache, d.nt, reinterpret_cast<const float *>(store->imaging))) return rc;
+    // 2. earlier steps, one checkpoint segment at a time: fp32 recompute from
+    //    the checkpoint (writing the imaging fields), then the adjoint sweep
+    const int n_seg = (t_cache + K - 1) / K;
     for (int seg = n_seg - 1; seg >= 0; --seg) {
-        const int t0 = seg * K, t1 = std::min(d.nt, t0 + K);
-        GB_CUDA(cudaMemcpyAsync(fb[0], reinterpret_cast<const char *>(checkpoints) + (size_t)seg * state_fl * 4,
-                                state_fl * 4, cudaMemcpyDeviceToDevice, st));
+        const int t0 = seg * K, t1 = std::min(t_cache, t0 + K);
         P->mark(1, true, st);
+        if (int rc = fork(gs)) return rc;
+        for (int i = 0; i < gs.n; ++i) {
+            int g0, gc;
+            launch_groups(gs, i, P->n_groups, &g0, &gc);
+            const int s0 = P->group_first(g0), ns = gs.n == 1 ? S : P->group_shots(g0);
+            if (int rc = restore_checkpoint(P, fb[0], store->checkpoints, seg, store->format, s0, ns, gs.at(i)))
+                return rc;
+        }
         for (int it = t0; it < t1; ++it) {
             const int b = (it - t0) & 1;
             F.it = it;
             F.out = fb[b ^ 1];
-            F.imaging = img + (size_t)(it - t0) * step_img;
-            if (int rc = launch_step(P, KF, fmaps[b], F, st)) return rc;
+            F.imaging = wimg + (size_t)(it - t0) * step_img;
+            for (int i = 0; i < gs.n; ++i) {
+                int g0, gc;
+                launch_groups(gs, i, P->n_groups, &g0, &gc);
+                if (int rc = launch_step(P, KF, fmaps[b], F, g0, gc, gs.at(i))) return rc;
+            }
         }
+        if (int rc = join(gs)) return rc;
         P->mark(1, false, st);
-        P->mark(2, true, st);
-        for (int it = t1 - 1; it >= t0; --it) {
-            A.it = it;
-            A.out = mu[cur ^ 1];
-            A.img = img + (size_t)(it - t0) * step_img;
-            if (int rc = launch_step(P, KA, amaps[cur], A, st)) return rc;
-            cur ^= 1;
-        }
-        P->mark(2, false, st);
+        if (int rc = adjoint_sweep(t0, t1, wimg)) return rc;
     }
     grad_finish_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, G1, C1, G2, C2, P->n_groups, P->plane, d.nz, d.nx, d.nabc,
                                                 P->pitch, grad_vp, grad_rho);
     GB_CUDA(cudaGetLastError());
     ++P->launches;
+    return GB_OK;
+}
+
+int gb_workspace_status(const void *workspace, void *stream)
+{
+    g_last_error.clear();
+    if (!workspace) return fail(GB_E_ARG, "null workspace");
+    const char *ws = reinterpret_cast<const char *>(align256(reinterpret_cast<uintptr_t>(workspace)));
+    int flag = 0;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    GB_CUDA(cudaMemcpyAsync(&flag, ws, 4, cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaStreamSynchronize(st));
+    if (flag == GB_E_TIMEOUT) return fail(GB_E_TIMEOUT, "a device-side wait timed out");
+    if (flag != 0) return fail(flag, "device error flag set");
     return GB_OK;
 }
 
@@ -657,20 +946,6 @@ int gb_plan_profile(gb_plan *P, double *ms_forward, double *ms_recompute, double
     if (launches) *launches = P->launches;
     P->clear_events();
     P->launches = 0;
-    return GB_OK;
-}
-
-int gb_workspace_status(const void *workspace, void *stream)
-{
-    g_last_error.clear();
-    if (!workspace) return fail(GB_E_ARG, "null workspace");
-    const char *ws = reinterpret_cast<const char *>(align256(reinterpret_cast<uintptr_t>(workspace)));
-    int flag = 0;
-    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-    GB_CUDA(cudaMemcpyAsync(&flag, ws, 4, cudaMemcpyDeviceToHost, st));
-    GB_CUDA(cudaStreamSynchronize(st));
-    if (flag == GB_E_TIMEOUT) return fail(GB_E_TIMEOUT, "a device-side wait timed out");
-    if (flag != 0) return fail(flag, "device error flag set");
     return GB_OK;
 }
 
@@ -732,5 +1007,5 @@ extern "C" int gb_forward_static_scratch(gb_plan *P, const float *vp, const floa
     // gb_forward clears every part of the scratch that must start at zero
     // (both wavefield time levels, the energy sums, the status word)
     return gb_forward(P, vp, rho, damp, wavelet, trace_p, trace_vx, trace_vz, energy_p, energy_vx, energy_vz,
-                      snapshot_every, snapshots, nullptr, 0, GB_CKPT_F32, scratch, kStaticScratchBytes, stream);
+                      snapshot_every, snapshots, nullptr, scratch, kStaticScratchBytes, stream);
 }

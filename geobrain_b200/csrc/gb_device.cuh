@@ -29,6 +29,7 @@ constexpr int RW = 128;          // sP / sVZ row pitch (floats)
 constexpr int VXW = 136;         // sVX row pitch (floats)
 constexpr int NWARP = 8;
 constexpr int NTHR = NWARP * 32;
+constexpr int kMaxShotsPerCta = 64;
 
 template <int R, int TZ>
 struct Geo {

@@ -14,9 +14,14 @@
 // The two free-surface mirror rows are never stored: row fs-1 of p and vz is
 // only ever read by the next stage, so each CTA rebuilds it in shared memory
 // from the rows it mirrors.  Every other cell follows the reference exactly.
+//
+// Tiles whose halo rectangles lie inside every update mask and see no
+// damping (most of the grid: the PML is a thin frame) take a fast path with
+// no per-cell masks and no damping terms; the arithmetic of the cells is the
+// same either way.
 #pragma once
 
-#include "gb_device.cuh"
+#include "gb_stencil.cuh"
 
 namespace gb {
 
@@ -38,6 +43,7 @@ struct FwdArgs {
     StepGeom g;
     int it;                          // time step index
     const float *a1, *k1, *a2, *k2, *k3;   // coefficient planes, Nz x pitch
+    const int *tile_fast;            // per tile: 1 = no masks and no damping anywhere it reads
     float *out;                      // next state [S][3][plane]
     const int *src_z, *src_x;        // padded source cells
     const float *wavelet;            // [S][nt]
@@ -47,6 +53,7 @@ struct FwdArgs {
     float *energy;                   // [3][plane] padded accumulators or null
     float *imaging;                  // [S][plane] -div(v) on the p mask, or null
     long long img_field_stride;      // IMG == 2: dx(p), dz(p) blocks follow at this stride
+    int grp0, grp_count;             // shot groups this launch covers
     int *err;
 };
 
@@ -61,22 +68,51 @@ __device__ __forceinline__ void stage_loads(const CUtensorMap *mP, const CUtenso
     tma_load_3d(buf + P_FL + VX_FL, mVZ, bar, x0 - 4, z0 - 2 * R, 3 * s + 2);
 }
 
+// Shared-memory layout of both step kernels: two field stages, then a1 on
+// the p rectangle and a2 on the tile rows (loaded once per CTA), then the
+// mbarriers.
+template <int R, int TZ>
+struct StepSmem {
+    using G = Geo<R, TZ>;
+    static constexpr int A1_FL = G::PR * RW;
+    static constexpr int A2_FL = TZ * RW;
+    static constexpr int COEF_FL = A1_FL + A2_FL;
+    static constexpr uint32_t COEF_BYTES = COEF_FL * 4u;
+    static constexpr size_t BYTES = 2 * G::STAGE_BYTES + COEF_BYTES + 32;
+};
+
+// Does this tile need per-cell masks?  (Pure geometry; the damping part of
+// the fast-path test is precomputed per tile in tile_fast.)
+template <int R, int TZ>
+__device__ __forceinline__ bool tile_is_interior(const StepGeom &g, int z0, int x0)
+{
+    return z0 - 2 * R >= g.fs + 1 && z0 - R >= g.p_r0 && z0 + TZ + R - 1 <= g.p_r1 && x0 - 4 >= g.p_c0 &&
+           x0 + TX + 3 <= g.p_c1 && z0 >= g.vx_r0 && z0 >= g.vz_r0 && z0 + TZ - 1 <= g.vx_r1 &&
+           z0 + TZ - 1 <= g.vz_r1 && x0 >= g.vx_c0 && x0 >= g.vz_c0 && x0 + TX - 1 <= g.vx_c1 &&
+           x0 + TX - 1 <= g.vz_c1;
+}
+
 // IMG: 0 no imaging fields; 1 store I = -div(v^n) on the p mask (velocity
 // gradient); 2 also store Jx = dx(p), Jz = dz(p) on the vx / vz masks (density).
 template <int R, int TZ, bool FS, bool ENERGY, int IMG>
-__global__ void __launch_bounds__(NTHR, 1)
+__global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
 fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mVX,
-                const __grid_constant__ CUtensorMap mVZ, const FwdArgs A)
+                const __grid_constant__ CUtensorMap mVZ, const __grid_constant__ CUtensorMap mA1,
+                const __grid_constant__ CUtensorMap mA2, const FwdArgs A)
 {
     using G = Geo<R, TZ>;
+    using SM = StepSmem<R, TZ>;
     const StepGeom &g = A.g;
     extern __shared__ __align__(128) float smem[];
-    float *stage[2] = {smem, smem + G::STAGE_FL};
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * G::STAGE_FL);
-    float *eacc = reinterpret_cast<float *>(bars + 2);   // [3][TZ][TX] when ENERGY
+    __shared__ int2 s_src[kMaxShotsPerCta];   // (z, x) source cell of each shot of this CTA
+    float *sA1 = smem + 2 * G::STAGE_FL;
+    float *sA2 = sA1 + SM::A1_FL;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sA1 + SM::COEF_FL);
 
-    const int group = blockIdx.x % g.n_groups;
-    const int tile = blockIdx.x / g.n_groups;
+    // launch covers shot groups [grp0, grp0 + grp_count): one launch for all
+    // groups, or one launch per group when groups run on their own streams
+    const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
+    const int tile = (int)(blockIdx.x / A.grp_count);
     const int z0 = (tile / g.tiles_x) * TZ;
     const int x0 = (tile % g.tiles_x) * TX;
     const int s0 = group * g.shots_per_cta;
@@ -86,26 +122,46 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
         fence_mbar_init();
     }
     __syncthreads();
     if (threadIdx.x == 0) {
+        mbar_arrive_expect_tx(&bars[2], SM::COEF_BYTES);
+        tma_load_2d(sA1, &mA1, &bars[2], x0 - 4, z0 - R);
+        tma_load_2d(sA2, &mA2, &bars[2], x0 - 4, z0);
         for (int k = 0; k < 2 && k < ns; ++k)
-            stage_loads<R>(&mP, &mVX, &mVZ, stage[k], &bars[k], G::STAGE_BYTES, x0, z0, s0 + k, G::P_FL,
-                           G::VX_FL);
+            stage_loads<R>(&mP, &mVX, &mVZ, smem + k * G::STAGE_FL, &bars[k], G::STAGE_BYTES, x0, z0, s0 + k,
+                           G::P_FL, G::VX_FL);
     }
-    if (ENERGY) {
-        for (int i = threadIdx.x; i < 3 * TZ * TX; i += NTHR) eacc[i] = 0.f;
+    for (int k = threadIdx.x; k < ns; k += NTHR) s_src[k] = make_int2(A.src_z[s0 + k], A.src_x[s0 + k]);
+    const bool fast = A.tile_fast[tile] != 0;
+    const int rcv0 = A.rcv_ptr[tile], rcv1 = A.rcv_ptr[tile + 1];
+    const bool has_rcv = rcv1 > rcv0 && (A.tr_p || A.tr_vx || A.tr_vz);
+    if (!__syncthreads_and(mbar_wait_bounded(&bars[2], 0))) {
+        if (threadIdx.x == 0) {
+            atomicExch(A.err, -4);
+            for (int k = 0; k < 2 && k < ns; ++k) mbar_wait_bounded(&bars[k], 0);
+        }
+        return;
     }
 
-    // this thread's columns in the 128-wide rectangles: x0 - 4 + 4*lane + q
-    const int gx0 = x0 - 4 + 4 * lane;
+    const int gx0 = x0 - 4 + 4 * lane;   // first of this thread's 4 columns
+    const int rb = warp * G::LP, rc = min(G::LP, G::PR - rb);      // p-stage rows of this warp
+    const int vb = warp * G::LV, vcnt = min(G::LV, TZ - vb);       // v-stage rows of this warp
+    const bool vlane = lane >= 1 && lane <= 30;
+
+    float4 e_p[G::LV], e_vx[G::LV], e_vz[G::LV];
+    if (ENERGY) {
+#pragma unroll
+        for (int u = 0; u < G::LV; ++u) e_p[u] = e_vx[u] = e_vz[u] = zero4();
+    }
 
     for (int k = 0; k < ns; ++k) {
         const int s = s0 + k;
         const int b = k & 1;
-        // every thread polls (bounded); the vote makes the give-up decision
-        // uniform so no thread is left waiting at a barrier
+        // every thread polls (bounded); the vote makes a give-up uniform, and
+        // also tells that every thread is done with shot k-1's buffer
         if (!__syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1))) {
             if (threadIdx.x == 0) {
                 atomicExch(A.err, -4);
@@ -113,11 +169,14 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
             }
             return;
         }
-        float *sP = stage[b];
+        if (threadIdx.x == 0 && k >= 1 && k + 1 < ns)   // refill shot k-1's buffer with shot k+1
+            stage_loads<R>(&mP, &mVX, &mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
+                           s + 1, G::P_FL, G::VX_FL);
+        float *sP = smem + b * G::STAGE_FL;
         float *sVX = sP + G::P_FL;
         float *sVZ = sVX + G::VX_FL;
 
-        if (FS) {
+        if (FS && !fast) {
             // vz[fs-1] = vz[fs]: rebuild the mirror row the previous step did not store
             const int rm = g.fs - 1 - (z0 - 2 * R);
             if (rm >= 0 && rm + 1 < G::ZR)
@@ -127,59 +186,60 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
 
         // ---------------- p-stage: whole sP rectangle, in place -------------
         {
-            const int rb = warp * G::LP;
-            const int rc = min(G::LP, G::PR - rb);
             float4 wz[G::LP + 2 * R - 1];
 #pragma unroll
             for (int t = 0; t < G::LP + 2 * R - 1; ++t)
                 wz[t] = (t < rc + 2 * R - 1) ? lds4(sVZ + (rb + t) * RW + 4 * lane) : zero4();
-            const int sz = A.src_z[s], sx = A.src_x[s];
+            const int2 src = s_src[k];
+            const int sz = src.x, sx = src.y;
 #pragma unroll
             for (int u = 0; u < G::LP; ++u) {
                 if (u < rc) {
                     const int r = rb + u;
                     const int gz = z0 - R + r;
-                    float e[12];
-                    {
-                        const float4 e0 = lds4(sVX + r * VXW + 4 * lane);
-                        const float4 e1 = lds4(sVX + r * VXW + 4 * lane + 4);
-                        const float4 e2 = lds4(sVX + r * VXW + 4 * lane + 8);
-                        e[0] = e0.x; e[1] = e0.y; e[2] = e0.z; e[3] = e0.w;
-                        e[4] = e1.x; e[5] = e1.y; e[6] = e1.z; e[7] = e1.w;
-                        e[8] = e2.x; e[9] = e2.y; e[10] = e2.z; e[11] = e2.w;
-                    }
                     float4 pv = lds4(sP + r * RW + 4 * lane);
-                    const bool row_in = gz >= g.p_r0 && gz <= g.p_r1;
-                    const bool unit_in = row_in && (gx0 + 3 >= g.p_c0) && (gx0 <= g.p_c1);
-                    if (unit_in) {
-                        const long long o = (long long)gz * g.pitch + gx0;
-                        const float4 a1 = ldg4(A.a1 + o);
-                        const float4 k1 = ldg4(A.k1 + o);
-                        float4 img;
+                    float D[4];
+                    const float4 a1 = lds4(sA1 + r * RW + 4 * lane);
+                    const bool tile_cell = IMG >= 1 && r >= R && r < R + TZ && vlane;
+                    if (fast) {
+                        divergence4<R>(sVX + r * VXW, lane, wz, u, g.c, D);
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            float D = 0.f;
+                        for (int q = 0; q < 4; ++q) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], at(pv, q));
+                        if (tile_cell)
+                            stg4(A.imaging + (long long)s * g.plane + (long long)gz * g.pitch + gx0,
+                                 make_float4(-D[0], -D[1], -D[2], -D[3]));
+                    } else {
+                        const bool row_in = gz >= g.p_r0 && gz <= g.p_r1;
+                        if (row_in && (gx0 + 3 >= g.p_c0) && (gx0 <= g.p_c1)) {
+                            divergence4<R>(sVX + r * VXW, lane, wz, u, g.c, D);
+                            const long long o = (long long)gz * g.pitch + gx0;
+                            const float4 k1 = ldg4(A.k1 + o);
+                            float4 img;
 #pragma unroll
-                            for (int kk = 0; kk < R; ++kk)
-                                D += g.c[kk] * (((e[q + 4 + kk] - e[q + 3 - kk]) + at(wz[u + R + kk], q)) -
-                                                at(wz[u + R - 1 - kk], q));
-                            const int gx = gx0 + q;
-                            const bool m = gx >= g.p_c0 && gx <= g.p_c1;
-                            at(img, q) = m ? -D : 0.f;
-                            if (m) at(pv, q) = (1.f - at(k1, q)) * at(pv, q) - at(a1, q) * D;
+                            for (int q = 0; q < 4; ++q) {
+                                const int gx = gx0 + q;
+                                const bool m = gx >= g.p_c0 && gx <= g.p_c1;
+                                at(img, q) = m ? -D[q] : 0.f;
+                                if (m) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], (1.f - at(k1, q)) * at(pv, q));
+                            }
+                            if (tile_cell) stg4(A.imaging + (long long)s * g.plane + o, img);
                         }
-                        if (IMG >= 1 && r >= R && r < R + TZ && lane >= 1 && lane <= 30)
-                            stg4(A.imaging + (long long)s * g.plane + o, img);
                     }
-                    if (gz == sz && sx >= gx0 && sx < gx0 + 4)
-                        at(pv, sx - gx0) += g.dt * A.wavelet[(long long)s * g.nt + A.it];
+                    if (gz == sz && sx >= gx0 && sx < gx0 + 4) {
+                        const float amp = g.dt * A.wavelet[(long long)s * g.nt + A.it];
+                        const int q = sx - gx0;
+                        if (q == 0) pv.x += amp;
+                        else if (q == 1) pv.y += amp;
+                        else if (q == 2) pv.z += amp;
+                        else pv.w += amp;
+                    }
                     sts4(sP + r * RW + 4 * lane, pv);
                 }
             }
         }
         __syncthreads();
 
-        if (FS) {
+        if (FS && !fast) {
             // p[fs-1] = -p[fs+1] inside the rectangle
             const int rm = g.fs - 1 - (z0 - R);
             if (rm >= 0 && rm + 2 < G::PR)
@@ -188,59 +248,56 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
         }
 
         // ---------------- v-stage: tile only -------------------------------
-        if (lane >= 1 && lane <= 30) {
-            const int vb = warp * G::LV;
-            const int vc = min(G::LV, TZ - vb);
+        if (vlane) {
             float4 wp[G::LV + 2 * R - 1];
 #pragma unroll
             for (int t = 0; t < G::LV + 2 * R - 1; ++t)
-                wp[t] = (t < vc + 2 * R - 1) ? lds4(sP + (vb + 1 + t) * RW + 4 * lane) : zero4();
+                wp[t] = (t < vcnt + 2 * R - 1) ? lds4(sP + (vb + 1 + t) * RW + 4 * lane) : zero4();
 #pragma unroll
             for (int u = 0; u < G::LV; ++u) {
-                if (u < vc) {
+                if (u < vcnt) {
                     const int rv = vb + u;          // tile row
                     const int rr = rv + R;          // sP / sVX row
                     const int gz = z0 + rv;
-                    if (gz < g.Nz && gx0 < g.Nx) {
-                        float f[12];
-                        {
-                            const float4 f0 = lds4(sP + rr * RW + 4 * lane - 4);
-                            const float4 f1 = lds4(sP + rr * RW + 4 * lane);
-                            const float4 f2 = lds4(sP + rr * RW + 4 * lane + 4);
-                            f[0] = f0.x; f[1] = f0.y; f[2] = f0.z; f[3] = f0.w;
-                            f[4] = f1.x; f[5] = f1.y; f[6] = f1.z; f[7] = f1.w;
-                            f[8] = f2.x; f[9] = f2.y; f[10] = f2.z; f[11] = f2.w;
-                        }
+                    if (fast || (gz < g.Nz && gx0 < g.Nx)) {
+                        float Dx[4], Dz[4];
+                        float4 pv;
+                        grad_x4<R>(sP + rr * RW, lane, g.c, Dx, pv);
+                        grad_z4<R>(wp, u, g.c, Dz);
                         float4 vx = lds4(sVX + rr * VXW + 4 * lane + 4);
                         float4 vz = lds4(sVZ + (rv + 2 * R) * RW + 4 * lane);
+                        const float4 a2 = lds4(sA2 + rv * RW + 4 * lane);
                         const long long o = (long long)gz * g.pitch + gx0;
-                        const bool vx_row = gz >= g.vx_r0 && gz <= g.vx_r1;
-                        const bool vz_row = gz >= g.vz_r0 && gz <= g.vz_r1;
-                        const bool need = (vx_row && gx0 + 3 >= g.vx_c0 && gx0 <= g.vx_c1) ||
-                                          (vz_row && gx0 + 3 >= g.vz_c0 && gx0 <= g.vz_c1);
                         float4 jx = zero4(), jz = zero4();
-                        if (need) {
-                            const float4 a2 = ldg4(A.a2 + o);
-                            const float4 k2 = ldg4(A.k2 + o);
-                            const float4 k3 = ldg4(A.k3 + o);
+                        if (fast) {
 #pragma unroll
                             for (int q = 0; q < 4; ++q) {
-                                const int gx = gx0 + q;
-                                if (vx_row && gx >= g.vx_c0 && gx <= g.vx_c1) {
-                                    float D = 0.f;
+                                at(vx, q) = __fmaf_rn(-at(a2, q), Dx[q], at(vx, q));
+                                at(vz, q) = __fmaf_rn(-at(a2, q), Dz[q], at(vz, q));
+                            }
+                            if (IMG == 2) {
+                                jx = make_float4(Dx[0], Dx[1], Dx[2], Dx[3]);
+                                jz = make_float4(Dz[0], Dz[1], Dz[2], Dz[3]);
+                            }
+                        } else {
+                            const bool vx_row = gz >= g.vx_r0 && gz <= g.vx_r1;
+                            const bool vz_row = gz >= g.vz_r0 && gz <= g.vz_r1;
+                            const bool need = (vx_row && gx0 + 3 >= g.vx_c0 && gx0 <= g.vx_c1) ||
+                                              (vz_row && gx0 + 3 >= g.vz_c0 && gx0 <= g.vz_c1);
+                            if (need) {
+                                const float4 k2 = ldg4(A.k2 + o);
+                                const float4 k3 = ldg4(A.k3 + o);
 #pragma unroll
-                                    for (int kk = 0; kk < R; ++kk)
-                                        D += g.c[kk] * (f[q + 5 + kk] - f[q + 4 - kk]);
-                                    at(vx, q) = (1.f - at(k2, q)) * at(vx, q) - at(a2, q) * D;
-                                    at(jx, q) = D;
-                                }
-                                if (vz_row && gx >= g.vz_c0 && gx <= g.vz_c1) {
-                                    float D = 0.f;
-#pragma unroll
-                                    for (int kk = 0; kk < R; ++kk)
-                                        D += g.c[kk] * (at(wp[u + R + kk], q) - at(wp[u + R - 1 - kk], q));
-                                    at(vz, q) = (1.f - at(k3, q)) * at(vz, q) - at(a2, q) * D;
-                                    at(jz, q) = D;
+                                for (int q = 0; q < 4; ++q) {
+                                    const int gx = gx0 + q;
+                                    if (vx_row && gx >= g.vx_c0 && gx <= g.vx_c1) {
+                                        at(vx, q) = __fmaf_rn(-at(a2, q), Dx[q], (1.f - at(k2, q)) * at(vx, q));
+                                        at(jx, q) = Dx[q];
+                                    }
+                                    if (vz_row && gx >= g.vz_c0 && gx <= g.vz_c1) {
+                                        at(vz, q) = __fmaf_rn(-at(a2, q), Dz[q], (1.f - at(k3, q)) * at(vz, q));
+                                        at(jz, q) = Dz[q];
+                                    }
                                 }
                             }
                         }
@@ -248,22 +305,22 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                             stg4(A.imaging + (long long)s * g.plane + A.img_field_stride + o, jx);
                             stg4(A.imaging + (long long)s * g.plane + 2 * A.img_field_stride + o, jz);
                         }
-                        const float4 pv = make_float4(f[4], f[5], f[6], f[7]);
                         float *outs = A.out + (long long)s * 3 * g.plane + o;
                         stg4(outs, pv);
                         stg4(outs + g.plane, vx);
                         stg4(outs + 2 * g.plane, vz);
-                        sts4(sVX + rr * VXW + 4 * lane + 4, vx);
-                        sts4(sVZ + (rv + 2 * R) * RW + 4 * lane, vz);
+                        if (has_rcv) {
+                            sts4(sVX + rr * VXW + 4 * lane + 4, vx);
+                            sts4(sVZ + (rv + 2 * R) * RW + 4 * lane, vz);
+                        }
                         if (ENERGY && gz >= g.pml && gz < g.pml + g.nz) {
-                            float *ea = eacc + rv * TX + 4 * (lane - 1);
 #pragma unroll
                             for (int q = 0; q < 4; ++q) {
                                 const int gx = gx0 + q;
                                 if (gx >= g.pml && gx < g.pml + g.nx) {
-                                    ea[q] += at(pv, q) * at(pv, q);
-                                    ea[TZ * TX + q] += at(vx, q) * at(vx, q);
-                                    ea[2 * TZ * TX + q] += at(vz, q) * at(vz, q);
+                                    at(e_p[u], q) += at(pv, q) * at(pv, q);
+                                    at(e_vx[u], q) += at(vx, q) * at(vx, q);
+                                    at(e_vz[u], q) += at(vz, q) * at(vz, q);
                                 }
                             }
                         }
@@ -271,12 +328,11 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                 }
             }
         }
-        __syncthreads();
 
         // ---------------- receivers of this tile ---------------------------
-        if (A.tr_p || A.tr_vx || A.tr_vz) {
-            const int e0 = A.rcv_ptr[tile], e1 = A.rcv_ptr[tile + 1];
-            for (int e = e0 + threadIdx.x; e < e1; e += NTHR) {
+        if (has_rcv) {
+            __syncthreads();
+            for (int e = rcv0 + threadIdx.x; e < rcv1; e += NTHR) {
                 const int4 en = A.rcv_ent[e];
                 const int rr = en.x + R, cc = en.y + 4;
                 const long long t = ((long long)s * g.nt + A.it) * g.n_rcv + en.z;
@@ -286,34 +342,51 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
             }
         }
         // order this iteration's generic-proxy shared-memory writes before the
-        // TMA that refills the buffer
+        // TMA that refills the buffer (issued after the next iteration's vote)
         fence_proxy_async_smem();
-        __syncthreads();
-        if (threadIdx.x == 0 && k + 2 < ns) {
-            stage_loads<R>(&mP, &mVX, &mVZ, stage[b], &bars[b], G::STAGE_BYTES, x0, z0, s + 2, G::P_FL,
-                           G::VX_FL);
-        }
     }
 
-    if (ENERGY) {
+    if (ENERGY && vlane) {
         // add this CTA's partial sums (over its shots) into the padded maps
-        for (int i = threadIdx.x; i < TZ * (TX / 4); i += NTHR) {
-            const int rv = i / (TX / 4), c4 = i % (TX / 4);
-            const int gz = z0 + rv, gx = x0 + 4 * c4;
-            if (gz < g.Nz && gx < g.Nx) {
-                const long long o = (long long)gz * g.pitch + gx;
 #pragma unroll
-                for (int f = 0; f < 3; ++f)
-                    red_add_v4(A.energy + f * g.plane + o, lds4(eacc + f * TZ * TX + rv * TX + 4 * c4));
+        for (int u = 0; u < G::LV; ++u) {
+            const int gz = z0 + vb + u;
+            if (u < vcnt && gz >= g.pml && gz < g.pml + g.nz && gx0 < g.Nx) {
+                const long long o = (long long)gz * g.pitch + gx0;
+                red_add_v4(A.energy + o, e_p[u]);
+                red_add_v4(A.energy + g.plane + o, e_vx[u]);
+                red_add_v4(A.energy + 2 * g.plane + o, e_vz[u]);
             }
         }
     }
 }
 
-template <int R, int TZ, bool ENERGY>
+template <int R, int TZ>
 constexpr size_t fwd_smem_bytes()
 {
-    return 2 * Geo<R, TZ>::STAGE_BYTES + 16 + (ENERGY ? 3 * TZ * TX * 4 : 0);
+    return StepSmem<R, TZ>::BYTES;
+}
+
+// Per tile: 1 if the tile's rectangles need no masks (tile_is_interior) and
+// see no damping (k1 on the p rectangle, k2 / k3 on the tile all zero).
+template <int R, int TZ>
+__global__ void tile_fast_kernel(const StepGeom g, const float *__restrict__ k1, const float *__restrict__ k2,
+                                 const float *__restrict__ k3, int *flags)
+{
+    const int tile = blockIdx.x;
+    const int z0 = (tile / g.tiles_x) * TZ, x0 = (tile % g.tiles_x) * TX;
+    bool ok = tile_is_interior<R, TZ>(g, z0, x0);
+    bool damped = false;
+    if (ok) {
+        for (int i = threadIdx.x; i < (TZ + 2 * R) * RW; i += blockDim.x) {
+            const int r = i / RW, c = i % RW;
+            const long long o = (long long)(z0 - R + r) * g.pitch + (x0 - 4 + c);
+            damped |= k1[o] != 0.f;
+            if (r >= R && r < R + TZ && c >= 4 && c < 4 + TX) damped |= (k2[o] != 0.f) || (k3[o] != 0.f);
+        }
+    }
+    damped = __syncthreads_or(damped);
+    if (threadIdx.x == 0) flags[tile] = (ok && !damped) ? 1 : 0;
 }
 
 }  // namespace gb

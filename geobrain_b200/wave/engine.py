@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import os
 from collections import OrderedDict
 from dataclasses import dataclass
 from typing import Optional, Sequence
@@ -92,6 +93,12 @@ class Plan:
     def checkpoint_bytes(self, checkpoint_every: int, fmt: str) -> int:
         return int(self._lib.gb_plan_checkpoint_bytes(self.h, int(checkpoint_every), _lib.CKPT_FORMATS[fmt]))
 
+    def imaging_bytes(self, cached_steps: int, with_rho: bool = False) -> int:
+        return int(self._lib.gb_plan_imaging_bytes(self.h, int(cached_steps), int(bool(with_rho))))
+
+    def set_group_streams(self, enable: bool) -> None:
+        _lib.check(self._lib.gb_plan_set_group_streams(self.h, int(enable)))
+
 
 def get_plan(geo: Geometry, src_x, src_z, rcv_x, rcv_z) -> Plan:
     sx, sz, rx, rz = _i64(src_x), _i64(src_z), _i64(rcv_x), _i64(rcv_z)
@@ -120,9 +127,14 @@ def stream_handle(device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
 
 
+def make_store(checkpoints: Optional[torch.Tensor], checkpoint_every: int, fmt: str,
+               imaging: Optional[torch.Tensor], cached_steps: int, with_rho: bool) -> "_lib.GradStore":
+    return _lib.GradStore(_lib.ptr(checkpoints), int(checkpoint_every), _lib.CKPT_FORMATS[fmt], _lib.ptr(imaging),
+                          int(cached_steps), int(bool(with_rho)))
+
+
 def run_forward(plan: Plan, vp: torch.Tensor, rho: torch.Tensor, damp: torch.Tensor, src_v: torch.Tensor, *,
-                want_energy: bool = True, snapshot_every: int = 0, checkpoints: Optional[torch.Tensor] = None,
-                checkpoint_every: int = 0, ckpt_format: str = "fp32"):
+                want_energy: bool = True, snapshot_every: int = 0, store: Optional["_lib.GradStore"] = None):
     """One gb_forward call.  Returns (p, vx, vz, energies or None, snapshots or None)."""
     g = plan.geo
     dev = vp.device
@@ -132,14 +144,14 @@ def run_forward(plan: Plan, vp: torch.Tensor, rho: torch.Tensor, damp: torch.Ten
     energies = [torch.empty((g.nz, g.nx), **f32) for _ in range(3)] if want_energy else None
     nsnap = (nt + snapshot_every - 1) // snapshot_every if snapshot_every > 0 else 0
     snaps = torch.empty((nsnap, g.nz, g.nx), **f32) if nsnap else None
-    ws = workspace(plan.workspace_bytes(False, checkpoint_every), dev)
+    ws = workspace(plan.workspace_bytes(False, 0), dev)
     L = plan._lib
     with torch.cuda.device(dev):
         rc = L.gb_forward(plan.h, vp.data_ptr(), rho.data_ptr(), damp.data_ptr(), src_v.data_ptr(),
                           *[t.data_ptr() for t in traces],
                           *([e.data_ptr() for e in energies] if energies else [None, None, None]),
-                          int(snapshot_every), _lib.ptr(snaps), _lib.ptr(checkpoints), int(checkpoint_every),
-                          _lib.CKPT_FORMATS[ckpt_format], ws.data_ptr(), ws.numel(), stream_handle(dev))
+                          int(snapshot_every), _lib.ptr(snaps), ctypes.byref(store) if store is not None else None,
+                          ws.data_ptr(), ws.numel(), stream_handle(dev))
     _lib.check(rc)
     return traces[0], traces[1], traces[2], energies, snaps
 
@@ -169,25 +181,40 @@ def choose_checkpoint_every(plan: Plan, checkpoint_segments: int = 1, checkpoint
     nt = plan.geo.nt
     if checkpoint_every > 0:
         return min(int(checkpoint_every), nt)
-    state = plan.checkpoint_bytes(1, fmt)                              # one stored state
-    img_step = plan.checkpoint_bytes(1, "fp32") / 3 * (3 if with_rho else 1)   # imaging fields of one step
+    state = plan.checkpoint_bytes(nt, fmt)                             # one stored state
+    img_step = plan.imaging_bytes(1, with_rho)                         # imaging fields of one step
     k = int(max(1, round(math.sqrt(nt * state / max(img_step, 1.0)))))
     k = min(k, max(1, -(-nt // max(1, checkpoint_segments))))
     return max(1, min(k, nt))
 
 
-def run_backward(plan: Plan, vp, rho, damp, src_v, res_p, res_vx, res_vz, checkpoints, checkpoint_every: int,
-                 fmt: str, want_rho: bool):
+def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device) -> int:
+    """How many of the last time steps keep their imaging fields from the
+    forward (those steps skip the recompute).  imaging_cache: 'auto' (up to
+    half of the device memory free right now), a byte budget, or 0."""
+    per = plan.imaging_bytes(1, with_rho)
+    if imaging_cache in (None, 0, False):
+        return 0
+    if imaging_cache == "auto":
+        free, _ = torch.cuda.mem_get_info(device)
+        budget = int(os.environ.get("GEOBRAIN_B200_IMAGING_CACHE_BYTES", free // 2))
+    else:
+        budget = int(imaging_cache)
+    return int(max(0, min(plan.geo.nt, budget // max(per, 1))))
+
+
+def run_backward(plan: Plan, vp, rho, damp, src_v, res_p, res_vx, res_vz, store: "_lib.GradStore",
+                 want_rho: bool):
     g = plan.geo
     dev = vp.device
     grad_vp = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32)
     grad_rho = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32) if want_rho else None
-    ws = workspace(plan.workspace_bytes(2 if want_rho else 1, checkpoint_every), dev)
+    ws = workspace(plan.workspace_bytes(2 if store.with_rho else 1, store.checkpoint_every), dev)
     with torch.cuda.device(dev):
         rc = plan._lib.gb_backward(plan.h, vp.data_ptr(), rho.data_ptr(), damp.data_ptr(), src_v.data_ptr(),
-                                   _lib.ptr(res_p), _lib.ptr(res_vx), _lib.ptr(res_vz), checkpoints.data_ptr(),
-                                   int(checkpoint_every), _lib.CKPT_FORMATS[fmt], grad_vp.data_ptr(),
-                                   _lib.ptr(grad_rho), ws.data_ptr(), ws.numel(), stream_handle(dev))
+                                   _lib.ptr(res_p), _lib.ptr(res_vx), _lib.ptr(res_vz), ctypes.byref(store),
+                                   grad_vp.data_ptr(), _lib.ptr(grad_rho), ws.data_ptr(), ws.numel(),
+                                   stream_handle(dev))
     _lib.check(rc)
     return grad_vp, grad_rho
 
@@ -196,30 +223,38 @@ class AcousticFunction(torch.autograd.Function):
     """Traces (p, vx, vz) as a differentiable function of (vp, rho).
 
     forward: gb_forward keeping checkpoints every K steps (fp32, or bf16 /
-    fp16 with per-snapshot scales); backward: gb_backward (recompute +
-    adjoint + imaging), in place of autograd through ~40 ops per step
+    fp16 with per-snapshot scales) and the imaging fields of the last
+    time steps that fit the cache budget; backward: gb_backward (adjoint with
+    the imaging condition, fp32 recompute of the uncached segments), in place
+    of autograd through ~40 ops per step
     (geobrain/physics/wave/kernels/acoustic_2d.py:448-460)."""
 
     @staticmethod
     def forward(ctx, vp, rho, plan, damp, src_v, opts):
+        dev = vp.device
         vp32 = vp.detach().to(torch.float32).contiguous()
         rho32 = rho.detach().to(torch.float32).contiguous()
-        K = opts["checkpoint_every"]
-        ckpt = torch.empty(plan.checkpoint_bytes(K, opts["fmt"]), dtype=torch.uint8, device=vp.device)
+        K, fmt, with_rho, cached = opts["checkpoint_every"], opts["fmt"], opts["with_rho"], opts["cached_steps"]
+        n_ck = -(-(plan.geo.nt - cached) // K)
+        ckpt = torch.empty(n_ck * plan.checkpoint_bytes(plan.geo.nt, fmt) if n_ck > 0 else 256,
+                           dtype=torch.uint8, device=dev)
+        img = torch.empty(max(plan.imaging_bytes(cached, with_rho), 256), dtype=torch.uint8, device=dev)
+        store = make_store(ckpt if n_ck > 0 else None, K, fmt, img if cached > 0 else None, cached, with_rho)
         p, vx, vz, en, snaps = run_forward(plan, vp32, rho32, damp, src_v, want_energy=opts["want_energy"],
-                                           snapshot_every=opts["snapshot_every"], checkpoints=ckpt,
-                                           checkpoint_every=K, ckpt_format=opts["fmt"])
+                                           snapshot_every=opts["snapshot_every"], store=store)
         ctx.plan, ctx.opts = plan, opts
-        ctx.save_for_backward(vp32, rho32, damp, src_v, ckpt)
+        ctx.store_keep = (ckpt, img)
+        ctx.store = store
+        ctx.save_for_backward(vp32, rho32, damp, src_v)
         if en is None:
-            en = [torch.zeros((plan.geo.nz, plan.geo.nx), device=vp.device) for _ in range(3)]
-        snaps = snaps if snaps is not None else torch.empty(0, device=vp.device)
+            en = [torch.zeros((plan.geo.nz, plan.geo.nx), device=dev) for _ in range(3)]
+        snaps = snaps if snaps is not None else torch.empty(0, device=dev)
         ctx.mark_non_differentiable(*en, snaps)
         return p, vx, vz, en[0], en[1], en[2], snaps
 
     @staticmethod
     def backward(ctx, gp, gvx, gvz, *unused):
-        vp32, rho32, damp, src_v, ckpt = ctx.saved_tensors
+        vp32, rho32, damp, src_v = ctx.saved_tensors
         need_vp, need_rho = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         if not (need_vp or need_rho):
             return None, None, None, None, None, None
@@ -227,14 +262,15 @@ class AcousticFunction(torch.autograd.Function):
         if all(r is None for r in res):
             z = torch.zeros_like(vp32)
             return (z if need_vp else None), (z.clone() if need_rho else None), None, None, None, None
-        gvp, grho = run_backward(ctx.plan, vp32, rho32, damp, src_v, *res, ckpt, ctx.opts["checkpoint_every"],
-                                 ctx.opts["fmt"], need_rho)
+        gvp, grho = run_backward(ctx.plan, vp32, rho32, damp, src_v, *res, ctx.store,
+                                 need_rho and bool(ctx.store.with_rho))
+        ctx.store_keep = None
         return (gvp if need_vp else None), (grho if need_rho else None), None, None, None, None
 
 
 def differentiable_forward(plan: Plan, vp, rho, damp, src_v, *, device, snapshot_every: int = 0,
                            checkpoint_segments: int = 1, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
-                           want_energy: bool = True) -> dict:
+                           want_energy: bool = True, imaging_cache="auto") -> dict:
     if snapshot_dtype not in _lib.CKPT_FORMATS:
         raise ValueError(f"snapshot_dtype must be one of {sorted(_lib.CKPT_FORMATS)}")
     need_rho = bool(getattr(rho, "requires_grad", False))
@@ -244,7 +280,9 @@ def differentiable_forward(plan: Plan, vp, rho, damp, src_v, *, device, snapshot
         if t.device != device:
             raise ValueError(f"{name} is on {t.device}, expected {device}")
     K = choose_checkpoint_every(plan, checkpoint_segments, checkpoint_every, snapshot_dtype, need_rho)
-    opts = dict(checkpoint_every=K, fmt=snapshot_dtype, want_energy=want_energy, snapshot_every=snapshot_every)
+    cached = choose_cached_steps(plan, imaging_cache, need_rho, device)
+    opts = dict(checkpoint_every=K, fmt=snapshot_dtype, want_energy=want_energy, snapshot_every=snapshot_every,
+                with_rho=need_rho, cached_steps=cached)
     p, vx, vz, e0, e1, e2, snaps = AcousticFunction.apply(vp_t, rho_t, plan, damp, src_v, opts)
     out = {"p": p, "vx": vx, "vz": vz, "forward_wavefield_p": e0, "forward_wavefield_vx": e1,
            "forward_wavefield_vz": e2}

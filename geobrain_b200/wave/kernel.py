@@ -10,8 +10,9 @@ adjoint (engine.AcousticFunction); the energy maps are detached, as in the
 reference.
 
 Additions, all keyword-only with defaults that keep the reference's
-behaviour: fd_order (4 or 8), checkpoint_every / snapshot_dtype (gradient
-memory), want_energy (skip the energy sums).
+behaviour: fd_order (4 or 8); checkpoint_every, snapshot_dtype ('fp32',
+'bf16', 'fp16') and imaging_cache ('auto', a byte budget, or 0) for the
+gradient's memory; want_energy (skip the energy sums).
 """
 from __future__ import annotations
 
@@ -44,7 +45,7 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
                             checkpoint_segments: int = 1, device: torch.device = torch.device("cpu"),
                             dtype: torch.dtype = torch.float32, snapshot_every: int = 0, *,
                             fd_order: int = 4, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
-                            want_energy: bool = True):
+                            want_energy: bool = True, imaging_cache="auto"):
     device = torch.device(device)
     if device.type != "cuda":
         raise ValueError(f"geobrain_b200 runs on CUDA devices only (device={device})")
@@ -86,7 +87,8 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
                                              snapshot_every=int(snapshot_every),
                                              checkpoint_segments=int(checkpoint_segments),
                                              checkpoint_every=int(checkpoint_every),
-                                             snapshot_dtype=snapshot_dtype, want_energy=want_energy)
+                                             snapshot_dtype=snapshot_dtype, want_energy=want_energy,
+                                             imaging_cache=imaging_cache)
     vp_t = _as_f32(vp.detach() if torch.is_tensor(vp) else vp, device, "vp")
     rho_t = _as_f32(rho.detach() if torch.is_tensor(rho) else rho, device, "rho")
     p, vx, vz, en, snaps = engine.run_forward(plan, vp_t, rho_t, damp_t, w, want_energy=want_energy,

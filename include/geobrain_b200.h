@@ -52,6 +52,25 @@ typedef struct gb_model_desc {
 #define GB_CKPT_BF16  1   /* bf16 with one fp32 scale per (checkpoint, shot, field) */
 #define GB_CKPT_F16   2   /* fp16 with one fp32 scale per (checkpoint, shot, field) */
 
+/* What the forward keeps for a later gb_backward (replaces the
+ * torch.utils.checkpoint segments of acoustic_2d.py:430,448-460):
+ *   checkpoints       full state every checkpoint_every steps, in `format`,
+ *                     gb_plan_checkpoint_bytes(plan, checkpoint_every, format)
+ *                     bytes (may be NULL when cached_steps == nt);
+ *   imaging           the fp32 imaging fields of the last cached_steps time
+ *                     steps, gb_plan_imaging_bytes(plan, cached_steps,
+ *                     with_rho) bytes (may be NULL when cached_steps == 0);
+ *                     those steps need no recompute in the backward;
+ *   with_rho          keep / compute the fields the density gradient needs. */
+typedef struct gb_grad_store {
+    void *checkpoints;
+    int32_t checkpoint_every;
+    int32_t format;
+    void *imaging;
+    int32_t cached_steps;
+    int32_t with_rho;
+} gb_grad_store;
+
 typedef struct gb_plan gb_plan;   /* opaque */
 
 /* Build a plan for one model: validates sizes and positions (host arrays of
@@ -68,6 +87,11 @@ void gb_plan_destroy(gb_plan *plan);
  * default.  Used by the autotuner. */
 int gb_plan_set_tiling(gb_plan *plan, int tile_rows, int shots_per_cta);
 
+/* Run each group of shots on its own stream (forked from and joined back to
+ * the caller's stream; on by default).  Groups never interact, so their
+ * kernels fill each other's tails. */
+int gb_plan_set_group_streams(gb_plan *plan, int enable);
+
 /* Bytes of device workspace gb_forward / gb_backward need.  with_gradient:
  * 0 forward only; 1 adds the adjoint state, the imaging buffer of one
  * checkpoint segment and the velocity-gradient sums; 2 also the density
@@ -77,6 +101,9 @@ size_t gb_plan_workspace_bytes(const gb_plan *plan, int with_gradient, int check
 /* Bytes of checkpoint storage for a given segment length and format. */
 size_t gb_plan_checkpoint_bytes(const gb_plan *plan, int checkpoint_every, int ckpt_format);
 
+/* Bytes of the imaging cache for the last cached_steps time steps. */
+size_t gb_plan_imaging_bytes(const gb_plan *plan, int cached_steps, int with_rho);
+
 /* Forward modelling, all nt steps, on `stream` (acoustic_forward_kernel,
  * acoustic_2d.py:294-501).  Device pointers:
  *   vp, rho   (nz, nx) float32       damp (Nz, Nx) float32
@@ -85,30 +112,30 @@ size_t gb_plan_checkpoint_bytes(const gb_plan *plan, int checkpoint_every, int c
  *   energy_p / energy_vx / energy_vz (nz, nx) float32, NULL skips the energy sums
  *   snapshots ((nt + snapshot_every - 1) / snapshot_every, nz, nx) float32,
  *             pressure of shot 0 at the end of each snapshot chunk, or NULL
- *   checkpoints: NULL, or storage of gb_plan_checkpoint_bytes(checkpoint_every,
- *             ckpt_format) that receives the states gb_backward restarts from.
+ *   store     NULL for plain modelling, or what to keep for gb_backward.
  */
 int gb_forward(gb_plan *plan, const float *vp, const float *rho, const float *damp,
                const float *wavelet,
                float *trace_p, float *trace_vx, float *trace_vz,
                float *energy_p, float *energy_vx, float *energy_vz,
-               int32_t snapshot_every, float *snapshots,
-               void *checkpoints, int32_t checkpoint_every, int32_t ckpt_format,
+               int32_t snapshot_every, float *snapshots, const gb_grad_store *store,
                void *workspace, size_t workspace_bytes, void *stream);
 
 /* Gradient of a loss L with respect to vp and rho, given the adjoint sources
  * res_* = dL/d(trace_*) (n_shots, nt, n_rcv) float32 (any may be NULL), and
- * the checkpoints a gb_forward call with the same plan, model and
- * checkpoint_every wrote.  Recomputes each segment forward in fp32 from its
- * checkpoint, runs the hand-written adjoint backwards through it with the
- * zero-lag imaging condition fused in, sums over shots and time with
- * compensated fp32 summation and folds the padding back into the edge cells
- * (the adjoint of pad_model).  grad_vp / grad_rho are (nz, nx) float32 and
- * are overwritten; grad_rho may be NULL. */
+ * the store a gb_forward call with the same plan and model filled.  Runs the
+ * hand-written adjoint backwards in time with the zero-lag imaging condition
+ * fused in: over the cached steps first, then one checkpoint segment at a
+ * time after an fp32 recompute of that segment from its checkpoint.  Sums
+ * over shots and time with compensated fp32 summation and folds the padding
+ * back into the edge cells (the adjoint of pad_model).  grad_vp / grad_rho
+ * are (nz, nx) float32 and are overwritten; grad_rho may be NULL (it needs a
+ * store made with with_rho).  Workspace: gb_plan_workspace_bytes(plan,
+ * with_rho ? 2 : 1, checkpoint_every). */
 int gb_backward(gb_plan *plan, const float *vp, const float *rho, const float *damp,
                 const float *wavelet,
                 const float *res_p, const float *res_vx, const float *res_vz,
-                const void *checkpoints, int32_t checkpoint_every, int32_t ckpt_format,
+                const gb_grad_store *store,
                 float *grad_vp, float *grad_rho,
                 void *workspace, size_t workspace_bytes, void *stream);
 

@@ -31,7 +31,7 @@ def cuda_grad(c, device, fd_order=4, lin=None, want_rho=True, **kw):
                for k in ("p", "vx", "vz") if lin.get(k) is not None)
     loss.backward()
     torch.cuda.synchronize()
-    return vp.grad.cpu().numpy(), (rho.grad.cpu().numpy() if want_rho else None), float(loss)
+    return vp.grad.cpu().numpy(), (rho.grad.cpu().numpy() if want_rho else None), float(loss.detach())
 
 
 @pytest.mark.parametrize("name", ["small_nofs", "small_fs"])
@@ -52,14 +52,55 @@ def test_eighth_order_gradient_matches_oracle(cuda_device, name):
     assert orc.rel_l2(grho, rrho) < GTOL
 
 
-def test_segment_length_does_not_change_gradient(cuda_device):
-    """fp32 checkpoints restart the recompute bit for bit, so any segment
-    length gives the identical gradient."""
+@pytest.mark.parametrize("imaging_cache", [0, "auto", "partial"])
+def test_segment_length_and_cache_do_not_change_gradient(cuda_device, imaging_cache):
+    """fp32 checkpoints restart the recompute bit for bit, and cached imaging
+    fields are the same numbers the recompute writes, so every segment length
+    and cache size gives the identical gradient."""
     c = load_case("small_nofs")
-    base, _, _ = cuda_grad(c, cuda_device, fd_order=8, want_rho=False, checkpoint_every=c["nt"])
+    base, _, _ = cuda_grad(c, cuda_device, fd_order=8, want_rho=False, checkpoint_every=c["nt"], imaging_cache=0)
+    if imaging_cache == "partial":
+        from geobrain_b200.wave import engine
+        geo = engine.Geometry(c["nz"], c["nx"], c["nabc"], c["nt"], c["dt"], c["dx"], 4, False)
+        plan = engine.get_plan(geo, c["src_x"], c["src_z"], c["rcv_x"], c["rcv_z"])
+        imaging_cache = plan.imaging_bytes(c["nt"] // 3 + 5, False)      # a third of the steps, off-segment
     for k in (1, 7, 64):
-        g, _, _ = cuda_grad(c, cuda_device, fd_order=8, want_rho=False, checkpoint_every=k)
+        g, _, _ = cuda_grad(c, cuda_device, fd_order=8, want_rho=False, checkpoint_every=k,
+                            imaging_cache=imaging_cache)
         np.testing.assert_array_equal(g, base)
+
+
+def test_group_streams_do_not_change_results(cuda_device):
+    from geobrain_b200.wave import engine
+    c = load_case("small_fs")
+    geo = engine.Geometry(c["nz"], c["nx"], c["nabc"], c["nt"], c["dt"], c["dx"], 2, True)
+    plan = engine.get_plan(geo, c["src_x"], c["src_z"], c["rcv_x"], c["rcv_z"])
+    plan.set_tiling(16, 1)                 # three groups of one shot
+    try:
+        a = cuda_grad(c, cuda_device, imaging_cache=0, checkpoint_every=50)
+        plan.set_group_streams(False)
+        b = cuda_grad(c, cuda_device, imaging_cache=0, checkpoint_every=50)
+    finally:
+        plan.set_group_streams(True)
+        plan.set_tiling(16, 0)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert a[2] == b[2]
+
+
+@pytest.mark.parametrize("fmt,tol", [("fp16", 1e-3), ("bf16", 1e-2)])
+def test_16bit_checkpoints_within_budget(cuda_device, fmt, tol):
+    """Snapshots stored in 16 bits with a per-snapshot scale; the recompute
+    from them runs in fp32, so the only error is each segment restarting from
+    a rounded state (12 restarts here, the harshest case).  fp16 keeps 11
+    significant bits (about 6e-4 here), bf16 8 bits (about 8x more)."""
+    c = load_case("small_nofs")
+    g, _, _ = cuda_grad(c, cuda_device, fd_order=8, want_rho=False, checkpoint_every=20, imaging_cache=0,
+                        snapshot_dtype=fmt)
+    rvp, _, _ = orc.gradient(**oracle_kwargs(c), res_p=c["lin_p"], res_vx=c["lin_vx"], res_vz=c["lin_vz"],
+                             half=4, dtype=np.float64)
+    err = orc.rel_l2(g, rvp)
+    assert err < tol, err
 
 
 def test_velocity_only_gradient_matches_full(cuda_device):
