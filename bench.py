@@ -285,9 +285,11 @@ def main():
     # roofline of the kernels, from the CUDA-event phase timings of the timed region
     peak, peak_kind = measured_peaks()
     nt, cells = w.nt, w.cells
-    per_step_fwd = prof["forward_ms"] / args.steps / nt          # ms per forward launch (fwd + energy)
-    per_step_rec = prof["recompute_ms"] / args.steps / nt        # ms per recompute launch (fwd + imaging)
-    per_step_adj = prof["adjoint_ms"] / args.steps / nt          # ms per adjoint launch
+    # ms per time step of each phase (all shot groups of a step together)
+    per_step_fwd = prof["forward_ms"] / max(prof["forward_steps"], 1)
+    per_step_rec = prof["recompute_ms"] / max(prof["recompute_steps"], 1)
+    per_step_adj = prof["adjoint_ms"] / max(prof["adjoint_steps"], 1)
+    cached_frac = 1.0 - prof["recompute_steps"] / max(prof["adjoint_steps"], 1)
     b_fwd = S * cells * (24 + 8 / S)                              # fields r+w, a1 / a2 shared by the shots
     b_rec = S * cells * (24 + 4 + 8 / S)                          # + imaging field written
     b_adj = S * cells * (24 + 4 + 16 / S)                         # + imaging read, coefficients, gradient sums
@@ -301,11 +303,12 @@ def main():
         v["frac"] = v["achieved_gbs"] / peak
     # dominant kernel by share of the timed region; fwd_step runs twice per
     # gradient (forward pass and recompute), adj_step once
-    t_fwd = (per_step_fwd + per_step_rec) * nt
-    t_adj = per_step_adj * nt
+    t_fwd = prof["forward_ms"] + prof["recompute_ms"]
+    t_adj = prof["adjoint_ms"]
     if t_fwd >= t_adj:
         tname = "fwd_step"
-        achieved = (b_fwd + b_rec) / ((per_step_fwd + per_step_rec) * 1e-3) / 1e9
+        n_f, n_r = prof["forward_steps"], prof["recompute_steps"]
+        achieved = (b_fwd * n_f + b_rec * n_r) / (t_fwd * 1e-3) / 1e9
     else:
         tname = "adj_step"
         achieved = b_adj / (per_step_adj * 1e-3) / 1e9
@@ -313,7 +316,7 @@ def main():
                 "frac": achieved / peak,
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
-                "share_of_step": max(t_fwd, t_adj) / ms_step, "traffic": ncu_traffic(tname)}
+                "share_of_step": max(t_fwd, t_adj) / args.steps / ms_step, "traffic": ncu_traffic(tname)}
     grad_bytes = units / world * (56 + 16 / S)
     grad_roof = {"algorithmic_bytes_per_unit": 56 + 16 / S,
                  "achieved": grad_bytes / (ms_step * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
@@ -338,6 +341,7 @@ def main():
         "gradient_roofline": grad_roof,
         "kernels": kern,
         "phase_ms_per_step": {k: prof[k] / args.steps for k in ("forward_ms", "recompute_ms", "adjoint_ms")},
+        "imaging_cache_fraction": cached_frac,
         "gpu_launches": int(prof["launches"]),
         "clocks": clocks,
         "cpu_baseline": cpu,

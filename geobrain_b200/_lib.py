@@ -61,7 +61,8 @@ SIGNATURES = {
     "gb_workspace_status": (ctypes.c_int, [_P, _P]),
     "gb_plan_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_plan_profile": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
-                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]),
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                       ctypes.POINTER(ctypes.c_longlong)]),
     "gb_static_scratch_bytes": (_SZ, []),
     "gb_forward_static_scratch": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P]),
     "gb_last_error": (ctypes.c_char_p, []),

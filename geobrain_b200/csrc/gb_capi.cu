@@ -123,6 +123,7 @@ struct gb_plan {
     bool prof = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[3];   // forward, recompute, adjoint
     long long launches = 0;
+    long long phase_steps[3] = {0, 0, 0};                     // time steps run per phase
 
     ~gb_plan()
     {
@@ -731,6 +732,7 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
     if (int rc = fork(gs)) return rc;
     const size_t step_img = (size_t)n_img * S * P->plane;
     int snap_i = 0;
+    P->phase_steps[0] += d.nt;
     for (int it = 0; it < d.nt; ++it) {
         const int b = it & 1;
         A.it = it;
@@ -850,6 +852,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     // adjoint sweep over [t0, t1) in reverse, imaging fields at img_base[(it - t0)]
     auto adjoint_sweep = [&](int t0, int t1, const float *img_base) -> int {
         P->mark(2, true, st);
+        P->phase_steps[2] += t1 - t0;
         if (int rc = fork(gs)) return rc;
         for (int it = t1 - 1; it >= t0; --it) {
             A.it = it;
@@ -876,6 +879,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     for (int seg = n_seg - 1; seg >= 0; --seg) {
         const int t0 = seg * K, t1 = std::min(t_cache, t0 + K);
         P->mark(1, true, st);
+        P->phase_steps[1] += t1 - t0;
         if (int rc = fork(gs)) return rc;
         for (int i = 0; i < gs.n; ++i) {
             int g0, gc;
@@ -926,10 +930,12 @@ int gb_plan_set_profiling(gb_plan *P, int enable)
     P->prof = enable != 0;
     P->clear_events();
     P->launches = 0;
+    for (auto &n : P->phase_steps) n = 0;
     return GB_OK;
 }
 
-int gb_plan_profile(gb_plan *P, double *ms_forward, double *ms_recompute, double *ms_adjoint, long long *launches)
+int gb_plan_profile(gb_plan *P, double *ms_forward, double *ms_recompute, double *ms_adjoint, long long *launches,
+                    long long *phase_steps)
 {
     if (!P) return fail(GB_E_ARG, "null plan");
     double *outs[3] = {ms_forward, ms_recompute, ms_adjoint};
@@ -944,8 +950,11 @@ int gb_plan_profile(gb_plan *P, double *ms_forward, double *ms_recompute, double
         if (outs[ph]) *outs[ph] = sum;
     }
     if (launches) *launches = P->launches;
+    if (phase_steps)
+        for (int ph = 0; ph < 3; ++ph) phase_steps[ph] = P->phase_steps[ph];
     P->clear_events();
     P->launches = 0;
+    for (auto &n : P->phase_steps) n = 0;
     return GB_OK;
 }
 

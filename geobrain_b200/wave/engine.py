@@ -83,9 +83,11 @@ class Plan:
         launches since the last call (needs set_profiling(True))."""
         f, r, a = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
         n = ctypes.c_longlong()
+        steps = (ctypes.c_longlong * 3)()
         _lib.check(self._lib.gb_plan_profile(self.h, ctypes.byref(f), ctypes.byref(r), ctypes.byref(a),
-                                             ctypes.byref(n)))
-        return {"forward_ms": f.value, "recompute_ms": r.value, "adjoint_ms": a.value, "launches": n.value}
+                                             ctypes.byref(n), steps))
+        return {"forward_ms": f.value, "recompute_ms": r.value, "adjoint_ms": a.value, "launches": n.value,
+                "forward_steps": steps[0], "recompute_steps": steps[1], "adjoint_steps": steps[2]}
 
     def workspace_bytes(self, with_gradient: bool = False, checkpoint_every: int = 0) -> int:
         return int(self._lib.gb_plan_workspace_bytes(self.h, int(with_gradient), int(checkpoint_every)))
@@ -191,13 +193,17 @@ def choose_checkpoint_every(plan: Plan, checkpoint_segments: int = 1, checkpoint
 def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device) -> int:
     """How many of the last time steps keep their imaging fields from the
     forward (those steps skip the recompute).  imaging_cache: 'auto' (up to
-    half of the device memory free right now), a byte budget, or 0."""
+    60 % of the device memory available right now, counting blocks the
+    caching allocator holds unused; GEOBRAIN_B200_IMAGING_CACHE_BYTES
+    overrides), a byte budget, or 0."""
     per = plan.imaging_bytes(1, with_rho)
     if imaging_cache in (None, 0, False):
         return 0
     if imaging_cache == "auto":
         free, _ = torch.cuda.mem_get_info(device)
-        budget = int(os.environ.get("GEOBRAIN_B200_IMAGING_CACHE_BYTES", free // 2))
+        # blocks torch's allocator holds but does not use are free for this too
+        avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+        budget = int(os.environ.get("GEOBRAIN_B200_IMAGING_CACHE_BYTES", int(avail * 0.6)))
     else:
         budget = int(imaging_cache)
     return int(max(0, min(plan.geo.nt, budget // max(per, 1))))

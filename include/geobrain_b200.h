@@ -141,13 +141,14 @@ int gb_backward(gb_plan *plan, const float *vp, const float *rho, const float *d
 
 /* Profiling (used by the benchmark): when enabled, gb_forward and
  * gb_backward record CUDA events on their stream around the forward loop,
- * each segment's fp32 recompute and each segment's adjoint sweep, and count
- * their kernel launches.  gb_plan_profile waits for those events, returns
- * the summed milliseconds per phase and the launch count since the last
+ * each segment's fp32 recompute and each adjoint sweep, and count their
+ * kernel launches and time steps.  gb_plan_profile waits for those events,
+ * returns the summed milliseconds per phase, the launch count and the time
+ * steps per phase (forward, recompute, adjoint; array of 3) since the last
  * call, and resets them.  Any output pointer may be NULL. */
 int gb_plan_set_profiling(gb_plan *plan, int enable);
 int gb_plan_profile(gb_plan *plan, double *ms_forward, double *ms_recompute, double *ms_adjoint,
-                    long long *launches);
+                    long long *launches, long long *phase_steps);
 
 /* Synchronises `stream` and reports the device-side status word of a
  * workspace after gb_forward / gb_backward: GB_OK, or GB_E_TIMEOUT if a
