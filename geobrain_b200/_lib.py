@@ -65,6 +65,9 @@ SIGNATURES = {
                                        ctypes.POINTER(ctypes.c_longlong)]),
     "gb_static_scratch_bytes": (_SZ, []),
     "gb_forward_static_scratch": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P]),
+    "gb_batch_workspace_bytes": (_SZ, [_P, ctypes.c_int]),
+    "gb_batch_forward": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _SZ, _P]),
+    "gb_batch_backward": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _SZ, _P]),
     "gb_last_error": (ctypes.c_char_p, []),
     "gb_version": (ctypes.c_char_p, []),
 }

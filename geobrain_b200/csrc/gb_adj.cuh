@@ -54,10 +54,9 @@ __device__ __forceinline__ void neumaier_add(float &s, float &c, float x)
 }
 
 template <int R, int TZ, bool FS, bool RHO>
-__global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
-adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mVX,
-                const __grid_constant__ CUtensorMap mVZ, const __grid_constant__ CUtensorMap mA1,
-                const __grid_constant__ CUtensorMap mA2, const AdjArgs A)
+__device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMap *mVX, const CUtensorMap *mVZ,
+                                         const CUtensorMap *mA1, const CUtensorMap *mA2, const AdjArgs &A,
+                                         const int group, const int tile)
 {
     using G = Geo<R, TZ>;
     using SM = StepSmem<R, TZ>;
@@ -67,10 +66,6 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
     float *sA2 = sA1 + SM::A1_FL;
     uint64_t *bars = reinterpret_cast<uint64_t *>(sA1 + SM::COEF_FL);
 
-    // launch covers shot groups [grp0, grp0 + grp_count): one launch for all
-    // groups, or one launch per group when groups run on their own streams
-    const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
-    const int tile = (int)(blockIdx.x / A.grp_count);
     const int z0 = (tile / g.tiles_x) * TZ;
     const int x0 = (tile % g.tiles_x) * TX;
     const int s0 = group * g.shots_per_cta;
@@ -89,10 +84,10 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bars[2], SM::COEF_BYTES);
-        tma_load_2d(sA1, &mA1, &bars[2], x0 - 4, z0 - R);
-        tma_load_2d(sA2, &mA2, &bars[2], x0 - 4, z0);
+        tma_load_2d(sA1, mA1, &bars[2], x0 - 4, z0 - R);
+        tma_load_2d(sA2, mA2, &bars[2], x0 - 4, z0);
         for (int k = 0; k < 2 && k < ns; ++k)
-            stage_loads<R>(&mP, &mVX, &mVZ, smem + k * G::STAGE_FL, &bars[k], G::STAGE_BYTES, x0, z0, s0 + k,
+            stage_loads<R>(mP, mVX, mVZ, smem + k * G::STAGE_FL, &bars[k], G::STAGE_BYTES, x0, z0, s0 + k,
                            G::P_FL, G::VX_FL);
     }
     if (!__syncthreads_and(mbar_wait_bounded(&bars[2], 0))) {
@@ -140,7 +135,7 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
             return;
         }
         if (threadIdx.x == 0 && k >= 1 && k + 1 < ns)   // refill shot k-1's buffer with shot k+1
-            stage_loads<R>(&mP, &mVX, &mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
+            stage_loads<R>(mP, mVX, mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
                            s + 1, G::P_FL, G::VX_FL);
         float *sP = smem + b * G::STAGE_FL;
         float *sVX = sP + G::P_FL;
@@ -200,7 +195,7 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                                     // share of the mirror row p[fs-1] = -p[fs+1]
                                     float M = 0.f;
 #pragma unroll
-                                    for (int kk = 0; kk < R; ++kk) M += g.c[kk] * at(wz[u + R - 2 + kk], q);
+                                    for (int kk = 0; kk < R; ++kk) M = __fmaf_rn(g.c[kk], at(wz[u + R - 2 + kk], q), M);
                                     d -= M;
                                 }
                                 const int gx = gx0 + q;
@@ -243,14 +238,14 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                             for (int q = 0; q < 4; ++q) {
                                 at(vx, q) = __fmaf_rn(at(a2, q), Dx[q], at(vx1, q));
                                 at(vz, q) = __fmaf_rn(at(a2, q), Dz[q], at(vz1, q));
-                                at(acc1[u], q) += at(mp1, q) * at(im[u], q);
+                                at(acc1[u], q) = __fmaf_rn(at(mp1, q), at(im[u], q), at(acc1[u], q));
                             }
                             pp = mp1;
                             if (RHO) {
 #pragma unroll
                                 for (int q = 0; q < 4; ++q) {
-                                    at(acc2[u], q) += at(vx1, q) * at(jx[u], q);
-                                    at(acc2[u], q) += at(vz1, q) * at(jz[u], q);
+                                    at(acc2[u], q) = __fmaf_rn(at(vx1, q), at(jx[u], q), at(acc2[u], q));
+                                    at(acc2[u], q) = __fmaf_rn(at(vz1, q), at(jz[u], q), at(acc2[u], q));
                                 }
                             }
                         } else {
@@ -269,17 +264,17 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                                     const int gx = gx0 + q;
                                     if (vx_row && gx >= g.vx_c0 && gx <= g.vx_c1) {
                                         at(vx, q) = __fmaf_rn(at(a2, q), Dx[q], (1.f - at(k2, q)) * at(vx1, q));
-                                        if (RHO) at(acc2[u], q) += at(vx1, q) * at(jx[u], q);
+                                        if (RHO) at(acc2[u], q) = __fmaf_rn(at(vx1, q), at(jx[u], q), at(acc2[u], q));
                                     }
                                     if (vz_row && gx >= g.vz_c0 && gx <= g.vz_c1) {
                                         float d = Dz[q];
                                         if (FS && gz == g.fs) {
                                             // the p update reads vz[fs-1] as vz[fs]
 #pragma unroll
-                                            for (int kk = 0; kk < R; ++kk) d += g.c[kk] * at(wp[u + R - 1 + kk], q);
+                                            for (int kk = 0; kk < R; ++kk) d = __fmaf_rn(g.c[kk], at(wp[u + R - 1 + kk], q), d);
                                         }
                                         at(vz, q) = __fmaf_rn(at(a2, q), d, (1.f - at(k3, q)) * at(vz1, q));
-                                        if (RHO) at(acc2[u], q) += at(vz1, q) * at(jz[u], q);
+                                        if (RHO) at(acc2[u], q) = __fmaf_rn(at(vz1, q), at(jz[u], q), at(acc2[u], q));
                                     }
                                 }
                             }
@@ -290,7 +285,7 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                                     const int gx = gx0 + q;
                                     if (gx >= g.p_c0 && gx <= g.p_c1) {
                                         at(pp, q) = (1.f - at(k1, q)) * at(mp1, q);
-                                        at(acc1[u], q) += at(mp1, q) * at(im[u], q);
+                                        at(acc1[u], q) = __fmaf_rn(at(mp1, q), at(im[u], q), at(acc1[u], q));
                                     }
                                 }
                             }
@@ -330,6 +325,17 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
             }
         }
     }
+}
+
+template <int R, int TZ, bool FS, bool RHO>
+__global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
+adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mVX,
+                const __grid_constant__ CUtensorMap mVZ, const __grid_constant__ CUtensorMap mA1,
+                const __grid_constant__ CUtensorMap mA2, const AdjArgs A)
+{
+    const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
+    const int tile = (int)(blockIdx.x / A.grp_count);
+    adj_body<R, TZ, FS, RHO>(&mP, &mVX, &mVZ, &mA1, &mA2, A, group, tile);
 }
 
 template <int R, int TZ>

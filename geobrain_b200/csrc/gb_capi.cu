@@ -4,6 +4,7 @@
 
 #include "gb_adj.cuh"
 #include "gb_aux.cuh"
+#include "gb_batch.cuh"
 #include "gb_fwd.cuh"
 
 #include <cudaTypedefs.h>
@@ -955,6 +956,391 @@ int gb_plan_profile(gb_plan *P, double *ms_forward, double *ms_recompute, double
     P->clear_events();
     P->launches = 0;
     for (auto &n : P->phase_steps) n = 0;
+    return GB_OK;
+}
+
+}  // extern "C"
+
+
+// ---------------------------------------------------------------------------
+// Batches of models: one launch per time step for all of them.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <int R, bool FS, bool EN, int IMG>
+void *fwd_batch_fn()
+{
+    return reinterpret_cast<void *>(&fwd_batch_kernel<R, 16, FS, EN, IMG>);
+}
+
+template <int R, bool FS>
+void *fwd_batch_pick(bool en, int img)
+{
+    if (img == 1) return en ? fwd_batch_fn<R, FS, true, 1>() : fwd_batch_fn<R, FS, false, 1>();
+    if (img == 2) return en ? fwd_batch_fn<R, FS, true, 2>() : fwd_batch_fn<R, FS, false, 2>();
+    return en ? fwd_batch_fn<R, FS, true, 0>() : fwd_batch_fn<R, FS, false, 0>();
+}
+
+StepKernel fwd_batch_kernel_for(int R, bool fs, bool en, int img)
+{
+    StepKernel k{nullptr, 0};
+    if (R == 2) {
+        k.fn = fs ? fwd_batch_pick<2, true>(en, img) : fwd_batch_pick<2, false>(en, img);
+        k.smem = fwd_smem_bytes<2, 16>();
+    } else if (R == 4) {
+        k.fn = fs ? fwd_batch_pick<4, true>(en, img) : fwd_batch_pick<4, false>(en, img);
+        k.smem = fwd_smem_bytes<4, 16>();
+    }
+    return k;
+}
+
+StepKernel adj_batch_kernel_for(int R, bool fs, bool rho)
+{
+    StepKernel k{nullptr, 0};
+    if (R == 2) {
+        k.fn = fs ? (rho ? (void *)&adj_batch_kernel<2, 16, true, true> : (void *)&adj_batch_kernel<2, 16, true, false>)
+                  : (rho ? (void *)&adj_batch_kernel<2, 16, false, true> : (void *)&adj_batch_kernel<2, 16, false, false>);
+        k.smem = adj_smem_bytes<2, 16>();
+    } else if (R == 4) {
+        k.fn = fs ? (rho ? (void *)&adj_batch_kernel<4, 16, true, true> : (void *)&adj_batch_kernel<4, 16, true, false>)
+                  : (rho ? (void *)&adj_batch_kernel<4, 16, false, true> : (void *)&adj_batch_kernel<4, 16, false, false>);
+        k.smem = adj_smem_bytes<4, 16>();
+    }
+    return k;
+}
+
+struct BatchLayout {
+    size_t models, maps, items, total;
+    long long n_items;
+};
+
+BatchLayout batch_layout(gb_plan *const *plans, int n)
+{
+    BatchLayout B{};
+    B.n_items = 0;
+    for (int m = 0; m < n; ++m) B.n_items += (long long)plans[m]->n_tiles * plans[m]->n_groups;
+    size_t o = 0;
+    B.models = o; o = align256(o + (size_t)n * sizeof(BatchModel));
+    B.maps = o; o = align256(o + (size_t)n * sizeof(BatchMaps));
+    B.items = o; o = align256(o + (size_t)std::max<long long>(B.n_items, 1) * 16);
+    B.total = o;
+    return B;
+}
+
+int check_batch(gb_plan *const *plans, int n, const gb_model_io *io, bool gradient)
+{
+    if (!plans || !io || n < 1) return fail(GB_E_ARG, "empty batch");
+    for (int m = 0; m < n; ++m) {
+        const gb_plan *P = plans[m];
+        if (!P) return fail(GB_E_ARG, "null plan in batch");
+        if (P->R != plans[0]->R || (P->d.free_surface != 0) != (plans[0]->d.free_surface != 0))
+            return fail(GB_E_ARG, "a batch needs one stencil order and one free-surface setting");
+        if (P->tz != 16) return fail(GB_E_ARG, "batched plans use 16-row tiles (gb_plan_set_tiling(plan, 16, ...))");
+        const gb_model_io &x = io[m];
+        if (!x.vp || !x.rho || !x.damp || !x.wavelet || !x.workspace) return fail(GB_E_ARG, "null model input");
+        if (gradient) {
+            if (!x.store || !x.grad_vp) return fail(GB_E_ARG, "gradient needs a store and grad_vp for every model");
+            if (int rc = check_store(P, x.store)) return rc;
+            if (x.store->checkpoint_every != io[0].store->checkpoint_every ||
+                (x.store->with_rho != 0) != (io[0].store->with_rho != 0) || x.store->format != io[0].store->format)
+                return fail(GB_E_ARG, "a batch shares checkpoint_every, format and with_rho");
+            if (x.grad_rho && !x.store->with_rho) return fail(GB_E_ARG, "density gradient needs with_rho stores");
+        } else if (x.store) {
+            if (int rc = check_store(P, x.store)) return rc;
+            if (x.store->checkpoint_every != io[0].store->checkpoint_every ||
+                (x.store->with_rho != 0) != (io[0].store->with_rho != 0))
+                return fail(GB_E_ARG, "a batch shares checkpoint_every and with_rho");
+        }
+    }
+    return GB_OK;
+}
+
+int upload_batch(gb_plan *const *plans, int n, const std::vector<BatchModel> &models,
+                 const std::vector<BatchMaps> &maps, char *bws, const BatchLayout &B, cudaStream_t st)
+{
+    std::vector<int4> items;
+    items.reserve(B.n_items);
+    for (int m = 0; m < n; ++m)
+        for (int t = 0; t < plans[m]->n_tiles; ++t)
+            for (int g = 0; g < plans[m]->n_groups; ++g) items.push_back(int4{m, t, g, 0});
+    GB_CUDA(cudaMemcpyAsync(bws + B.models, models.data(), n * sizeof(BatchModel), cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(bws + B.maps, maps.data(), n * sizeof(BatchMaps), cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(bws + B.items, items.data(), items.size() * 16, cudaMemcpyHostToDevice, st));
+    return GB_OK;
+}
+
+int make_state_maps(const gb_plan *P, const float *buf, CUtensorMap (&m)[3])
+{
+    const int n_planes = 3 * P->d.n_shots;
+    if (int rc = make_map(&m[0], buf, P->Nx, P->Nz, P->pitch, n_planes, RW, box_rows_p(P->R, P->tz))) return rc;
+    if (int rc = make_map(&m[1], buf, P->Nx, P->Nz, P->pitch, n_planes, VXW, box_rows_p(P->R, P->tz))) return rc;
+    return make_map(&m[2], buf, P->Nx, P->Nz, P->pitch, n_planes, RW, box_rows_vz(P->R, P->tz));
+}
+
+int launch_batch(gb_plan *P0, const StepKernel &K, long long n_items, void **args, cudaStream_t st)
+{
+    GB_CUDA(cudaLaunchKernel(K.fn, dim3((unsigned)n_items), dim3(NTHR), args, K.smem, st));
+    ++P0->launches;
+    return GB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t gb_batch_workspace_bytes(gb_plan *const *plans, int n_models)
+{
+    if (!plans || n_models < 1) return 0;
+    for (int m = 0; m < n_models; ++m)
+        if (!plans[m]) return 0;
+    return batch_layout(plans, n_models).total + 256;
+}
+
+int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *batch_workspace,
+                     size_t batch_workspace_bytes, void *stream)
+{
+    g_last_error.clear();
+    if (int rc = check_batch(plans, n, io, false)) return rc;
+    const BatchLayout B = batch_layout(plans, n);
+    char *bws = aligned_ws(batch_workspace);
+    if (!batch_workspace || batch_workspace_bytes < B.total + (size_t)(bws - reinterpret_cast<char *>(batch_workspace)))
+        return fail(GB_E_WORKSPACE, "batch workspace too small");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    gb_plan *P0 = plans[0];
+    const bool fs = P0->d.free_surface != 0;
+    std::vector<BatchModel> models(n);
+    std::vector<BatchMaps> maps(n);
+    bool any_energy = false, any_cache = false, rho = false;
+    int maxnt = 0, K = 0;
+    P0->mark(0, true, st);
+    for (int m = 0; m < n; ++m) {
+        gb_plan *P = plans[m];
+        const gb_model_io &x = io[m];
+        const Layout L = layout(P);
+        char *ws = aligned_ws(x.workspace);
+        if (x.workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(x.workspace)))
+            return fail(GB_E_WORKSPACE, "workspace of model " + std::to_string(m) + " too small");
+        Setup Su;
+        if (int rc = common_setup(P, L, ws, x.vp, x.rho, x.damp, st, &Su)) return rc;
+        const int S = P->d.n_shots;
+        float *buf0 = reinterpret_cast<float *>(ws + L.fields), *buf1 = buf0 + (size_t)S * 3 * P->plane;
+        float *energy = reinterpret_cast<float *>(ws + L.energy);
+        const bool want_energy = x.energy_p || x.energy_vx || x.energy_vz;
+        GB_CUDA(cudaMemsetAsync(buf0, 0, (size_t)2 * S * 3 * P->plane * 4, st));
+        if (want_energy) GB_CUDA(cudaMemsetAsync(energy, 0, 3 * P->plane * 4, st));
+        BatchModel &M = models[m];
+        M = BatchModel{};
+        FwdArgs &F = M.f;
+        F.g = P->geom();
+        F.a1 = Su.a1; F.k1 = Su.k1; F.a2 = Su.a2; F.k2 = Su.k2; F.k3 = Su.k3;
+        F.tile_fast = Su.tile_fast;
+        F.src_z = Su.d_src; F.src_x = Su.d_src + S;
+        F.wavelet = x.wavelet;
+        F.rcv_ptr = Su.d_rptr; F.rcv_ent = Su.d_rent;
+        F.tr_p = x.trace_p; F.tr_vx = x.trace_vx; F.tr_vz = x.trace_vz;
+        F.energy = want_energy ? energy : nullptr;
+        F.img_field_stride = (long long)S * P->plane;
+        F.err = Su.err;
+        M.fld[0] = buf0;
+        M.fld[1] = buf1;
+        M.nt = P->d.nt;
+        const gb_grad_store *sto = x.store;
+        M.K = sto ? std::min<int>(sto->checkpoint_every, P->d.nt) : P->d.nt;
+        M.t_cache = sto ? P->d.nt - sto->cached_steps : P->d.nt;
+        M.cache = sto && sto->cached_steps > 0 ? reinterpret_cast<float *>(sto->imaging) : nullptr;
+        M.step_img = (long long)((sto && sto->with_rho) ? 3 : 1) * S * P->plane;
+        if (int rc = make_state_maps(P, buf0, maps[m].fld[0])) return rc;
+        if (int rc = make_state_maps(P, buf1, maps[m].fld[1])) return rc;
+        if (int rc = make_map2d(&maps[m].a1, Su.a1, P->Nx, P->Nz, P->pitch, RW, box_rows_p(P->R, P->tz))) return rc;
+        if (int rc = make_map2d(&maps[m].a2, Su.a2, P->Nx, P->Nz, P->pitch, RW, P->tz)) return rc;
+        any_energy |= want_energy;
+        any_cache |= M.cache != nullptr;
+        rho |= sto && sto->with_rho;
+        maxnt = std::max(maxnt, M.nt);
+        K = M.K;
+    }
+    if (int rc = upload_batch(plans, n, models, maps, bws, B, st)) return rc;
+    const StepKernel K0 = fwd_batch_kernel_for(P0->R, fs, any_energy, any_cache ? (rho ? 2 : 1) : 0);
+    if (int rc = prepare_kernel(K0)) return rc;
+    const int4 *items = reinterpret_cast<const int4 *>(bws + B.items);
+    const BatchModel *dmodels = reinterpret_cast<const BatchModel *>(bws + B.models);
+    const BatchMaps *dmaps = reinterpret_cast<const BatchMaps *>(bws + B.maps);
+    int mode = kBatchForward, t0 = 0;
+    P0->phase_steps[0] += maxnt;
+    for (int tau = 0; tau < maxnt; ++tau) {
+        for (int m = 0; m < n; ++m) {
+            const gb_grad_store *sto = io[m].store;
+            if (sto && tau < std::min(models[m].t_cache, models[m].nt) && tau % models[m].K == 0) {
+                const Layout L = layout(plans[m]);
+                unsigned int *amax = reinterpret_cast<unsigned int *>(aligned_ws(io[m].workspace) + L.amax);
+                if (int rc = save_checkpoint(plans[m], models[m].fld[tau & 1], sto->checkpoints, tau / models[m].K,
+                                             sto->format, amax, 0, plans[m]->d.n_shots, st))
+                    return rc;
+            }
+        }
+        int tau_v = tau;
+        void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps, (void *)&tau_v, (void *)&mode, (void *)&t0};
+        if (int rc = launch_batch(P0, K0, B.n_items, args, st)) return rc;
+    }
+    for (int m = 0; m < n; ++m) {
+        const gb_model_io &x = io[m];
+        float *eouts[3] = {x.energy_p, x.energy_vx, x.energy_vz};
+        const Layout L = layout(plans[m]);
+        float *energy = reinterpret_cast<float *>(aligned_ws(x.workspace) + L.energy);
+        for (int f = 0; f < 3; ++f)
+            if (eouts[f]) {
+                const gb_model_desc &d = plans[m]->d;
+                extract_interior_kernel<<<148, 256, 0, st>>>(energy + f * plans[m]->plane, d.nz, d.nx, d.nabc,
+                                                             plans[m]->pitch, eouts[f]);
+                GB_CUDA(cudaGetLastError());
+                ++P0->launches;
+            }
+    }
+    (void)K;
+    P0->mark(0, false, st);
+    return GB_OK;
+}
+
+int gb_batch_backward(gb_plan *const *plans, int n, const gb_model_io *io, void *batch_workspace,
+                      size_t batch_workspace_bytes, void *stream)
+{
+    g_last_error.clear();
+    if (int rc = check_batch(plans, n, io, true)) return rc;
+    const BatchLayout B = batch_layout(plans, n);
+    char *bws = aligned_ws(batch_workspace);
+    if (!batch_workspace || batch_workspace_bytes < B.total + (size_t)(bws - reinterpret_cast<char *>(batch_workspace)))
+        return fail(GB_E_WORKSPACE, "batch workspace too small");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    gb_plan *P0 = plans[0];
+    const bool fs = P0->d.free_surface != 0;
+    const bool rho = io[0].store->with_rho != 0;
+    const int K = std::min<int>(io[0].store->checkpoint_every, 1 << 30);
+    std::vector<BatchModel> models(n);
+    std::vector<BatchMaps> maps(n);
+    std::vector<Layout> Ls;
+    int maxnt = 0;
+    for (int m = 0; m < n; ++m) {
+        gb_plan *P = plans[m];
+        const gb_model_io &x = io[m];
+        const int Km = std::min<int>(K, P->d.nt);
+        const Layout L = layout(P, rho ? 2 : 1, Km);
+        Ls.push_back(L);
+        char *ws = aligned_ws(x.workspace);
+        if (x.workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(x.workspace)))
+            return fail(GB_E_WORKSPACE, "workspace of model " + std::to_string(m) + " too small");
+        Setup Su;
+        if (int rc = common_setup(P, L, ws, x.vp, x.rho, x.damp, st, &Su)) return rc;
+        const int S = P->d.n_shots;
+        const size_t state_fl = (size_t)S * 3 * P->plane;
+        float *fb0 = reinterpret_cast<float *>(ws + L.fields), *mu0 = reinterpret_cast<float *>(ws + L.mu);
+        float *G1 = reinterpret_cast<float *>(ws + L.g1), *C1 = reinterpret_cast<float *>(ws + L.c1);
+        float *G2 = rho ? reinterpret_cast<float *>(ws + L.g2) : nullptr;
+        float *C2 = rho ? reinterpret_cast<float *>(ws + L.c2) : nullptr;
+        int *d_aptr = reinterpret_cast<int *>(ws + L.arcv_ptr);
+        int4 *d_aent = reinterpret_cast<int4 *>(ws + L.arcv_ent);
+        GB_CUDA(cudaMemcpyAsync(d_aptr, P->arcv_ptr.data(), (P->n_tiles + 1) * 4, cudaMemcpyHostToDevice, st));
+        if (!P->arcv_ent.empty())
+            GB_CUDA(cudaMemcpyAsync(d_aent, P->arcv_ent.data(), P->arcv_ent.size() * 16, cudaMemcpyHostToDevice, st));
+        GB_CUDA(cudaMemsetAsync(mu0, 0, 2 * state_fl * 4, st));
+        GB_CUDA(cudaMemsetAsync(G1, 0, (size_t)P->n_groups * P->plane * 4, st));
+        GB_CUDA(cudaMemsetAsync(C1, 0, (size_t)P->n_groups * P->plane * 4, st));
+        if (G2) {
+            GB_CUDA(cudaMemsetAsync(G2, 0, (size_t)P->n_groups * P->plane * 4, st));
+            GB_CUDA(cudaMemsetAsync(C2, 0, (size_t)P->n_groups * P->plane * 4, st));
+        }
+        BatchModel &M = models[m];
+        M = BatchModel{};
+        FwdArgs &F = M.f;
+        F.g = P->geom();
+        F.a1 = Su.a1; F.k1 = Su.k1; F.a2 = Su.a2; F.k2 = Su.k2; F.k3 = Su.k3;
+        F.tile_fast = Su.tile_fast;
+        F.src_z = Su.d_src; F.src_x = Su.d_src + S;
+        F.wavelet = x.wavelet;
+        F.rcv_ptr = Su.d_rptr; F.rcv_ent = Su.d_rent;
+        F.img_field_stride = (long long)S * P->plane;
+        F.err = Su.err;
+        AdjArgs &A = M.a;
+        A.g = F.g;
+        A.a1 = Su.a1; A.k1 = Su.k1; A.a2 = Su.a2; A.k2 = Su.k2; A.k3 = Su.k3;
+        A.tile_fast = Su.tile_fast;
+        A.rcv_ptr = d_aptr; A.rcv_ent = d_aent;
+        A.res_p = x.res_p; A.res_vx = x.res_vx; A.res_vz = x.res_vz;
+        A.img_field_stride = (long long)S * P->plane;
+        A.G1 = G1; A.C1 = C1; A.G2 = G2; A.C2 = C2;
+        A.err = Su.err;
+        M.fld[0] = fb0;
+        M.fld[1] = fb0 + state_fl;
+        M.mu[0] = mu0;
+        M.mu[1] = mu0 + state_fl;
+        M.nt = P->d.nt;
+        M.K = Km;
+        M.t_cache = P->d.nt - x.store->cached_steps;
+        M.cache = x.store->cached_steps > 0 ? reinterpret_cast<float *>(x.store->imaging) : nullptr;
+        M.segimg = reinterpret_cast<float *>(ws + L.img);
+        M.step_img = (long long)(rho ? 3 : 1) * S * P->plane;
+        if (int rc = make_state_maps(P, M.fld[0], maps[m].fld[0])) return rc;
+        if (int rc = make_state_maps(P, M.fld[1], maps[m].fld[1])) return rc;
+        if (int rc = make_state_maps(P, M.mu[0], maps[m].mu[0])) return rc;
+        if (int rc = make_state_maps(P, M.mu[1], maps[m].mu[1])) return rc;
+        if (int rc = make_map2d(&maps[m].a1, Su.a1, P->Nx, P->Nz, P->pitch, RW, box_rows_p(P->R, P->tz))) return rc;
+        if (int rc = make_map2d(&maps[m].a2, Su.a2, P->Nx, P->Nz, P->pitch, RW, P->tz)) return rc;
+        maxnt = std::max(maxnt, M.nt);
+    }
+    if (int rc = upload_batch(plans, n, models, maps, bws, B, st)) return rc;
+    const StepKernel KF = fwd_batch_kernel_for(P0->R, fs, false, rho ? 2 : 1);
+    const StepKernel KA = adj_batch_kernel_for(P0->R, fs, rho);
+    if (int rc = prepare_kernel(KF)) return rc;
+    if (int rc = prepare_kernel(KA)) return rc;
+    const int4 *items = reinterpret_cast<const int4 *>(bws + B.items);
+    const BatchModel *dmodels = reinterpret_cast<const BatchModel *>(bws + B.models);
+    const BatchMaps *dmaps = reinterpret_cast<const BatchMaps *>(bws + B.maps);
+
+    // batch-wide segments of K steps; a model recomputes a segment only for
+    // its steps below min(nt, t_cache)
+    const int Kb = std::min(K, maxnt);
+    const int seg_top = (maxnt - 1) / Kb;
+    for (int seg = seg_top; seg >= 0; --seg) {
+        const int t0 = seg * Kb, t1 = std::min(maxnt, t0 + Kb);
+        int rec_end = t0;
+        for (int m = 0; m < n; ++m) {
+            const int lim = std::min(models[m].nt, models[m].t_cache);
+            if (t0 < lim) {
+                if (int rc = restore_checkpoint(plans[m], models[m].fld[0], io[m].store->checkpoints, t0 / models[m].K,
+                                                io[m].store->format, 0, plans[m]->d.n_shots, st))
+                    return rc;
+                rec_end = std::max(rec_end, std::min(t1, lim));
+            }
+        }
+        if (rec_end > t0) {
+            P0->mark(1, true, st);
+            P0->phase_steps[1] += rec_end - t0;
+            int mode = kBatchRecompute, tz0 = t0;
+            for (int tau = t0; tau < rec_end; ++tau) {
+                int tau_v = tau;
+                void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps, (void *)&tau_v, (void *)&mode,
+                                (void *)&tz0};
+                if (int rc = launch_batch(P0, KF, B.n_items, args, st)) return rc;
+            }
+            P0->mark(1, false, st);
+        }
+        P0->mark(2, true, st);
+        P0->phase_steps[2] += t1 - t0;
+        for (int tau = t1 - 1; tau >= t0; --tau) {
+            int tau_v = tau;
+            void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps, (void *)&tau_v};
+            if (int rc = launch_batch(P0, KA, B.n_items, args, st)) return rc;
+        }
+        P0->mark(2, false, st);
+    }
+    for (int m = 0; m < n; ++m) {
+        const gb_model_desc &d = plans[m]->d;
+        const BatchModel &M = models[m];
+        grad_finish_kernel<<<4 * 148, 256, 0, st>>>(io[m].vp, io[m].rho, M.a.G1, M.a.C1, M.a.G2, M.a.C2,
+                                                    plans[m]->n_groups, plans[m]->plane, d.nz, d.nx, d.nabc,
+                                                    plans[m]->pitch, io[m].grad_vp, io[m].grad_rho);
+        GB_CUDA(cudaGetLastError());
+        ++P0->launches;
+    }
     return GB_OK;
 }
 

@@ -94,11 +94,13 @@ __device__ __forceinline__ bool tile_is_interior(const StepGeom &g, int z0, int 
 
 // IMG: 0 no imaging fields; 1 store I = -div(v^n) on the p mask (velocity
 // gradient); 2 also store Jx = dx(p), Jz = dz(p) on the vx / vz masks (density).
+// The body of one CTA: tile `tile`, shot group `group` of the model A
+// describes; the maps are the TMA descriptors of the input state and of the
+// a1 / a2 planes.
 template <int R, int TZ, bool FS, bool ENERGY, int IMG>
-__global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
-fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mVX,
-                const __grid_constant__ CUtensorMap mVZ, const __grid_constant__ CUtensorMap mA1,
-                const __grid_constant__ CUtensorMap mA2, const FwdArgs A)
+__device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMap *mVX, const CUtensorMap *mVZ,
+                                         const CUtensorMap *mA1, const CUtensorMap *mA2, const FwdArgs &A,
+                                         const int group, const int tile)
 {
     using G = Geo<R, TZ>;
     using SM = StepSmem<R, TZ>;
@@ -109,10 +111,6 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
     float *sA2 = sA1 + SM::A1_FL;
     uint64_t *bars = reinterpret_cast<uint64_t *>(sA1 + SM::COEF_FL);
 
-    // launch covers shot groups [grp0, grp0 + grp_count): one launch for all
-    // groups, or one launch per group when groups run on their own streams
-    const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
-    const int tile = (int)(blockIdx.x / A.grp_count);
     const int z0 = (tile / g.tiles_x) * TZ;
     const int x0 = (tile % g.tiles_x) * TX;
     const int s0 = group * g.shots_per_cta;
@@ -128,10 +126,10 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bars[2], SM::COEF_BYTES);
-        tma_load_2d(sA1, &mA1, &bars[2], x0 - 4, z0 - R);
-        tma_load_2d(sA2, &mA2, &bars[2], x0 - 4, z0);
+        tma_load_2d(sA1, mA1, &bars[2], x0 - 4, z0 - R);
+        tma_load_2d(sA2, mA2, &bars[2], x0 - 4, z0);
         for (int k = 0; k < 2 && k < ns; ++k)
-            stage_loads<R>(&mP, &mVX, &mVZ, smem + k * G::STAGE_FL, &bars[k], G::STAGE_BYTES, x0, z0, s0 + k,
+            stage_loads<R>(mP, mVX, mVZ, smem + k * G::STAGE_FL, &bars[k], G::STAGE_BYTES, x0, z0, s0 + k,
                            G::P_FL, G::VX_FL);
     }
     for (int k = threadIdx.x; k < ns; k += NTHR) s_src[k] = make_int2(A.src_z[s0 + k], A.src_x[s0 + k]);
@@ -170,7 +168,7 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
             return;
         }
         if (threadIdx.x == 0 && k >= 1 && k + 1 < ns)   // refill shot k-1's buffer with shot k+1
-            stage_loads<R>(&mP, &mVX, &mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
+            stage_loads<R>(mP, mVX, mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
                            s + 1, G::P_FL, G::VX_FL);
         float *sP = smem + b * G::STAGE_FL;
         float *sVX = sP + G::P_FL;
@@ -205,7 +203,7 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                         divergence4<R>(sVX + r * VXW, lane, wz, u, g.c, D);
 #pragma unroll
                         for (int q = 0; q < 4; ++q) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], at(pv, q));
-                        if (tile_cell)
+                        if (tile_cell && A.imaging)
                             stg4(A.imaging + (long long)s * g.plane + (long long)gz * g.pitch + gx0,
                                  make_float4(-D[0], -D[1], -D[2], -D[3]));
                     } else {
@@ -222,16 +220,18 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                                 at(img, q) = m ? -D[q] : 0.f;
                                 if (m) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], (1.f - at(k1, q)) * at(pv, q));
                             }
-                            if (tile_cell) stg4(A.imaging + (long long)s * g.plane + o, img);
+                            if (tile_cell && A.imaging) stg4(A.imaging + (long long)s * g.plane + o, img);
                         }
                     }
                     if (gz == sz && sx >= gx0 && sx < gx0 + 4) {
-                        const float amp = g.dt * A.wavelet[(long long)s * g.nt + A.it];
+                        // p + dt * w, rounded after the product and after the
+                        // sum as the reference does (acoustic_2d.py:230-233)
+                        const float amp = __fmul_rn(g.dt, A.wavelet[(long long)s * g.nt + A.it]);
                         const int q = sx - gx0;
-                        if (q == 0) pv.x += amp;
-                        else if (q == 1) pv.y += amp;
-                        else if (q == 2) pv.z += amp;
-                        else pv.w += amp;
+                        if (q == 0) pv.x = __fadd_rn(pv.x, amp);
+                        else if (q == 1) pv.y = __fadd_rn(pv.y, amp);
+                        else if (q == 2) pv.z = __fadd_rn(pv.z, amp);
+                        else pv.w = __fadd_rn(pv.w, amp);
                     }
                     sts4(sP + r * RW + 4 * lane, pv);
                 }
@@ -301,7 +301,7 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                                 }
                             }
                         }
-                        if (IMG == 2) {
+                        if (IMG == 2 && A.imaging) {
                             stg4(A.imaging + (long long)s * g.plane + A.img_field_stride + o, jx);
                             stg4(A.imaging + (long long)s * g.plane + 2 * A.img_field_stride + o, jz);
                         }
@@ -318,9 +318,9 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                             for (int q = 0; q < 4; ++q) {
                                 const int gx = gx0 + q;
                                 if (gx >= g.pml && gx < g.pml + g.nx) {
-                                    at(e_p[u], q) += at(pv, q) * at(pv, q);
-                                    at(e_vx[u], q) += at(vx, q) * at(vx, q);
-                                    at(e_vz[u], q) += at(vz, q) * at(vz, q);
+                                    at(e_p[u], q) = __fmaf_rn(at(pv, q), at(pv, q), at(e_p[u], q));
+                                    at(e_vx[u], q) = __fmaf_rn(at(vx, q), at(vx, q), at(e_vx[u], q));
+                                    at(e_vz[u], q) = __fmaf_rn(at(vz, q), at(vz, q), at(e_vz[u], q));
                                 }
                             }
                         }
@@ -346,7 +346,7 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
         fence_proxy_async_smem();
     }
 
-    if (ENERGY && vlane) {
+    if (ENERGY && vlane && A.energy) {
         // add this CTA's partial sums (over its shots) into the padded maps
 #pragma unroll
         for (int u = 0; u < G::LV; ++u) {
@@ -359,6 +359,20 @@ fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
             }
         }
     }
+}
+
+// Single-model launch: blockIdx covers shot groups [grp0, grp0 + grp_count)
+// of every tile (one launch for all groups, or one per group when the groups
+// run on their own streams).
+template <int R, int TZ, bool FS, bool ENERGY, int IMG>
+__global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
+fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mVX,
+                const __grid_constant__ CUtensorMap mVZ, const __grid_constant__ CUtensorMap mA1,
+                const __grid_constant__ CUtensorMap mA2, const FwdArgs A)
+{
+    const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
+    const int tile = (int)(blockIdx.x / A.grp_count);
+    fwd_body<R, TZ, FS, ENERGY, IMG>(&mP, &mVX, &mVZ, &mA1, &mA2, A, group, tile);
 }
 
 template <int R, int TZ>

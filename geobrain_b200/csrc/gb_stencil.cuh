@@ -1,6 +1,8 @@
 // Stencil evaluation on the shared-memory rectangles, shared by the forward
 // and adjoint step kernels.  Each lane owns 4 adjacent columns; the
-// z-direction taps come from a per-warp register window.
+// z-direction taps come from a per-warp register window.  Every tap is an
+// explicit fused multiply-add, so every kernel that inlines these rounds the
+// same way.
 #pragma once
 
 #include "gb_device.cuh"
@@ -31,7 +33,7 @@ __device__ __forceinline__ void divergence4(const float *vxr, int lane, const fl
         float d = 0.f;
 #pragma unroll
         for (int k = 0; k < R; ++k)
-            d += c[k] * (((e[q + 4 + k] - e[q + 3 - k]) + at(wz[u + R + k], q)) - at(wz[u + R - 1 - k], q));
+            d = __fmaf_rn(c[k], ((e[q + 4 + k] - e[q + 3 - k]) + at(wz[u + R + k], q)) - at(wz[u + R - 1 - k], q), d);
         D[q] = d;
     }
 }
@@ -57,7 +59,7 @@ __device__ __forceinline__ void grad_x4(const float *pr, int lane, const float (
     for (int q = 0; q < 4; ++q) {
         float d = 0.f;
 #pragma unroll
-        for (int k = 0; k < R; ++k) d += c[k] * (f[q + 5 + k] - f[q + 4 - k]);
+        for (int k = 0; k < R; ++k) d = __fmaf_rn(c[k], f[q + 5 + k] - f[q + 4 - k], d);
         D[q] = d;
     }
 }
@@ -72,7 +74,7 @@ __device__ __forceinline__ void grad_z4(const float4 *wp, int u, const float (&c
     for (int q = 0; q < 4; ++q) {
         float d = 0.f;
 #pragma unroll
-        for (int k = 0; k < R; ++k) d += c[k] * (at(wp[u + R + k], q) - at(wp[u + R - 1 - k], q));
+        for (int k = 0; k < R; ++k) d = __fmaf_rn(c[k], at(wp[u + R + k], q) - at(wp[u + R - 1 - k], q), d);
         D[q] = d;
     }
 }

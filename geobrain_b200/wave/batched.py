@@ -1,10 +1,235 @@
-"""Batched propagation of many models (placeholder until the batched engine lands)."""
+"""Many models in one batch: one kernel launch per time step for all of them.
+
+``acoustic_forward_batched(models)`` takes a list of per-model argument
+dicts (the keyword arguments of ``acoustic_forward_kernel``: nx, nz, dx, dz,
+nt, dt, nabc, free_surface, src_x, src_z, src_n, src_v, rcv_x, rcv_z, rcv_n,
+damp, vp, rho) and returns the list of result dicts.  Models may differ in
+grid size, step count, shots and receivers (an SVGD / HMC particle ensemble,
+or unrelated models), but share the stencil order and the free-surface
+setting.  When any vp / rho requires grad, the traces are differentiable
+through the batched hand-written adjoint.
+
+This replaces the serial per-particle loop of GeoBrain's inverse-problem
+bridge (geobrain/core/inverse.py:104-110), which calls the propagator once
+per particle.
+"""
 from __future__ import annotations
 
+import ctypes
+from typing import List, Sequence
 
-class AcousticBatch:  # pragma: no cover - filled in with the batched engine
-    pass
+import numpy as np
+import torch
+
+from .. import _lib
+from . import engine
+from .kernel import _as_f32
+
+BATCH_TILE_ROWS = 16
 
 
-def acoustic_forward_batched(*args, **kwargs):  # pragma: no cover
-    raise NotImplementedError
+class ModelIO(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "vp", "rho", "damp", "wavelet", "trace_p", "trace_vx", "trace_vz", "energy_p", "energy_vx", "energy_vz",
+        "res_p", "res_vx", "res_vz", "grad_vp", "grad_rho", "store", "workspace")] + [
+        ("workspace_bytes", ctypes.c_size_t)]
+
+
+def _bind():
+    return _lib.load()
+
+
+class _Prepared:
+    """Plans, device inputs and sizes of one batch."""
+
+    def __init__(self, models: Sequence[dict], fd_order: int, device):
+        if not models:
+            raise ValueError("empty batch")
+        self.device = device
+        self.plans, self.inputs = [], []
+        fs0 = bool(models[0].get("free_surface", False))
+        for i, m in enumerate(models):
+            if bool(m.get("free_surface", False)) != fs0:
+                raise ValueError("all models of a batch share the free-surface setting")
+            if float(m["dx"]) != float(m.get("dz", m["dx"])):
+                raise ValueError(f"model {i}: grid spacing must be equal")
+            src_n, rcv_n = int(m["src_n"]), int(m["rcv_n"])
+            geo = engine.Geometry(int(m["nz"]), int(m["nx"]), int(m["nabc"]), int(m["nt"]), float(m["dt"]),
+                                  float(m["dx"]), engine.FD_ORDERS[fd_order], fs0)
+            plan = engine.get_plan(geo, engine._i64(m["src_x"])[:src_n], engine._i64(m["src_z"])[:src_n],
+                                   engine._i64(m["rcv_x"])[:rcv_n], engine._i64(m["rcv_z"])[:rcv_n])
+            plan.set_tiling(BATCH_TILE_ROWS, min(plan.n_shots, 8))
+            w = _as_f32(m["src_v"], device, "src_v")
+            if w.dim() == 1:
+                w = w.unsqueeze(0).expand(src_n, -1)
+            w = w.contiguous()
+            damp = _as_f32(m["damp"], device, "damp")
+            self.plans.append(plan)
+            self.inputs.append((m["vp"], m["rho"], damp, w))
+        self.plan_arr = (ctypes.c_void_p * len(self.plans))(*[p.h.value for p in self.plans])
+
+
+def _forward(prep: _Prepared, vps, rhos, want_energy: bool, stores=None):
+    L = _bind()
+    dev = prep.device
+    n = len(prep.plans)
+    ios = (ModelIO * n)()
+    keep, outs = [], []
+    for i, plan in enumerate(prep.plans):
+        g = plan.geo
+        S, NR = plan.n_shots, plan.n_rcv
+        tr = [torch.empty((S, g.nt, NR), device=dev) for _ in range(3)]
+        en = [torch.empty((g.nz, g.nx), device=dev) for _ in range(3)] if want_energy else None
+        grad = stores is not None
+        ws = engine.workspace(plan.workspace_bytes(False, 0), dev)
+        _, _, damp, w = prep.inputs[i]
+        io = ios[i]
+        io.vp, io.rho, io.damp, io.wavelet = vps[i].data_ptr(), rhos[i].data_ptr(), damp.data_ptr(), w.data_ptr()
+        io.trace_p, io.trace_vx, io.trace_vz = [t.data_ptr() for t in tr]
+        if en:
+            io.energy_p, io.energy_vx, io.energy_vz = [e.data_ptr() for e in en]
+        io.store = ctypes.addressof(stores[i]) if grad else None
+        io.workspace, io.workspace_bytes = ws.data_ptr(), ws.numel()
+        keep.append(ws)
+        outs.append((tr, en))
+    bws = engine.workspace(L.gb_batch_workspace_bytes(prep.plan_arr, n), dev)
+    with torch.cuda.device(dev):
+        rc = L.gb_batch_forward(prep.plan_arr, n, ios, bws.data_ptr(), bws.numel(), engine.stream_handle(dev))
+    _lib.check(rc)
+    return outs
+
+
+class _BatchFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, prep, opts, *params):
+        n = len(prep.plans)
+        vps = [p.detach().to(torch.float32).contiguous() for p in params[:n]]
+        rhos = [p.detach().to(torch.float32).contiguous() for p in params[n:]]
+        dev = prep.device
+        K, fmt, with_rho = opts["K"], opts["fmt"], opts["with_rho"]
+        stores, keep = [], []
+        for i, plan in enumerate(prep.plans):
+            cached = opts["cached"][i]
+            n_ck = -(-(plan.geo.nt - cached) // min(K, plan.geo.nt))
+            ck = torch.empty(max(n_ck * plan.checkpoint_bytes(plan.geo.nt, fmt), 256), dtype=torch.uint8, device=dev)
+            img = torch.empty(max(plan.imaging_bytes(cached, with_rho), 256), dtype=torch.uint8, device=dev)
+            stores.append(engine.make_store(ck if n_ck > 0 else None, min(K, plan.geo.nt), fmt,
+                                            img if cached > 0 else None, cached, with_rho))
+            keep.append((ck, img))
+        outs = _forward(prep, vps, rhos, opts["want_energy"], stores)
+        ctx.prep, ctx.opts, ctx.stores, ctx.keep = prep, opts, stores, keep
+        ctx.save_for_backward(*vps, *rhos)
+        flat = []
+        nondiff = []
+        for tr, en in outs:
+            if en is None:
+                en = [torch.zeros((1,), device=dev) for _ in range(3)]
+            flat += tr + en
+            nondiff += en
+        ctx.mark_non_differentiable(*nondiff)
+        return tuple(flat)
+
+    @staticmethod
+    def backward(ctx, *grads):
+        prep = ctx.prep
+        n = len(prep.plans)
+        saved = ctx.saved_tensors
+        vps, rhos = saved[:n], saved[n:]
+        need_vp = any(ctx.needs_input_grad[2:2 + n])
+        need_rho = any(ctx.needs_input_grad[2 + n:])
+        L = _bind()
+        dev = prep.device
+        ios = (ModelIO * n)()
+        keep, gv, gr = [], [], []
+        for i, plan in enumerate(prep.plans):
+            g = plan.geo
+            res = [None if t is None else t.to(torch.float32).contiguous() for t in grads[6 * i:6 * i + 3]]
+            gvp = torch.empty((g.nz, g.nx), device=dev)
+            grho = torch.empty((g.nz, g.nx), device=dev) if (need_rho and ctx.stores[i].with_rho) else None
+            st = ctx.stores[i]
+            ws = engine.workspace(plan.workspace_bytes(2 if st.with_rho else 1, st.checkpoint_every), dev)
+            _, _, damp, w = prep.inputs[i]
+            io = ios[i]
+            io.vp, io.rho, io.damp, io.wavelet = vps[i].data_ptr(), rhos[i].data_ptr(), damp.data_ptr(), w.data_ptr()
+            io.res_p, io.res_vx, io.res_vz = [_lib.ptr(r) for r in res]
+            io.grad_vp, io.grad_rho = gvp.data_ptr(), _lib.ptr(grho)
+            io.store = ctypes.addressof(st)
+            io.workspace, io.workspace_bytes = ws.data_ptr(), ws.numel()
+            keep.append((ws, res))
+            gv.append(gvp)
+            gr.append(grho)
+        bws = engine.workspace(L.gb_batch_workspace_bytes(prep.plan_arr, n), dev)
+        with torch.cuda.device(dev):
+            rc = L.gb_batch_backward(prep.plan_arr, n, ios, bws.data_ptr(), bws.numel(), engine.stream_handle(dev))
+        _lib.check(rc)
+        ctx.keep = None
+        out_vp = [g if ctx.needs_input_grad[2 + i] else None for i, g in enumerate(gv)]
+        out_rho = [g if ctx.needs_input_grad[2 + n + i] else None for i, g in enumerate(gr)]
+        return (None, None, *out_vp, *out_rho)
+
+
+def acoustic_forward_batched(models: Sequence[dict], *, fd_order: int = 8, device=None, want_energy: bool = True,
+                             checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
+                             imaging_cache="auto") -> List[dict]:
+    """Forward-model every model of `models` together; see the module doc."""
+    if fd_order not in engine.FD_ORDERS:
+        raise ValueError(f"fd_order must be one of {sorted(engine.FD_ORDERS)}")
+    device = torch.device(device if device is not None else models[0]["vp"].device)
+    if device.type != "cuda":
+        raise ValueError(f"geobrain_b200 runs on CUDA devices only (device={device})")
+    for m in models:
+        if int(m.get("snapshot_every", 0)) > 0:
+            raise ValueError("snapshots are not taken in batched runs; use acoustic_forward_kernel")
+    prep = _Prepared(models, fd_order, device)
+    vps = [_as_f32(m["vp"], device, "vp") if not torch.is_tensor(m["vp"]) or not m["vp"].requires_grad else m["vp"]
+           for m in models]
+    rhos = [_as_f32(m["rho"], device, "rho") if not torch.is_tensor(m["rho"]) or not m["rho"].requires_grad
+            else m["rho"] for m in models]
+    needs_grad = torch.is_grad_enabled() and any(t.requires_grad for t in vps + rhos)
+    outs = []
+    if not needs_grad:
+        res = _forward(prep, [v.detach().float().contiguous() for v in vps],
+                       [r.detach().float().contiguous() for r in rhos], want_energy)
+        for plan, (tr, en) in zip(prep.plans, res):
+            outs.append(engine.pack_output(plan, tr[0], tr[1], tr[2], en, None))
+        return outs
+    with_rho = any(r.requires_grad for r in rhos)
+    K = max(engine.choose_checkpoint_every(p, 1, checkpoint_every, snapshot_dtype, with_rho) for p in prep.plans)
+    # split the imaging-cache budget over the models in proportion to their steps
+    if imaging_cache in (0, None, False):
+        cached = [0] * len(prep.plans)
+    else:
+        per_step = [p.imaging_bytes(1, with_rho) for p in prep.plans]
+        if imaging_cache == "auto":
+            free, _ = torch.cuda.mem_get_info(device)
+            avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+            budget = int(avail * 0.5)
+        else:
+            budget = int(imaging_cache)
+        total = sum(p.geo.nt * b for p, b in zip(prep.plans, per_step))
+        frac = min(1.0, budget / max(total, 1))
+        cached = [int(frac * p.geo.nt) for p in prep.plans]
+    opts = dict(K=K, fmt=snapshot_dtype, with_rho=with_rho, want_energy=want_energy, cached=cached)
+    flat = _BatchFunction.apply(prep, opts, *vps, *rhos)
+    for i, plan in enumerate(prep.plans):
+        p, vx, vz, e0, e1, e2 = flat[6 * i:6 * i + 6]
+        en = [e0, e1, e2] if want_energy else None
+        outs.append(engine.pack_output(plan, p, vx, vz, en, None))
+    return outs
+
+
+class AcousticBatch:
+    """A fixed list of models, modelled together on every call."""
+
+    def __init__(self, models: Sequence[dict], fd_order: int = 8, device=None):
+        self.models = list(models)
+        self.fd_order = fd_order
+        self.device = device
+
+    def forward(self, vps=None, **kw) -> List[dict]:
+        models = self.models
+        if vps is not None:
+            models = [dict(m, vp=v) for m, v in zip(models, vps)]
+        return acoustic_forward_batched(models, fd_order=self.fd_order, device=self.device, **kw)
+
+    __call__ = forward

@@ -150,6 +150,32 @@ int gb_plan_set_profiling(gb_plan *plan, int enable);
 int gb_plan_profile(gb_plan *plan, double *ms_forward, double *ms_recompute, double *ms_adjoint,
                     long long *launches, long long *phase_steps);
 
+/* Batches of models (velocity particles of one ensemble, or unrelated models
+ * of uneven size and step count).  Every plan of a batch uses one stencil
+ * order, one free-surface setting and 16-row tiles; a gradient batch shares
+ * checkpoint_every, snapshot format and with_rho.  Each model keeps its own
+ * workspace (gb_plan_workspace_bytes as for the single-model calls) and
+ * outputs; the batch workspace holds the per-model descriptors and the work
+ * list.  One kernel launch per time step advances every model still running
+ * (replaces the serial per-particle forward_fn loop of
+ * geobrain/core/inverse.py:104-110). */
+typedef struct gb_model_io {
+    const float *vp, *rho, *damp, *wavelet;         /* as gb_forward */
+    float *trace_p, *trace_vx, *trace_vz;           /* forward outputs (may be NULL) */
+    float *energy_p, *energy_vx, *energy_vz;        /* forward outputs (may be NULL) */
+    const float *res_p, *res_vx, *res_vz;           /* backward inputs (may be NULL) */
+    float *grad_vp, *grad_rho;                      /* backward outputs */
+    const gb_grad_store *store;                     /* what the forward keeps (NULL: plain modelling) */
+    void *workspace;                                /* this model's workspace */
+    size_t workspace_bytes;
+} gb_model_io;
+
+size_t gb_batch_workspace_bytes(gb_plan *const *plans, int n_models);
+int gb_batch_forward(gb_plan *const *plans, int n_models, const gb_model_io *io,
+                     void *batch_workspace, size_t batch_workspace_bytes, void *stream);
+int gb_batch_backward(gb_plan *const *plans, int n_models, const gb_model_io *io,
+                      void *batch_workspace, size_t batch_workspace_bytes, void *stream);
+
 /* Synchronises `stream` and reports the device-side status word of a
  * workspace after gb_forward / gb_backward: GB_OK, or GB_E_TIMEOUT if a
  * bounded wait inside a kernel gave up. */
