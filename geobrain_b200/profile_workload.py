@@ -44,7 +44,7 @@ def main() -> None:
         K = w.nt
         ck = torch.empty(plan.checkpoint_bytes(K, "fp32"), dtype=torch.uint8, device=dev)
         store = engine.make_store(ck, K, "fp32", None, 0, False)
-        p, _, _, _, _ = engine.run_forward(plan, vp, rho, damp, src_v, want_energy=False, store=store)
+        p, _, _, _, _ = engine.run_forward(plan, vp, rho, damp, src_v, want_energy=args.energy, store=store)
         engine.run_backward(plan, vp, rho, damp, src_v, p, None, None, store, False)
     torch.cuda.synchronize()
     print("profile_workload: ok")
