@@ -4,9 +4,13 @@
 Workload (one "step" = one full gradient evaluation): the 400 x 1200 model,
 dx 10 m, dt 0.8 ms, 3000 time steps, 8th-order stencil, 30-cell PML, 32
 Ricker shots, 1200 receivers, L2 misfit on pressure against data modelled in
-the true model; forward with checkpoints, residual, hand-written adjoint,
-dL/dvp.  Metric: Gcell-updates/s, one unit = one (shot, padded cell, time
-step) forward update plus its adjoint update (recompute not counted).
+the true model; forward keeping the imaging fields (24-bit by default, so all
+3000 steps fit in HBM; checkpoints and recompute for whatever does not fit),
+residual, hand-written adjoint, dL/dvp.  Metric: Gcell-updates/s, one unit =
+one (shot, padded cell, time step) forward update plus its adjoint update
+(recompute not counted).  The gradient's relative L2 difference from the
+all-fp32 path (fp32 checkpoints, fp32 recompute, no cache) is measured once
+outside the timed region and reported.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -41,6 +45,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nt", type=int, default=3000, help="time steps of the workload (3000 = full)")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--imaging-dtype", default="fp24", choices=["fp32", "fp24", "bf16"],
+                    help="storage of the cached imaging fields")
     return ap.parse_args()
 
 
@@ -212,9 +218,10 @@ def main():
         d_obs = wave.acoustic_forward_kernel(vp=torch.tensor(w.vp_true, device=dev), rho=rho_t, want_energy=False,
                                              **common)["p"].contiguous()
 
-    def gradient_step(vp_dev, d_obs_dev):
+    def gradient_step(vp_dev, d_obs_dev, imaging_dtype=args.imaging_dtype, imaging_cache="auto"):
         vp = vp_dev.detach().requires_grad_(True)
-        out = wave.acoustic_forward_kernel(vp=vp, rho=rho_t, **common)
+        out = wave.acoustic_forward_kernel(vp=vp, rho=rho_t, imaging_dtype=imaging_dtype,
+                                           imaging_cache=imaging_cache, **common)
         res = out["p"] - d_obs_dev
         loss = 0.5 * (res * res).sum()
         loss.backward()
@@ -290,9 +297,13 @@ def main():
     per_step_rec = prof["recompute_ms"] / max(prof["recompute_steps"], 1)
     per_step_adj = prof["adjoint_ms"] / max(prof["adjoint_steps"], 1)
     cached_frac = 1.0 - prof["recompute_steps"] / max(prof["adjoint_steps"], 1)
-    b_fwd = S * cells * (24 + 8 / S)                              # fields r+w, a1 / a2 shared by the shots
-    b_rec = S * cells * (24 + 4 + 8 / S)                          # + imaging field written
-    b_adj = S * cells * (24 + 4 + 16 / S)                         # + imaging read, coefficients, gradient sums
+    eb = {"fp32": 4, "fp24": 3, "bf16": 2}[args.imaging_dtype]   # bytes per cached imaging value
+    # per time step: fields r+w, a1 / a2 shared by the shots; the forward
+    # writes the imaging field of cached steps, the recompute of the others;
+    # the adjoint reads it (cached or recomputed), coefficients, gradient sums
+    b_fwd = S * cells * (24 + 8 / S + eb * cached_frac)
+    b_rec = S * cells * (24 + 4 + 8 / S)
+    b_adj = S * cells * (24 + 16 / S + eb * cached_frac + 4 * (1 - cached_frac))
     kern = {
         "fwd_step (forward)": {"ms_per_launch": per_step_fwd, "bytes_per_launch": b_fwd},
         "fwd_step (recompute)": {"ms_per_launch": per_step_rec, "bytes_per_launch": b_rec},
@@ -318,9 +329,17 @@ def main():
                 else "fallback 6.65 TB/s",
                 "share_of_step": max(t_fwd, t_adj) / args.steps / ms_step, "traffic": ncu_traffic(tname)}
     grad_bytes = units / world * (56 + 16 / S)
-    grad_roof = {"algorithmic_bytes_per_unit": 56 + 16 / S,
+    grad_roof = {"algorithmic_bytes_per_unit": 56 + 16 / S, "kernels": "fwd_step + adj_step (+ recompute)",
                  "achieved": grad_bytes / (ms_step * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                  "frac": grad_bytes / (ms_step * 1e-3) / 1e9 / peak}
+
+    # accuracy of the timed configuration: gradient against the all-fp32 path
+    g_fast, _ = gradient_step(vp0, d_obs)
+    g_ref, _ = gradient_step(vp0, d_obs, imaging_dtype="fp32", imaging_cache=0)
+    grad_check = {"rel_l2_vs_fp32_storage": float(torch.linalg.vector_norm(g_fast - g_ref) /
+                                                  torch.linalg.vector_norm(g_ref)),
+                  "reference_path": "fp32 checkpoints, fp32 recompute of every step, no imaging cache"}
+    del g_fast, g_ref
 
     extras = {}
     if not args.no_extras and world == 1:
@@ -333,6 +352,7 @@ def main():
         "config": {"workload": "fwi_400x1200", "grid": [w.nz, w.nx], "nabc": w.nabc, "dx": w.dx, "dt": w.dt,
                    "nt": w.nt, "fd_order": w.fd_order, "n_shots_per_gpu": S, "n_receivers": int(w.rcv_x.size),
                    "misfit": "L2 on pressure", "checkpoints": "fp32, auto segment length",
+                   "imaging_cache": f"{args.imaging_dtype}, auto budget ({cached_frac:.0%} of steps cached)",
                    "l2": "inputs larger than L2 (fields 2 x 222 MB per state, no flush needed)",
                    "parallelism": f"shots{world}" if world > 1 else "single GPU"},
         "e2e": {"value": units / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
@@ -342,6 +362,7 @@ def main():
         "kernels": kern,
         "phase_ms_per_step": {k: prof[k] / args.steps for k in ("forward_ms", "recompute_ms", "adjoint_ms")},
         "imaging_cache_fraction": cached_frac,
+        "gradient_check": grad_check,
         "gpu_launches": int(prof["launches"]),
         "clocks": clocks,
         "cpu_baseline": cpu,

@@ -20,6 +20,7 @@ GB_E_TIMEOUT = -4
 GB_E_UNSUPPORTED = -5
 
 CKPT_FORMATS = {"fp32": 0, "bf16": 1, "fp16": 2}
+IMAGING_FORMATS = {"fp32": 0, "bf16": 1, "fp24": 3}
 
 
 class GbError(RuntimeError):
@@ -40,7 +41,8 @@ class ModelDesc(ctypes.Structure):
 
 class GradStore(ctypes.Structure):
     _fields_ = [("checkpoints", ctypes.c_void_p), ("checkpoint_every", ctypes.c_int32), ("format", ctypes.c_int32),
-                ("imaging", ctypes.c_void_p), ("cached_steps", ctypes.c_int32), ("with_rho", ctypes.c_int32)]
+                ("imaging", ctypes.c_void_p), ("cached_steps", ctypes.c_int32), ("with_rho", ctypes.c_int32),
+                ("imaging_format", ctypes.c_int32)]
 
 
 _P = ctypes.c_void_p
@@ -54,7 +56,7 @@ SIGNATURES = {
     "gb_plan_set_tiling": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_workspace_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_checkpoint_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
-    "gb_plan_imaging_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
+    "gb_plan_imaging_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gb_plan_set_group_streams": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P, _P, _SZ, _P]),
     "gb_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),

@@ -37,7 +37,8 @@ struct AdjArgs {
     const int4 *rcv_ent;                     // (padded z, padded x, receiver, 0)
     const float *res_p, *res_vx, *res_vz;    // [S][nt][n_rcv] or null
     const float *img;                        // [S][plane] I_n (and Jx, Jz planes after it when RHO)
-    long long img_field_stride;              // distance between the I, Jx, Jz blocks
+    long long img_field_stride;              // distance between the I, Jx, Jz blocks (elements)
+    int img_fmt;                             // storage format of the imaging fields (kImg*)
     float *G1, *C1, *G2, *C2;                // [n_groups][plane] sums and compensations
     int grp0, grp_count;             // shot groups this launch covers
     int *err;
@@ -53,11 +54,14 @@ __device__ __forceinline__ void neumaier_add(float &s, float &c, float x)
     s = t;
 }
 
-template <int R, int TZ, bool FS, bool RHO>
+// IMGF: storage format of the imaging fields (kImg*), or -1 to read it from
+// A.img_fmt at run time (batched launches, where it varies per model).
+template <int R, int TZ, bool FS, bool RHO, int IMGF>
 __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMap *mVX, const CUtensorMap *mVZ,
                                          const CUtensorMap *mA1, const CUtensorMap *mA2, const AdjArgs &A,
                                          const int group, const int tile)
 {
+    const int img_fmt = IMGF >= 0 ? IMGF : A.img_fmt;
     using G = Geo<R, TZ>;
     using SM = StepSmem<R, TZ>;
     const StepGeom &g = A.g;
@@ -115,16 +119,16 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
         const int s = s0 + k;
         const int b = k & 1;
         // imaging fields of this shot's tile cells: issued now, used in stage B
-        float4 im[G::LV], jx[G::LV], jz[G::LV];
+        ImgRaw im[G::LV], jx[G::LV], jz[G::LV];
 #pragma unroll
         for (int u = 0; u < G::LV; ++u) {
             const int gz = z0 + vb + u;
             const bool ok = vlane && u < vcnt && gz < g.Nz && gx0 < g.Nx;
-            const float *imp = A.img + (long long)s * g.plane + (long long)gz * g.pitch + gx0;
-            im[u] = ok ? ldg4(imp) : zero4();
+            const long long io = (long long)s * g.plane + (long long)gz * g.pitch + gx0;
+            im[u] = ok ? load_img_raw(A.img, io, img_fmt) : img_raw_zero();
             if (RHO) {
-                jx[u] = ok ? ldg4(imp + A.img_field_stride) : zero4();
-                jz[u] = ok ? ldg4(imp + 2 * A.img_field_stride) : zero4();
+                jx[u] = ok ? load_img_raw(A.img, io + A.img_field_stride, img_fmt) : img_raw_zero();
+                jz[u] = ok ? load_img_raw(A.img, io + 2 * A.img_field_stride, img_fmt) : img_raw_zero();
             }
         }
         if (!__syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1))) {
@@ -232,20 +236,23 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
                         const float4 vz1 = lds4(sVZ + (rv + 2 * R) * RW + 4 * lane);
                         const float4 a2 = lds4(sA2 + rv * RW + 4 * lane);
                         const long long o = (long long)gz * g.pitch + gx0;
+                        const float4 imv = decode_img4(im[u], img_fmt);
+                        const float4 jxv = RHO ? decode_img4(jx[u], img_fmt) : zero4();
+                        const float4 jzv = RHO ? decode_img4(jz[u], img_fmt) : zero4();
                         float4 vx, vz, pp;
                         if (fast) {
 #pragma unroll
                             for (int q = 0; q < 4; ++q) {
                                 at(vx, q) = __fmaf_rn(at(a2, q), Dx[q], at(vx1, q));
                                 at(vz, q) = __fmaf_rn(at(a2, q), Dz[q], at(vz1, q));
-                                at(acc1[u], q) = __fmaf_rn(at(mp1, q), at(im[u], q), at(acc1[u], q));
+                                at(acc1[u], q) = __fmaf_rn(at(mp1, q), at(imv, q), at(acc1[u], q));
                             }
                             pp = mp1;
                             if (RHO) {
 #pragma unroll
                                 for (int q = 0; q < 4; ++q) {
-                                    at(acc2[u], q) = __fmaf_rn(at(vx1, q), at(jx[u], q), at(acc2[u], q));
-                                    at(acc2[u], q) = __fmaf_rn(at(vz1, q), at(jz[u], q), at(acc2[u], q));
+                                    at(acc2[u], q) = __fmaf_rn(at(vx1, q), at(jxv, q), at(acc2[u], q));
+                                    at(acc2[u], q) = __fmaf_rn(at(vz1, q), at(jzv, q), at(acc2[u], q));
                                 }
                             }
                         } else {
@@ -264,7 +271,7 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
                                     const int gx = gx0 + q;
                                     if (vx_row && gx >= g.vx_c0 && gx <= g.vx_c1) {
                                         at(vx, q) = __fmaf_rn(at(a2, q), Dx[q], (1.f - at(k2, q)) * at(vx1, q));
-                                        if (RHO) at(acc2[u], q) = __fmaf_rn(at(vx1, q), at(jx[u], q), at(acc2[u], q));
+                                        if (RHO) at(acc2[u], q) = __fmaf_rn(at(vx1, q), at(jxv, q), at(acc2[u], q));
                                     }
                                     if (vz_row && gx >= g.vz_c0 && gx <= g.vz_c1) {
                                         float d = Dz[q];
@@ -274,7 +281,7 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
                                             for (int kk = 0; kk < R; ++kk) d = __fmaf_rn(g.c[kk], at(wp[u + R - 1 + kk], q), d);
                                         }
                                         at(vz, q) = __fmaf_rn(at(a2, q), d, (1.f - at(k3, q)) * at(vz1, q));
-                                        if (RHO) at(acc2[u], q) = __fmaf_rn(at(vz1, q), at(jz[u], q), at(acc2[u], q));
+                                        if (RHO) at(acc2[u], q) = __fmaf_rn(at(vz1, q), at(jzv, q), at(acc2[u], q));
                                     }
                                 }
                             }
@@ -285,7 +292,7 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
                                     const int gx = gx0 + q;
                                     if (gx >= g.p_c0 && gx <= g.p_c1) {
                                         at(pp, q) = (1.f - at(k1, q)) * at(mp1, q);
-                                        at(acc1[u], q) = __fmaf_rn(at(mp1, q), at(im[u], q), at(acc1[u], q));
+                                        at(acc1[u], q) = __fmaf_rn(at(mp1, q), at(imv, q), at(acc1[u], q));
                                     }
                                 }
                             }
@@ -327,7 +334,7 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
     }
 }
 
-template <int R, int TZ, bool FS, bool RHO>
+template <int R, int TZ, bool FS, bool RHO, int IMGF>
 __global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
 adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mVX,
                 const __grid_constant__ CUtensorMap mVZ, const __grid_constant__ CUtensorMap mA1,
@@ -335,7 +342,7 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
 {
     const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
     const int tile = (int)(blockIdx.x / A.grp_count);
-    adj_body<R, TZ, FS, RHO>(&mP, &mVX, &mVZ, &mA1, &mA2, A, group, tile);
+    adj_body<R, TZ, FS, RHO, IMGF>(&mP, &mVX, &mVZ, &mA1, &mA2, A, group, tile);
 }
 
 template <int R, int TZ>

@@ -30,10 +30,18 @@ struct BatchModel {
     float *fld[2];           // forward state levels
     float *mu[2];            // adjoint state levels
     float *cache;            // imaging cache of steps >= t_cache, or null
-    float *segimg;           // imaging fields of the segment being recomputed
-    long long step_img;      // floats per step of imaging fields
+    float *segimg;           // imaging fields of the segment being recomputed (fp32)
+    long long step_img;      // elements per step of imaging fields
     int nt, t_cache, K;
+    int cache_fmt;           // storage format of the cache (kImg*)
 };
+
+// Step `j` of the imaging cache (elements of 2, 3 or 4 bytes).
+__device__ __forceinline__ float *cache_step(const BatchModel &M, int j)
+{
+    const int es = M.cache_fmt == kImgBF16 ? 2 : M.cache_fmt == kImgF24 ? 3 : 4;
+    return reinterpret_cast<float *>(reinterpret_cast<char *>(M.cache) + (long long)j * M.step_img * es);
+}
 
 constexpr int kBatchForward = 0;
 constexpr int kBatchRecompute = 1;
@@ -54,9 +62,11 @@ fwd_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ 
         A.it = tau;
         A.out = M.fld[par ^ 1];
         if (mode == kBatchForward) {
-            A.imaging = (M.cache && tau >= M.t_cache) ? M.cache + (long long)(tau - M.t_cache) * M.step_img : nullptr;
+            A.imaging = (M.cache && tau >= M.t_cache) ? cache_step(M, tau - M.t_cache) : nullptr;
+            A.img_fmt = M.cache_fmt;
         } else {
             A.imaging = M.segimg + (long long)(tau - t0) * M.step_img;
+            A.img_fmt = 0;
             A.energy = nullptr;
             A.tr_p = A.tr_vx = A.tr_vz = nullptr;
         }
@@ -81,12 +91,13 @@ adj_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ 
         A = M.a;
         A.it = tau;
         A.out = M.mu[par ^ 1];
-        A.img = (M.cache && tau >= M.t_cache) ? M.cache + (long long)(tau - M.t_cache) * M.step_img
-                                              : M.segimg + (long long)(tau - (tau / M.K) * M.K) * M.step_img;
+        const bool cached = M.cache && tau >= M.t_cache;
+        A.img = cached ? cache_step(M, tau - M.t_cache) : M.segimg + (long long)(tau - (tau / M.K) * M.K) * M.step_img;
+        A.img_fmt = cached ? M.cache_fmt : 0;
     }
     __syncthreads();
     const BatchMaps &mp = maps[item.x];
-    adj_body<R, TZ, FS, RHO>(&mp.mu[par][0], &mp.mu[par][1], &mp.mu[par][2], &mp.a1, &mp.a2, A, item.z, item.y);
+    adj_body<R, TZ, FS, RHO, -1>(&mp.mu[par][0], &mp.mu[par][1], &mp.mu[par][2], &mp.a1, &mp.a2, A, item.z, item.y);
 }
 
 }  // namespace gb

@@ -322,22 +322,34 @@ StepKernel fwd_kernel(int R, int tz, bool fs, bool en, int im)
     return k;
 }
 
-template <int R, int TZ>
-void *adj_pick(bool fs, bool rho)
+template <int R, int TZ, int IMGF>
+void *adj_pick_f(bool fs, bool rho)
 {
-    if (fs) return rho ? reinterpret_cast<void *>(&adj_step_kernel<R, TZ, true, true>)
-                       : reinterpret_cast<void *>(&adj_step_kernel<R, TZ, true, false>);
-    return rho ? reinterpret_cast<void *>(&adj_step_kernel<R, TZ, false, true>)
-               : reinterpret_cast<void *>(&adj_step_kernel<R, TZ, false, false>);
+    if (fs) return rho ? reinterpret_cast<void *>(&adj_step_kernel<R, TZ, true, true, IMGF>)
+                       : reinterpret_cast<void *>(&adj_step_kernel<R, TZ, true, false, IMGF>);
+    return rho ? reinterpret_cast<void *>(&adj_step_kernel<R, TZ, false, true, IMGF>)
+               : reinterpret_cast<void *>(&adj_step_kernel<R, TZ, false, false, IMGF>);
 }
 
-StepKernel adj_kernel(int R, int tz, bool fs, bool rho)
+// The default 16-row tiles get one kernel per imaging format (the loads are
+// issued early, ahead of the stage wait, and a format switch there costs);
+// the 32-row tiles read the format at run time.
+template <int R, int TZ>
+void *adj_pick(bool fs, bool rho, int img_fmt)
+{
+    if (TZ != 16) return adj_pick_f<R, TZ, -1>(fs, rho);
+    if (img_fmt == GB_IMG_BF16) return adj_pick_f<R, TZ, kImgBF16>(fs, rho);
+    if (img_fmt == GB_IMG_F24) return adj_pick_f<R, TZ, kImgF24>(fs, rho);
+    return adj_pick_f<R, TZ, kImgF32>(fs, rho);
+}
+
+StepKernel adj_kernel(int R, int tz, bool fs, bool rho, int img_fmt)
 {
     StepKernel k{nullptr, 0};
-    if (R == 2 && tz == 32) { k.fn = adj_pick<2, 32>(fs, rho); k.smem = adj_smem_bytes<2, 32>(); }
-    if (R == 2 && tz == 16) { k.fn = adj_pick<2, 16>(fs, rho); k.smem = adj_smem_bytes<2, 16>(); }
-    if (R == 4 && tz == 32) { k.fn = adj_pick<4, 32>(fs, rho); k.smem = adj_smem_bytes<4, 32>(); }
-    if (R == 4 && tz == 16) { k.fn = adj_pick<4, 16>(fs, rho); k.smem = adj_smem_bytes<4, 16>(); }
+    if (R == 2 && tz == 32) { k.fn = adj_pick<2, 32>(fs, rho, img_fmt); k.smem = adj_smem_bytes<2, 32>(); }
+    if (R == 2 && tz == 16) { k.fn = adj_pick<2, 16>(fs, rho, img_fmt); k.smem = adj_smem_bytes<2, 16>(); }
+    if (R == 4 && tz == 32) { k.fn = adj_pick<4, 32>(fs, rho, img_fmt); k.smem = adj_smem_bytes<4, 32>(); }
+    if (R == 4 && tz == 16) { k.fn = adj_pick<4, 16>(fs, rho, img_fmt); k.smem = adj_smem_bytes<4, 16>(); }
     return k;
 }
 
@@ -555,6 +567,18 @@ int common_setup(gb_plan *P, const Layout &L, char *ws, const float *vp, const f
 
 char *aligned_ws(void *workspace) { return reinterpret_cast<char *>(align256(reinterpret_cast<uintptr_t>(workspace))); }
 
+bool img_format_ok(int f) { return f == GB_IMG_F32 || f == GB_IMG_BF16 || f == GB_IMG_F24; }
+size_t img_esize(int f) { return f == GB_IMG_BF16 ? 2 : f == GB_IMG_F24 ? 3 : 4; }
+static_assert(GB_IMG_F32 == kImgF32 && GB_IMG_BF16 == kImgBF16 && GB_IMG_F24 == kImgF24,
+              "imaging format codes of the header and the kernels agree");
+
+// Element `e` of an imaging buffer whose elements are esize bytes, as the
+// float pointer the kernels take (they widen the short formats themselves).
+float *img_at(void *base, size_t e, size_t esize)
+{
+    return reinterpret_cast<float *>(reinterpret_cast<char *>(base) + e * esize);
+}
+
 int check_store(const gb_plan *P, const gb_grad_store *store)
 {
     if (!store) return GB_OK;
@@ -562,6 +586,8 @@ int check_store(const gb_plan *P, const gb_grad_store *store)
     if (store->format < GB_CKPT_F32 || store->format > GB_CKPT_F16) return fail(GB_E_ARG, "unknown checkpoint format");
     if (store->cached_steps < 0 || store->cached_steps > P->d.nt) return fail(GB_E_ARG, "cached_steps out of range");
     if (store->cached_steps > 0 && !store->imaging) return fail(GB_E_ARG, "cached_steps > 0 needs an imaging buffer");
+    if (!img_format_ok(store->imaging_format))
+        return fail(GB_E_ARG, "imaging_format must be GB_IMG_F32, GB_IMG_BF16 or GB_IMG_F24");
     if (store->cached_steps < P->d.nt && !store->checkpoints) return fail(GB_E_ARG, "checkpoint storage missing");
     return GB_OK;
 }
@@ -670,10 +696,11 @@ size_t gb_plan_checkpoint_bytes(const gb_plan *p, int checkpoint_every, int ckpt
     return n_ck * ck_bytes(p, ckpt_format);
 }
 
-size_t gb_plan_imaging_bytes(const gb_plan *p, int cached_steps, int with_rho)
+size_t gb_plan_imaging_bytes(const gb_plan *p, int cached_steps, int with_rho, int imaging_format)
 {
     if (!p || cached_steps < 0) return 0;
-    return (size_t)cached_steps * (with_rho ? 3 : 1) * p->d.n_shots * p->plane * 4;
+    if (!img_format_ok(imaging_format)) return 0;
+    return (size_t)cached_steps * (with_rho ? 3 : 1) * p->d.n_shots * p->plane * img_esize(imaging_format);
 }
 
 int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp, const float *wavelet,
@@ -726,7 +753,9 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
     A.tr_p = trace_p; A.tr_vx = trace_vx; A.tr_vz = trace_vz;
     A.energy = want_energy ? energy : nullptr;
     A.img_field_stride = (long long)S * P->plane;
+    A.img_fmt = store ? store->imaging_format : GB_IMG_F32;
     A.err = Su.err;
+    const size_t img_es = store ? img_esize(store->imaging_format) : 4;
 
     GroupStreams gs;
     if (int rc = group_streams(P, st, &gs)) return rc;
@@ -739,7 +768,7 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
         A.it = it;
         A.out = buf[b ^ 1];
         const bool keep = store && it >= t_cache;
-        A.imaging = keep ? reinterpret_cast<float *>(store->imaging) + (size_t)(it - t_cache) * step_img : nullptr;
+        A.imaging = keep ? img_at(store->imaging, (size_t)(it - t_cache) * step_img, img_es) : nullptr;
         for (int i = 0; i < gs.n; ++i) {
             int g0, gc;
             launch_groups(gs, i, P->n_groups, &g0, &gc);
@@ -785,7 +814,9 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     const int K = std::min<int>(store->checkpoint_every, d.nt);
     const bool rho_fields = store->with_rho != 0;
     const int with_grad = rho_fields ? 2 : 1;
-    const Layout L = layout(P, with_grad, K);
+    // recompute segments lie in [0, nt - cached_steps): the segment buffer
+    // holds at most that many steps
+    const Layout L = layout(P, with_grad, std::max(1, std::min(K, d.nt - store->cached_steps)));
     char *ws = aligned_ws(workspace);
     if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
         return fail(GB_E_WORKSPACE, "workspace too small");
@@ -815,9 +846,11 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
 
     const bool fs = d.free_surface != 0;
     const StepKernel KF = fwd_kernel(P->R, P->tz, fs, false, rho_fields ? 2 : 1);
-    const StepKernel KA = adj_kernel(P->R, P->tz, fs, rho_fields);
+    const StepKernel KA = adj_kernel(P->R, P->tz, fs, rho_fields, GB_IMG_F32);            // recomputed segments
+    const StepKernel KC = adj_kernel(P->R, P->tz, fs, rho_fields, store->imaging_format);  // cached steps
     if (int rc = prepare_kernel(KF)) return rc;
     if (int rc = prepare_kernel(KA)) return rc;
+    if (int rc = prepare_kernel(KC)) return rc;
     Maps fmaps[2], amaps[2];
     for (int b = 0; b < 2; ++b) {
         if (int rc = make_maps(P, fb[b], Su.a1, Su.a2, &fmaps[b])) return rc;
@@ -851,18 +884,20 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     int cur = 0;   // adjoint state lives in mu[cur]
 
     // adjoint sweep over [t0, t1) in reverse, imaging fields at img_base[(it - t0)]
-    auto adjoint_sweep = [&](int t0, int t1, const float *img_base) -> int {
+    auto adjoint_sweep = [&](int t0, int t1, void *img_base, int img_fmt) -> int {
         P->mark(2, true, st);
         P->phase_steps[2] += t1 - t0;
         if (int rc = fork(gs)) return rc;
         for (int it = t1 - 1; it >= t0; --it) {
             A.it = it;
             A.out = mu[cur ^ 1];
-            A.img = img_base + (size_t)(it - t0) * step_img;
+            A.img = img_at(img_base, (size_t)(it - t0) * step_img, img_esize(img_fmt));
+            A.img_fmt = img_fmt;
             for (int i = 0; i < gs.n; ++i) {
                 int g0, gc;
                 launch_groups(gs, i, P->n_groups, &g0, &gc);
-                if (int rc = launch_step(P, KA, amaps[cur], A, g0, gc, gs.at(i))) return rc;
+                if (int rc = launch_step(P, img_fmt == GB_IMG_F32 ? KA : KC, amaps[cur], A, g0, gc, gs.at(i)))
+                    return rc;
             }
             cur ^= 1;
         }
@@ -873,7 +908,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
 
     // 1. steps whose imaging fields the forward kept
     if (store->cached_steps > 0)
-        if (int rc = adjoint_sweep(t_cache, d.nt, reinterpret_cast<const float *>(store->imaging))) return rc;
+        if (int rc = adjoint_sweep(t_cache, d.nt, store->imaging, store->imaging_format)) return rc;
     // 2. earlier steps, one checkpoint segment at a time: fp32 recompute from
     //    the checkpoint (writing the imaging fields), then the adjoint sweep
     const int n_seg = (t_cache + K - 1) / K;
@@ -902,7 +937,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
         }
         if (int rc = join(gs)) return rc;
         P->mark(1, false, st);
-        if (int rc = adjoint_sweep(t0, t1, wimg)) return rc;
+        if (int rc = adjoint_sweep(t0, t1, wimg, GB_IMG_F32)) return rc;
     }
     grad_finish_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, G1, C1, G2, C2, P->n_groups, P->plane, d.nz, d.nx, d.nabc,
                                                 P->pitch, grad_vp, grad_rho);
@@ -1111,7 +1146,7 @@ int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *
     std::vector<BatchModel> models(n);
     std::vector<BatchMaps> maps(n);
     bool any_energy = false, any_cache = false, rho = false;
-    int maxnt = 0, K = 0;
+    int maxnt = 0;
     P0->mark(0, true, st);
     for (int m = 0; m < n; ++m) {
         gb_plan *P = plans[m];
@@ -1148,6 +1183,7 @@ int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *
         M.K = sto ? std::min<int>(sto->checkpoint_every, P->d.nt) : P->d.nt;
         M.t_cache = sto ? P->d.nt - sto->cached_steps : P->d.nt;
         M.cache = sto && sto->cached_steps > 0 ? reinterpret_cast<float *>(sto->imaging) : nullptr;
+        M.cache_fmt = sto ? sto->imaging_format : GB_IMG_F32;
         M.step_img = (long long)((sto && sto->with_rho) ? 3 : 1) * S * P->plane;
         if (int rc = make_state_maps(P, buf0, maps[m].fld[0])) return rc;
         if (int rc = make_state_maps(P, buf1, maps[m].fld[1])) return rc;
@@ -1157,7 +1193,6 @@ int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *
         any_cache |= M.cache != nullptr;
         rho |= sto && sto->with_rho;
         maxnt = std::max(maxnt, M.nt);
-        K = M.K;
     }
     if (int rc = upload_batch(plans, n, models, maps, bws, B, st)) return rc;
     const StepKernel K0 = fwd_batch_kernel_for(P0->R, fs, any_energy, any_cache ? (rho ? 2 : 1) : 0);
@@ -1196,7 +1231,6 @@ int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *
                 ++P0->launches;
             }
     }
-    (void)K;
     P0->mark(0, false, st);
     return GB_OK;
 }
@@ -1276,6 +1310,7 @@ int gb_batch_backward(gb_plan *const *plans, int n, const gb_model_io *io, void 
         M.K = Km;
         M.t_cache = P->d.nt - x.store->cached_steps;
         M.cache = x.store->cached_steps > 0 ? reinterpret_cast<float *>(x.store->imaging) : nullptr;
+        M.cache_fmt = x.store->imaging_format;
         M.segimg = reinterpret_cast<float *>(ws + L.img);
         M.step_img = (long long)(rho ? 3 : 1) * S * P->plane;
         if (int rc = make_state_maps(P, M.fld[0], maps[m].fld[0])) return rc;

@@ -131,6 +131,79 @@ __device__ __forceinline__ float at(const float4 &v, int q)
     return reinterpret_cast<const float *>(&v)[q];
 }
 
+// Storage formats of the imaging fields kept for the adjoint (the values of
+// GB_IMG_* in the C header):
+//   kImgF32   fp32;
+//   kImgBF16  bf16, the upper 16 bits of the fp32 rounded to nearest even;
+//   kImgF24   the upper 24 bits of the fp32 (sign, 8-bit exponent, 15-bit
+//             mantissa) rounded to nearest even, 3 bytes, packed 4 values to
+//             3 words.
+// Both short formats keep the fp32 exponent, so no scale is needed and
+// widening back is exact.  `o` is an element offset, a multiple of 4.
+constexpr int kImgF32 = 0;
+constexpr int kImgBF16 = 1;
+constexpr int kImgF24 = 3;
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
+{
+    uint32_t r;
+    asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+// fp32 -> upper 24 bits, round to nearest even on the 8 dropped bits (a carry
+// into the exponent is the correct rounding up to the next binade).
+__device__ __forceinline__ uint32_t round24(float x)
+{
+    const uint32_t u = __float_as_uint(x);
+    return (u + 0x7fu + ((u >> 8) & 1u)) >> 8;
+}
+__device__ __forceinline__ void store_img4(float *base, long long o, int fmt, float4 v)
+{
+    if (fmt == kImgBF16) {
+        uint2 u = make_uint2(pack_bf16x2(v.x, v.y), pack_bf16x2(v.z, v.w));
+        *reinterpret_cast<uint2 *>(reinterpret_cast<uint16_t *>(base) + o) = u;
+    } else if (fmt == kImgF24) {
+        const uint32_t t0 = round24(v.x), t1 = round24(v.y), t2 = round24(v.z), t3 = round24(v.w);
+        uint32_t *w = reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(base) + 3 * o);
+        w[0] = t0 | (t1 << 24);
+        w[1] = (t1 >> 8) | (t2 << 16);
+        w[2] = (t2 >> 16) | (t3 << 8);
+    } else {
+        stg4(base + o, v);
+    }
+}
+// Imaging values as loaded: 4 fp32 words, 2 bf16x2 words or 3 packed fp24
+// words.  Loading and widening are separate so that the loads can be issued
+// well ahead of the use without the widening waiting on them.
+struct ImgRaw {
+    uint32_t w0, w1, w2, w3;
+};
+__device__ __forceinline__ ImgRaw img_raw_zero() { return ImgRaw{0u, 0u, 0u, 0u}; }
+__device__ __forceinline__ ImgRaw load_img_raw(const float *base, long long o, int fmt)
+{
+    if (fmt == kImgBF16) {
+        const uint2 u = __ldg(reinterpret_cast<const uint2 *>(reinterpret_cast<const uint16_t *>(base) + o));
+        return ImgRaw{u.x, u.y, 0u, 0u};
+    }
+    if (fmt == kImgF24) {
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(reinterpret_cast<const char *>(base) + 3 * o);
+        return ImgRaw{__ldg(w), __ldg(w + 1), __ldg(w + 2), 0u};
+    }
+    const uint4 u = __ldg(reinterpret_cast<const uint4 *>(base + o));
+    return ImgRaw{u.x, u.y, u.z, u.w};
+}
+// All-zero words widen to 0.0 in every format.
+__device__ __forceinline__ float4 decode_img4(const ImgRaw &r, int fmt)
+{
+    if (fmt == kImgBF16)
+        return make_float4(__uint_as_float(r.w0 << 16), __uint_as_float(r.w0 & 0xffff0000u),
+                           __uint_as_float(r.w1 << 16), __uint_as_float(r.w1 & 0xffff0000u));
+    if (fmt == kImgF24)
+        return make_float4(__uint_as_float(r.w0 << 8), __uint_as_float(((r.w0 >> 24) | (r.w1 << 8)) << 8),
+                           __uint_as_float(((r.w1 >> 16) | (r.w2 << 16)) << 8), __uint_as_float(r.w2 & 0xffffff00u));
+    return make_float4(__uint_as_float(r.w0), __uint_as_float(r.w1), __uint_as_float(r.w2), __uint_as_float(r.w3));
+}
+
 __device__ __forceinline__ void red_add_v4(float *p, float4 v)
 {
     asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(v.x), "f"(v.y), "f"(v.z),

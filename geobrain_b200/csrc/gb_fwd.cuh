@@ -52,7 +52,8 @@ struct FwdArgs {
     float *tr_p, *tr_vx, *tr_vz;     // [S][nt][n_rcv] or null
     float *energy;                   // [3][plane] padded accumulators or null
     float *imaging;                  // [S][plane] -div(v) on the p mask, or null
-    long long img_field_stride;      // IMG == 2: dx(p), dz(p) blocks follow at this stride
+    long long img_field_stride;      // IMG == 2: dx(p), dz(p) blocks follow at this stride (elements)
+    int img_fmt;                     // storage format of the imaging fields (kImg*)
     int grp0, grp_count;             // shot groups this launch covers
     int *err;
 };
@@ -204,8 +205,8 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
 #pragma unroll
                         for (int q = 0; q < 4; ++q) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], at(pv, q));
                         if (tile_cell && A.imaging)
-                            stg4(A.imaging + (long long)s * g.plane + (long long)gz * g.pitch + gx0,
-                                 make_float4(-D[0], -D[1], -D[2], -D[3]));
+                            store_img4(A.imaging, (long long)s * g.plane + (long long)gz * g.pitch + gx0,
+                                       A.img_fmt, make_float4(-D[0], -D[1], -D[2], -D[3]));
                     } else {
                         const bool row_in = gz >= g.p_r0 && gz <= g.p_r1;
                         if (row_in && (gx0 + 3 >= g.p_c0) && (gx0 <= g.p_c1)) {
@@ -220,7 +221,8 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                                 at(img, q) = m ? -D[q] : 0.f;
                                 if (m) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], (1.f - at(k1, q)) * at(pv, q));
                             }
-                            if (tile_cell && A.imaging) stg4(A.imaging + (long long)s * g.plane + o, img);
+                            if (tile_cell && A.imaging)
+                                store_img4(A.imaging, (long long)s * g.plane + o, A.img_fmt, img);
                         }
                     }
                     if (gz == sz && sx >= gx0 && sx < gx0 + 4) {
@@ -302,8 +304,9 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                             }
                         }
                         if (IMG == 2 && A.imaging) {
-                            stg4(A.imaging + (long long)s * g.plane + A.img_field_stride + o, jx);
-                            stg4(A.imaging + (long long)s * g.plane + 2 * A.img_field_stride + o, jz);
+                            store_img4(A.imaging, (long long)s * g.plane + A.img_field_stride + o, A.img_fmt, jx);
+                            store_img4(A.imaging, (long long)s * g.plane + 2 * A.img_field_stride + o, A.img_fmt,
+                                       jz);
                         }
                         float *outs = A.out + (long long)s * 3 * g.plane + o;
                         stg4(outs, pv);

@@ -106,15 +106,15 @@ class _BatchFunction(torch.autograd.Function):
         vps = [p.detach().to(torch.float32).contiguous() for p in params[:n]]
         rhos = [p.detach().to(torch.float32).contiguous() for p in params[n:]]
         dev = prep.device
-        K, fmt, with_rho = opts["K"], opts["fmt"], opts["with_rho"]
+        K, fmt, with_rho, ifmt = opts["K"], opts["fmt"], opts["with_rho"], opts["imaging_fmt"]
         stores, keep = [], []
         for i, plan in enumerate(prep.plans):
             cached = opts["cached"][i]
             n_ck = -(-(plan.geo.nt - cached) // min(K, plan.geo.nt))
             ck = torch.empty(max(n_ck * plan.checkpoint_bytes(plan.geo.nt, fmt), 256), dtype=torch.uint8, device=dev)
-            img = torch.empty(max(plan.imaging_bytes(cached, with_rho), 256), dtype=torch.uint8, device=dev)
+            img = torch.empty(max(plan.imaging_bytes(cached, with_rho, ifmt), 256), dtype=torch.uint8, device=dev)
             stores.append(engine.make_store(ck if n_ck > 0 else None, min(K, plan.geo.nt), fmt,
-                                            img if cached > 0 else None, cached, with_rho))
+                                            img if cached > 0 else None, cached, with_rho, ifmt))
             keep.append((ck, img))
         outs = _forward(prep, vps, rhos, opts["want_energy"], stores)
         ctx.prep, ctx.opts, ctx.stores, ctx.keep = prep, opts, stores, keep
@@ -170,7 +170,7 @@ class _BatchFunction(torch.autograd.Function):
 
 def acoustic_forward_batched(models: Sequence[dict], *, fd_order: int = 8, device=None, want_energy: bool = True,
                              checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
-                             imaging_cache="auto") -> List[dict]:
+                             imaging_cache="auto", imaging_dtype: str = "fp32") -> List[dict]:
     """Forward-model every model of `models` together; see the module doc."""
     if fd_order not in engine.FD_ORDERS:
         raise ValueError(f"fd_order must be one of {sorted(engine.FD_ORDERS)}")
@@ -199,7 +199,9 @@ def acoustic_forward_batched(models: Sequence[dict], *, fd_order: int = 8, devic
     if imaging_cache in (0, None, False):
         cached = [0] * len(prep.plans)
     else:
-        per_step = [p.imaging_bytes(1, with_rho) for p in prep.plans]
+        if imaging_dtype not in _lib.IMAGING_FORMATS:
+            raise ValueError(f"imaging_dtype must be one of {sorted(_lib.IMAGING_FORMATS)}")
+        per_step = [p.imaging_bytes(1, with_rho, imaging_dtype) for p in prep.plans]
         if imaging_cache == "auto":
             free, _ = torch.cuda.mem_get_info(device)
             avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
@@ -209,7 +211,8 @@ def acoustic_forward_batched(models: Sequence[dict], *, fd_order: int = 8, devic
         total = sum(p.geo.nt * b for p, b in zip(prep.plans, per_step))
         frac = min(1.0, budget / max(total, 1))
         cached = [int(frac * p.geo.nt) for p in prep.plans]
-    opts = dict(K=K, fmt=snapshot_dtype, with_rho=with_rho, want_energy=want_energy, cached=cached)
+    opts = dict(K=K, fmt=snapshot_dtype, with_rho=with_rho, want_energy=want_energy, cached=cached,
+                imaging_fmt=imaging_dtype)
     flat = _BatchFunction.apply(prep, opts, *vps, *rhos)
     for i, plan in enumerate(prep.plans):
         p, vx, vz, e0, e1, e2 = flat[6 * i:6 * i + 6]

@@ -95,8 +95,9 @@ class Plan:
     def checkpoint_bytes(self, checkpoint_every: int, fmt: str) -> int:
         return int(self._lib.gb_plan_checkpoint_bytes(self.h, int(checkpoint_every), _lib.CKPT_FORMATS[fmt]))
 
-    def imaging_bytes(self, cached_steps: int, with_rho: bool = False) -> int:
-        return int(self._lib.gb_plan_imaging_bytes(self.h, int(cached_steps), int(bool(with_rho))))
+    def imaging_bytes(self, cached_steps: int, with_rho: bool = False, fmt: str = "fp32") -> int:
+        return int(self._lib.gb_plan_imaging_bytes(self.h, int(cached_steps), int(bool(with_rho)),
+                                                   _lib.IMAGING_FORMATS[fmt]))
 
     def set_group_streams(self, enable: bool) -> None:
         _lib.check(self._lib.gb_plan_set_group_streams(self.h, int(enable)))
@@ -130,9 +131,10 @@ def stream_handle(device) -> int:
 
 
 def make_store(checkpoints: Optional[torch.Tensor], checkpoint_every: int, fmt: str,
-               imaging: Optional[torch.Tensor], cached_steps: int, with_rho: bool) -> "_lib.GradStore":
+               imaging: Optional[torch.Tensor], cached_steps: int, with_rho: bool,
+               imaging_fmt: str = "fp32") -> "_lib.GradStore":
     return _lib.GradStore(_lib.ptr(checkpoints), int(checkpoint_every), _lib.CKPT_FORMATS[fmt], _lib.ptr(imaging),
-                          int(cached_steps), int(bool(with_rho)))
+                          int(cached_steps), int(bool(with_rho)), _lib.IMAGING_FORMATS[imaging_fmt])
 
 
 def run_forward(plan: Plan, vp: torch.Tensor, rho: torch.Tensor, damp: torch.Tensor, src_v: torch.Tensor, *,
@@ -190,23 +192,49 @@ def choose_checkpoint_every(plan: Plan, checkpoint_segments: int = 1, checkpoint
     return max(1, min(k, nt))
 
 
-def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device) -> int:
+def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device, imaging_fmt: str = "fp32",
+                        checkpoint_every: int = 1, ckpt_fmt: str = "fp32") -> int:
     """How many of the last time steps keep their imaging fields from the
-    forward (those steps skip the recompute).  imaging_cache: 'auto' (up to
-    60 % of the device memory available right now, counting blocks the
-    caching allocator holds unused; GEOBRAIN_B200_IMAGING_CACHE_BYTES
-    overrides), a byte budget, or 0."""
-    per = plan.imaging_bytes(1, with_rho)
+    forward (those steps skip the recompute).  imaging_cache: a byte budget,
+    0, or 'auto': the most steps for which the cache, the checkpoints of the
+    remaining steps, the workspaces, the trace gradients and a margin (2 GiB
+    + 5 %) fit in the device memory available right now, counting blocks the
+    caching allocator holds unused (GEOBRAIN_B200_IMAGING_CACHE_BYTES
+    overrides it with a byte budget)."""
+    nt = plan.geo.nt
+    per = max(plan.imaging_bytes(1, with_rho, imaging_fmt), 1)
     if imaging_cache in (None, 0, False):
         return 0
-    if imaging_cache == "auto":
-        free, _ = torch.cuda.mem_get_info(device)
-        # blocks torch's allocator holds but does not use are free for this too
-        avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
-        budget = int(os.environ.get("GEOBRAIN_B200_IMAGING_CACHE_BYTES", int(avail * 0.6)))
-    else:
-        budget = int(imaging_cache)
-    return int(max(0, min(plan.geo.nt, budget // max(per, 1))))
+    if imaging_cache != "auto":
+        return int(max(0, min(nt, int(imaging_cache) // per)))
+    env = os.environ.get("GEOBRAIN_B200_IMAGING_CACHE_BYTES")
+    if env is not None:
+        return int(max(0, min(nt, int(env) // per)))
+    free, _ = torch.cuda.mem_get_info(device)
+    # blocks torch's allocator holds but does not use are free for this too
+    avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+    K = max(1, min(int(checkpoint_every), nt))
+    one_ck = plan.checkpoint_bytes(nt, ckpt_fmt)                      # one stored state
+    fixed = 3 * plan.n_shots * nt * plan.n_rcv * 4 + (2 << 30) + avail // 20
+
+    def need(c: int) -> int:
+        rest = nt - c
+        seg = max(1, min(K, rest))
+        return (c * per + -(-rest // K) * one_ck + plan.workspace_bytes(2 if with_rho else 1, seg) +
+                plan.workspace_bytes(0, 0) + fixed)
+
+    if need(nt) <= avail:                # no recompute at all (no segment buffer either)
+        return nt
+    if need(0) > avail:
+        return 0
+    lo, hi = 0, nt                       # largest c with need(c) <= avail; every lo kept fits
+    while lo < hi:
+        mid = (lo + hi + 1) // 2
+        if need(mid) <= avail:
+            lo = mid
+        else:
+            hi = mid - 1
+    return int(lo)
 
 
 def run_backward(plan: Plan, vp, rho, damp, src_v, res_p, res_vx, res_vz, store: "_lib.GradStore",
@@ -215,7 +243,8 @@ def run_backward(plan: Plan, vp, rho, damp, src_v, res_p, res_vx, res_vz, store:
     dev = vp.device
     grad_vp = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32)
     grad_rho = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32) if want_rho else None
-    ws = workspace(plan.workspace_bytes(2 if store.with_rho else 1, store.checkpoint_every), dev)
+    seg = max(1, min(store.checkpoint_every, g.nt - store.cached_steps))    # steps of one recompute segment
+    ws = workspace(plan.workspace_bytes(2 if store.with_rho else 1, seg), dev)
     with torch.cuda.device(dev):
         rc = plan._lib.gb_backward(plan.h, vp.data_ptr(), rho.data_ptr(), damp.data_ptr(), src_v.data_ptr(),
                                    _lib.ptr(res_p), _lib.ptr(res_vx), _lib.ptr(res_vz), ctypes.byref(store),
@@ -241,11 +270,12 @@ class AcousticFunction(torch.autograd.Function):
         vp32 = vp.detach().to(torch.float32).contiguous()
         rho32 = rho.detach().to(torch.float32).contiguous()
         K, fmt, with_rho, cached = opts["checkpoint_every"], opts["fmt"], opts["with_rho"], opts["cached_steps"]
+        ifmt = opts["imaging_fmt"]
         n_ck = -(-(plan.geo.nt - cached) // K)
         ckpt = torch.empty(n_ck * plan.checkpoint_bytes(plan.geo.nt, fmt) if n_ck > 0 else 256,
                            dtype=torch.uint8, device=dev)
-        img = torch.empty(max(plan.imaging_bytes(cached, with_rho), 256), dtype=torch.uint8, device=dev)
-        store = make_store(ckpt if n_ck > 0 else None, K, fmt, img if cached > 0 else None, cached, with_rho)
+        img = torch.empty(max(plan.imaging_bytes(cached, with_rho, ifmt), 256), dtype=torch.uint8, device=dev)
+        store = make_store(ckpt if n_ck > 0 else None, K, fmt, img if cached > 0 else None, cached, with_rho, ifmt)
         p, vx, vz, en, snaps = run_forward(plan, vp32, rho32, damp, src_v, want_energy=opts["want_energy"],
                                            snapshot_every=opts["snapshot_every"], store=store)
         ctx.plan, ctx.opts = plan, opts
@@ -276,9 +306,11 @@ class AcousticFunction(torch.autograd.Function):
 
 def differentiable_forward(plan: Plan, vp, rho, damp, src_v, *, device, snapshot_every: int = 0,
                            checkpoint_segments: int = 1, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
-                           want_energy: bool = True, imaging_cache="auto") -> dict:
+                           want_energy: bool = True, imaging_cache="auto", imaging_dtype: str = "fp32") -> dict:
     if snapshot_dtype not in _lib.CKPT_FORMATS:
         raise ValueError(f"snapshot_dtype must be one of {sorted(_lib.CKPT_FORMATS)}")
+    if imaging_dtype not in _lib.IMAGING_FORMATS:
+        raise ValueError(f"imaging_dtype must be one of {sorted(_lib.IMAGING_FORMATS)}")
     need_rho = bool(getattr(rho, "requires_grad", False))
     vp_t = vp if torch.is_tensor(vp) else torch.as_tensor(vp)
     rho_t = rho if torch.is_tensor(rho) else torch.as_tensor(rho)
@@ -286,9 +318,9 @@ def differentiable_forward(plan: Plan, vp, rho, damp, src_v, *, device, snapshot
         if t.device != device:
             raise ValueError(f"{name} is on {t.device}, expected {device}")
     K = choose_checkpoint_every(plan, checkpoint_segments, checkpoint_every, snapshot_dtype, need_rho)
-    cached = choose_cached_steps(plan, imaging_cache, need_rho, device)
+    cached = choose_cached_steps(plan, imaging_cache, need_rho, device, imaging_dtype, K, snapshot_dtype)
     opts = dict(checkpoint_every=K, fmt=snapshot_dtype, want_energy=want_energy, snapshot_every=snapshot_every,
-                with_rho=need_rho, cached_steps=cached)
+                with_rho=need_rho, cached_steps=cached, imaging_fmt=imaging_dtype)
     p, vx, vz, e0, e1, e2, snaps = AcousticFunction.apply(vp_t, rho_t, plan, damp, src_v, opts)
     out = {"p": p, "vx": vx, "vz": vz, "forward_wavefield_p": e0, "forward_wavefield_vx": e1,
            "forward_wavefield_vz": e2}

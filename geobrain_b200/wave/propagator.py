@@ -8,7 +8,7 @@ geobrain/physics/wave/propagators/acoustic.py:23-300:
     checkpointing off when no parameter requires grad (:199-202), selects
     one shot with shot_index (:205-216) and returns a WaveResult (:275).
 Opt-in additions: fd_order (4 or 8) in the constructor; checkpoint_every,
-snapshot_dtype, imaging_cache and want_energy in forward().
+snapshot_dtype, imaging_cache, imaging_dtype and want_energy in forward().
 """
 from __future__ import annotations
 
@@ -82,7 +82,8 @@ class AcousticPropagator(AbstractPropagator):
 
     def forward(self, model: Optional[AcousticModel] = None, shot_index: Optional[int] = None,
                 checkpoint_segments: int = 1, snapshot_every: int = 0, *, checkpoint_every: int = 0,
-                snapshot_dtype: str = "fp32", want_energy: bool = True, imaging_cache="auto") -> WaveResult:
+                snapshot_dtype: str = "fp32", want_energy: bool = True, imaging_cache="auto",
+                imaging_dtype: str = "fp32") -> WaveResult:
         model = model if model is not None else self.model
         model.forward()
         if checkpoint_segments > 1 and not any(p.requires_grad for p in model.parameters()):
@@ -98,7 +99,8 @@ class AcousticPropagator(AbstractPropagator):
             rcv_x=self.rcv_x, rcv_z=self.rcv_z, rcv_n=self.rcv_n, damp=self.damp, vp=model.vp, rho=model.rho,
             checkpoint_segments=checkpoint_segments, device=torch.device(self.device), dtype=self.dtype,
             snapshot_every=snapshot_every, fd_order=self.fd_order, checkpoint_every=checkpoint_every,
-            snapshot_dtype=snapshot_dtype, want_energy=want_energy, imaging_cache=imaging_cache)
+            snapshot_dtype=snapshot_dtype, want_energy=want_energy, imaging_cache=imaging_cache,
+            imaging_dtype=imaging_dtype)
         return WaveResult.from_dict(result)
 
     def __call__(self, model: Optional[AcousticModel] = None, shot_index: Optional[int] = None,

@@ -52,16 +52,32 @@ typedef struct gb_model_desc {
 #define GB_CKPT_BF16  1   /* bf16 with one fp32 scale per (checkpoint, shot, field) */
 #define GB_CKPT_F16   2   /* fp16 with one fp32 scale per (checkpoint, shot, field) */
 
+/* Storage formats of the imaging cache.  Both short formats keep the fp32
+ * exponent (no scale) and round to nearest even:
+ *   GB_IMG_BF16  16 bits (8-bit mantissa);
+ *   GB_IMG_F24   24 bits (15-bit mantissa), 3 bytes per value. */
+#define GB_IMG_F32   0
+#define GB_IMG_BF16  1
+#define GB_IMG_F24   3
+
 /* What the forward keeps for a later gb_backward (replaces the
  * torch.utils.checkpoint segments of acoustic_2d.py:430,448-460):
  *   checkpoints       full state every checkpoint_every steps, in `format`,
  *                     gb_plan_checkpoint_bytes(plan, checkpoint_every, format)
  *                     bytes (may be NULL when cached_steps == nt);
- *   imaging           the fp32 imaging fields of the last cached_steps time
- *                     steps, gb_plan_imaging_bytes(plan, cached_steps,
- *                     with_rho) bytes (may be NULL when cached_steps == 0);
- *                     those steps need no recompute in the backward;
- *   with_rho          keep / compute the fields the density gradient needs. */
+ *   imaging           the imaging fields of the last cached_steps time steps,
+ *                     gb_plan_imaging_bytes(plan, cached_steps, with_rho,
+ *                     imaging_format) bytes (may be NULL when
+ *                     cached_steps == 0); those steps need no recompute in
+ *                     the backward;
+ *   with_rho          keep / compute the fields the density gradient needs;
+ *   imaging_format    GB_IMG_F32, GB_IMG_F24 or GB_IMG_BF16.  The fields
+ *                     are only multiplied into the gradient sums, so each
+ *                     rounding error enters the gradient once and is not
+ *                     propagated by the wave equation; the sums cancel
+ *                     heavily, though, so the gradient's relative error is
+ *                     of the order of the format's precision (about 3e-3
+ *                     for bf16, 1e-5 for f24). */
 typedef struct gb_grad_store {
     void *checkpoints;
     int32_t checkpoint_every;
@@ -69,6 +85,7 @@ typedef struct gb_grad_store {
     void *imaging;
     int32_t cached_steps;
     int32_t with_rho;
+    int32_t imaging_format;
 } gb_grad_store;
 
 typedef struct gb_plan gb_plan;   /* opaque */
@@ -101,8 +118,9 @@ size_t gb_plan_workspace_bytes(const gb_plan *plan, int with_gradient, int check
 /* Bytes of checkpoint storage for a given segment length and format. */
 size_t gb_plan_checkpoint_bytes(const gb_plan *plan, int checkpoint_every, int ckpt_format);
 
-/* Bytes of the imaging cache for the last cached_steps time steps. */
-size_t gb_plan_imaging_bytes(const gb_plan *plan, int cached_steps, int with_rho);
+/* Bytes of the imaging cache for the last cached_steps time steps
+ * (imaging_format one of GB_IMG_*; 0 for an unknown format). */
+size_t gb_plan_imaging_bytes(const gb_plan *plan, int cached_steps, int with_rho, int imaging_format);
 
 /* Forward modelling, all nt steps, on `stream` (acoustic_forward_kernel,
  * acoustic_2d.py:294-501).  Device pointers:
@@ -131,7 +149,8 @@ int gb_forward(gb_plan *plan, const float *vp, const float *rho, const float *da
  * back into the edge cells (the adjoint of pad_model).  grad_vp / grad_rho
  * are (nz, nx) float32 and are overwritten; grad_rho may be NULL (it needs a
  * store made with with_rho).  Workspace: gb_plan_workspace_bytes(plan,
- * with_rho ? 2 : 1, checkpoint_every). */
+ * with_rho ? 2 : 1, min(checkpoint_every, nt - cached_steps)) (at least 1
+ * step: the recompute segments only cover the uncached steps). */
 int gb_backward(gb_plan *plan, const float *vp, const float *rho, const float *damp,
                 const float *wavelet,
                 const float *res_p, const float *res_vx, const float *res_vz,
