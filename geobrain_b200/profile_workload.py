@@ -1,11 +1,14 @@
 """Run a short slice of a benchmark workload, for profilers (ncu).
 
     python -m geobrain_b200.profile_workload --phase forward  --nt 6
-    python -m geobrain_b200.profile_workload --phase gradient --nt 6
+    python -m geobrain_b200.profile_workload --phase gradient --nt 6 [--imaging-dtype fp24]
 
 Builds the 400 x 1200 / 32-shot / 8th-order model of the benchmark, runs
 ``nt`` time steps of the forward (or forward + adjoint) once, synchronises
-and exits 0.  Everything stays on the device; nothing is timed.
+and exits 0.  Everything stays on the device; nothing is timed.  With
+--imaging-dtype the gradient keeps every step's imaging fields in that
+format (as the benchmark does); without it, one fp32 checkpoint and a
+recompute of all steps.
 """
 from __future__ import annotations
 
@@ -26,6 +29,7 @@ def main() -> None:
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--shots-per-cta", type=int, default=0)
     ap.add_argument("--energy", action="store_true")
+    ap.add_argument("--imaging-dtype", choices=["fp32", "fp24", "bf16"], default=None)
     args = ap.parse_args()
     dev = torch.device("cuda:0")
     w = synthetic.fwi_400x1200(nt=args.nt, n_shots=args.shots)
@@ -42,8 +46,12 @@ def main() -> None:
         engine.run_forward(plan, vp, rho, damp, src_v, want_energy=args.energy)
     else:
         K = w.nt
-        ck = torch.empty(plan.checkpoint_bytes(K, "fp32"), dtype=torch.uint8, device=dev)
-        store = engine.make_store(ck, K, "fp32", None, 0, False)
+        if args.imaging_dtype:
+            img = torch.empty(plan.imaging_bytes(w.nt, False, args.imaging_dtype), dtype=torch.uint8, device=dev)
+            store = engine.make_store(None, K, "fp32", img, w.nt, False, args.imaging_dtype)
+        else:
+            ck = torch.empty(plan.checkpoint_bytes(K, "fp32"), dtype=torch.uint8, device=dev)
+            store = engine.make_store(ck, K, "fp32", None, 0, False)
         p, _, _, _, _ = engine.run_forward(plan, vp, rho, damp, src_v, want_energy=args.energy, store=store)
         engine.run_backward(plan, vp, rho, damp, src_v, p, None, None, store, False)
     torch.cuda.synchronize()
