@@ -190,7 +190,7 @@ def main():
     import torch
     import torch.distributed as dist
     from geobrain_b200 import synthetic, wave
-    from geobrain_b200.wave import engine
+    from geobrain_b200.wave import engine, sharding
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -226,8 +226,9 @@ def main():
         loss = 0.5 * (res * res).sum()
         loss.backward()
         g = vp.grad
-        if world > 1:
-            dist.all_reduce(g)
+        if world > 1:      # one packed NCCL all-reduce of the gradient and the misfit
+            loss, g = sharding.allreduce_packed([loss.detach().reshape(1), g])
+            loss = loss.reshape(())
         return g, loss
 
     vp0 = torch.tensor(w.vp, device=dev)

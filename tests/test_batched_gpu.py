@@ -69,3 +69,31 @@ def test_batched_gradient_matches_single_model_path(cuda_device, imaging_cache, 
                              rcv_x=c["rcv_x"], rcv_z=c["rcv_z"], damp=c["damp"], vp=c["vp"], rho=c["rho"],
                              res_p=l.astype(np.float64), half=4)
     assert orc.rel_l2(m["vp"].grad.cpu().numpy(), rvp) < (1e-2 if imaging_dtype == "bf16" else 1e-4)
+
+
+def test_ensemble_log_likelihood_matches_per_particle_loop(cuda_device):
+    """An ensemble of velocity particles through the batched engine
+    (sharding.ensemble_forward + sharded_log_likelihood, one process)
+    against the reference's per-particle loop of Gaussian log-likelihoods
+    (geobrain/core/inverse.py:104-110) over acoustic_forward_kernel."""
+    from geobrain_b200.wave import acoustic_forward_kernel, sharding
+    c = synthetic_case(40, 90, 10, 80, 2, seed=5)
+    template = model_dict(c, cuda_device)
+    template.pop("vp")
+    rng = np.random.default_rng(1)
+    theta = torch.tensor(np.stack([c["vp"] * (1 + 0.02 * rng.standard_normal(c["vp"].shape)) for _ in range(3)])
+                         .reshape(3, -1), dtype=torch.float32, device=cuda_device)
+    observed = torch.tensor(orc.forward(nz=c["nz"], nx=c["nx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+                                        free_surface=False, src_x=c["src_x"], src_z=c["src_z"], src_v=c["src_v"],
+                                        rcv_x=c["rcv_x"], rcv_z=c["rcv_z"], damp=c["damp"], vp=c["vp"],
+                                        rho=c["rho"], half=4)["p"], dtype=torch.float32, device=cuda_device)
+    fwd = sharding.ensemble_forward(template, (c["nz"], c["nx"]), fd_order=8)
+    ll, grad = sharding.sharded_log_likelihood(theta, fwd, observed, noise_std=0.1)
+    for i in range(3):
+        t = theta[i].clone().reshape(c["nz"], c["nx"]).requires_grad_(True)
+        pred = acoustic_forward_kernel(**dict(template, vp=t), device=cuda_device, fd_order=8)["p"]
+        r = (pred.reshape(-1) - observed.reshape(-1)) / 0.1
+        li = -0.5 * (r * r).sum()
+        li.backward()
+        assert abs(float(ll[i]) - float(li.detach())) <= 1e-5 * abs(float(li.detach()))
+        assert orc.rel_l2(grad[i].reshape(c["nz"], c["nx"]).cpu().numpy(), t.grad.cpu().numpy()) < 1e-5

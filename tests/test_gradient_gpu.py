@@ -131,6 +131,32 @@ def test_short_imaging_cache_within_budget(cuda_device, fmt, tol, cache, want_rh
     assert not np.array_equal(gvp, g32)          # the cached steps really came from the short store
 
 
+def test_shot_subsets_sum_to_the_full_gradient(cuda_device):
+    """The rank-local FWI function of the sharded path: gradients of shot
+    subsets add up to the all-shot gradient (the split changes only the
+    order of the fp32 sums)."""
+    from geobrain_b200.wave import sharding
+    c = load_case("small_nofs")
+    kk = dict(nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+              free_surface=False, src_x=c["src_x"], src_z=c["src_z"], src_n=3,
+              src_v=torch.as_tensor(c["src_v"], device=cuda_device), rcv_x=c["rcv_x"], rcv_z=c["rcv_z"],
+              rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=cuda_device), device=cuda_device,
+              fd_order=8)
+    vp = torch.tensor(c["vp"], device=cuda_device)
+    rho = torch.tensor(c["rho"], device=cuda_device)
+    d_obs = torch.tensor(c["ref32_p"] * 0.9, device=cuda_device)
+    run = sharding.fwi_local_fn(kk, vp, rho, d_obs)
+    l_all, g_all = run([0, 1, 2])
+    l_a, g_a = run([0, 2])
+    l_b, g_b = run([1])
+    assert abs(float(l_a + l_b) - float(l_all)) <= 1e-5 * abs(float(l_all))
+    assert orc.rel_l2((g_a + g_b).cpu().numpy(), g_all.cpu().numpy()) < 1e-6
+    l_s, g_s = sharding.sharded_shot_gradient(3, run)          # one process: one call over all shots
+    np.testing.assert_array_equal(g_s.cpu().numpy(), g_all.cpu().numpy())
+    z_l, z_g = run([])
+    assert float(z_l) == 0.0 and not z_g.any()
+
+
 def test_velocity_only_gradient_matches_full(cuda_device):
     c = load_case("small_fs")
     g1, _, _ = cuda_grad(c, cuda_device, want_rho=False)
@@ -165,7 +191,7 @@ def test_gradient_central_difference(cuda_device):
         loss = 0.5 * ((out["p"].double() - d_obs.double()) ** 2).sum()
         if grad:
             loss.backward()
-            return float(loss), vp.grad.cpu().numpy().astype(np.float64)
+            return float(loss.detach()), vp.grad.cpu().numpy().astype(np.float64)
         return float(loss)
 
     _, g = loss_at(c["vp"], grad=True)
