@@ -58,6 +58,11 @@ SIGNATURES = {
     "gb_plan_checkpoint_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_imaging_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gb_plan_set_group_streams": (ctypes.c_int, [_P, ctypes.c_int]),
+    "gb_plan_set_graph_steps": (ctypes.c_int, [_P, ctypes.c_int]),
+    "gb_plan_autotune_workspace_bytes": (_SZ, [_P]),
+    "gb_plan_get_config": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "gb_plan_autotune": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _I32, _P, ctypes.POINTER(ctypes.c_float)]),
     "gb_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P, _P, _SZ, _P]),
     "gb_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
     "gb_workspace_status": (ctypes.c_int, [_P, _P]),

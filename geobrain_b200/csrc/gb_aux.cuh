@@ -118,4 +118,8 @@ __global__ void unpack16_kernel(const H *__restrict__ in, const float *__restric
         o[i] = from_h(p[i]) * scale;
 }
 
+// Step counter of graph-replayed forward chunks.
+__global__ void step_set_kernel(int *ctr, int value) { *ctr = value; }
+__global__ void step_advance_kernel(int *ctr, int by) { *ctr += by; }
+
 }  // namespace gb

@@ -125,14 +125,29 @@ struct gb_plan {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[3];   // forward, recompute, adjoint
     long long launches = 0;
     long long phase_steps[3] = {0, 0, 0};                     // time steps run per phase
+    // plain forward as replays of a CUDA graph of graph_steps steps (0 = off)
+    int graph_steps = 16;
+    cudaStream_t cap_stream = nullptr;                         // capture origin (never the legacy stream)
+    cudaGraphExec_t gexec = nullptr;
+    std::vector<uintptr_t> gkey;                               // what the instantiated graph baked in
 
     ~gb_plan()
     {
         clear_events();
+        release_graph();
         release_streams();
+    }
+    void release_graph()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+        gkey.clear();
     }
     void release_streams()
     {
+        release_graph();            // it references these streams' events
+        if (cap_stream) cudaStreamDestroy(cap_stream);
+        cap_stream = nullptr;
         for (auto s : gstream) cudaStreamDestroy(s);
         for (auto e : gjoin) cudaEventDestroy(e);
         if (gfork) cudaEventDestroy(gfork);
@@ -469,6 +484,54 @@ inline void launch_groups(const GroupStreams &gs, int i, int n_groups, int *g0, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// CUDA graph of a chunk of plain forward steps.  The graph holds C steps of
+// every shot group (C even, so step j of the chunk reads state level j & 1)
+// with the group fork / join, then advances a device step counter by C; the
+// step kernels take their step index from that counter.  It is captured once
+// for a given set of buffers and replayed nt / C times.
+// ---------------------------------------------------------------------------
+constexpr int kMaxGraphSteps = 64;
+
+int capture_forward_chunk(gb_plan *P, const StepKernel &K, const Maps (&maps)[2], float *const (&buf)[2],
+                          FwdArgs A, int C, int *step_ctr, cudaGraphExec_t *out)
+{
+    GroupStreams gs;
+    if (int rc = group_streams(P, nullptr, &gs)) return rc;      // (re)creating the group streams drops cap_stream
+    if (!P->cap_stream) GB_CUDA(cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking));
+    gs.main = P->cap_stream;
+    const long long launches = P->launches;
+    GB_CUDA(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = fork(gs);
+    A.step_base = step_ctr;
+    for (int j = 0; j < C && rc == GB_OK; ++j) {
+        A.it = j;
+        A.out = buf[(j & 1) ^ 1];
+        for (int i = 0; i < gs.n && rc == GB_OK; ++i) {
+            int g0, gc;
+            launch_groups(gs, i, P->n_groups, &g0, &gc);
+            rc = launch_step(P, K, maps[j & 1], A, g0, gc, gs.at(i));
+        }
+    }
+    if (rc == GB_OK) rc = join(gs);
+    if (rc == GB_OK) {
+        step_advance_kernel<<<1, 1, 0, P->cap_stream>>>(step_ctr, C);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(GB_E_CUDA, "graph capture: launch failed");
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(P->cap_stream, &graph);   // always end the capture
+    P->launches = launches;
+    if (rc != GB_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ec != cudaSuccess) return fail(GB_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return fail(GB_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    return GB_OK;
+}
+
 // Per-checkpoint sizes of the 16-bit formats.
 size_t ck16_bytes(const gb_plan *p) { return align256((size_t)p->d.n_shots * 3 * p->plane * 2); }
 size_t ck_scale_bytes(const gb_plan *p) { return align256((size_t)p->d.n_shots * 3 * 4); }
@@ -673,6 +736,7 @@ int gb_plan_set_tiling(gb_plan *p, int tile_rows, int shots_per_cta)
     if (tile_rows) p->tz = tile_rows;
     p->spc = shots_per_cta ? std::min(std::min(shots_per_cta, p->d.n_shots), kMaxShotsPerCta) : 0;
     p->retile();
+    p->release_graph();
     return GB_OK;
 }
 
@@ -680,6 +744,27 @@ int gb_plan_set_group_streams(gb_plan *p, int enable)
 {
     if (!p) return fail(GB_E_ARG, "null plan");
     p->group_streams = enable != 0;
+    p->release_graph();
+    return GB_OK;
+}
+
+int gb_plan_get_config(const gb_plan *p, int *tile_rows, int *shots_per_cta, int *group_streams, int *graph_steps)
+{
+    if (!p) return fail(GB_E_ARG, "null plan");
+    if (tile_rows) *tile_rows = p->tz;
+    if (shots_per_cta) *shots_per_cta = p->spc_eff;
+    if (group_streams) *group_streams = p->group_streams ? 1 : 0;
+    if (graph_steps) *graph_steps = p->graph_steps;
+    return GB_OK;
+}
+
+int gb_plan_set_graph_steps(gb_plan *p, int steps)
+{
+    if (!p) return fail(GB_E_ARG, "null plan");
+    if (steps < 0 || steps > kMaxGraphSteps || (steps & 1))
+        return fail(GB_E_ARG, "graph steps must be an even number in [0, " + std::to_string(kMaxGraphSteps) + "]");
+    p->graph_steps = steps;
+    p->release_graph();
     return GB_OK;
 }
 
@@ -763,7 +848,43 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
     const size_t step_img = (size_t)n_img * S * P->plane;
     int snap_i = 0;
     P->phase_steps[0] += d.nt;
-    for (int it = 0; it < d.nt; ++it) {
+    int it_first = 0;
+    // plain forward: whole chunks of graph_steps steps as graph replays
+    const int C = P->graph_steps;
+    const bool snaps_fit = snapshot_every <= 0 || !snapshots || snapshot_every % std::max(C, 1) == 0;
+    if (C > 0 && !store && snaps_fit && d.nt >= C) {
+        if (int rc = join(gs)) return rc;            // the chunks run from the caller's stream
+        int *step_ctr = reinterpret_cast<int *>(ws + L.err + 128);
+        int dev = -1;
+        GB_CUDA(cudaGetDevice(&dev));
+        const std::vector<uintptr_t> key = {
+            (uintptr_t)dev, (uintptr_t)ws, (uintptr_t)wavelet, (uintptr_t)trace_p, (uintptr_t)trace_vx,
+            (uintptr_t)trace_vz, (uintptr_t)want_energy, (uintptr_t)C, (uintptr_t)P->tz, (uintptr_t)P->spc_eff,
+            (uintptr_t)P->n_groups, (uintptr_t)gs.n, (uintptr_t)K0.fn};
+        if (!P->gexec || P->gkey != key) {
+            P->release_graph();
+            if (int rc = capture_forward_chunk(P, K0, maps, buf, A, C, step_ctr, &P->gexec)) return rc;
+            P->gkey = key;
+        }
+        step_set_kernel<<<1, 1, 0, st>>>(step_ctr, 0);
+        GB_CUDA(cudaGetLastError());
+        ++P->launches;
+        const int n_chunks = d.nt / C;
+        for (int k = 0; k < n_chunks; ++k) {
+            GB_CUDA(cudaGraphLaunch(P->gexec, st));
+            P->launches += (long long)C * gs.n + 1;
+            const int last = (k + 1) * C - 1;
+            if (snapshot_every > 0 && snapshots && ((last + 1) % snapshot_every == 0 || last == d.nt - 1)) {
+                GB_CUDA(cudaMemcpy2DAsync(snapshots + (size_t)snap_i * d.nz * d.nx, (size_t)d.nx * 4,
+                                          buf[0] + (size_t)d.nabc * P->pitch + d.nabc, (size_t)P->pitch * 4,
+                                          (size_t)d.nx * 4, d.nz, cudaMemcpyDeviceToDevice, st));
+                ++snap_i;
+            }
+        }
+        it_first = n_chunks * C;
+        if (int rc = fork(gs)) return rc;
+    }
+    for (int it = it_first; it < d.nt; ++it) {
         const int b = it & 1;
         A.it = it;
         A.out = buf[b ^ 1];
@@ -798,6 +919,102 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
             ++P->launches;
         }
     P->mark(0, false, st);
+    return GB_OK;
+}
+
+size_t gb_plan_autotune_workspace_bytes(gb_plan *p)
+{
+    if (!p) return 0;
+    const int tz = p->tz;
+    size_t m = 0;
+    for (int t : {16, 32}) {
+        p->tz = t;
+        p->retile();
+        m = std::max(m, gb_plan_workspace_bytes(p, 0, 0));
+    }
+    p->tz = tz;
+    p->retile();
+    return m;
+}
+
+int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float *damp, const float *wavelet,
+                     void *workspace, size_t workspace_bytes, int32_t steps, void *stream, float *best_ms_per_step)
+{
+    g_last_error.clear();
+    if (!P || !vp || !rho || !damp || !wavelet || !workspace) return fail(GB_E_ARG, "null argument");
+    if (steps < 2 || steps > P->d.nt) return fail(GB_E_ARG, "steps must be in [2, nt]");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    struct Config {
+        int tz, spc;
+        bool streams;
+        int graph;
+    };
+    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps};
+    const bool prof = P->prof;
+    const int nt = P->d.nt;
+    const long long launches = P->launches;
+    const int S = P->d.n_shots;
+    const int C = 16;
+    const int n = steps >= C ? steps / C * C : steps;       // whole graph chunks when graphs are tried
+    std::vector<Config> cands;
+    for (int tz : {16, 32})
+        for (int spc : {0, 1, 2, 4, 8, 16}) {
+            if (spc > S) continue;
+            for (int streams = 1; streams >= 0; --streams)
+                for (int graph : {0, C}) {
+                    if (graph > n) continue;
+                    cands.push_back({tz, spc, streams != 0, graph});
+                }
+        }
+    cudaEvent_t e0, e1;
+    GB_CUDA(cudaEventCreate(&e0));
+    GB_CUDA(cudaEventCreate(&e1));
+    P->prof = false;
+    P->d.nt = n;                       // time n steps; the wavelet is read within its first S * n samples
+    float best = -1.f;
+    Config win = saved;
+    int rc = GB_OK;
+    for (const Config &k : cands) {
+        P->tz = k.tz;
+        P->spc = k.spc;
+        P->retile();
+        P->group_streams = k.streams;
+        P->graph_steps = k.graph;
+        P->release_graph();
+        if (gb_plan_workspace_bytes(P, 0, 0) > workspace_bytes) continue;
+        if (k.streams && P->n_groups == 1) continue;      // same as without
+        float ms = -1.f;
+        for (int rep = 0; rep < 3 && rc == GB_OK; ++rep) {
+            if (cudaEventRecord(e0, st) != cudaSuccess) rc = fail(GB_E_CUDA, "event record failed");
+            if (rc == GB_OK)
+                rc = gb_forward(P, vp, rho, damp, wavelet, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0,
+                                nullptr, nullptr, workspace, workspace_bytes, stream);
+            if (rc == GB_OK && (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+                rc = fail(GB_E_CUDA, "event wait failed");
+            float t = 0.f;
+            if (rc == GB_OK && rep > 0 && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess)
+                ms = ms < 0 ? t : std::min(ms, t);   // the first run warms up (and captures a graph)
+        }
+        if (rc != GB_OK) break;
+        if (ms >= 0 && (best < 0 || ms < best)) {
+            best = ms;
+            win = k;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    P->d.nt = nt;
+    P->prof = prof;
+    P->launches = launches;
+    P->tz = win.tz;
+    P->spc = win.spc;
+    P->retile();
+    P->group_streams = win.streams;
+    P->graph_steps = win.graph;
+    P->release_graph();                // captured with the shortened step count
+    if (rc != GB_OK) return rc;
+    if (best < 0) return fail(GB_E_WORKSPACE, "no candidate fits the workspace");
+    if (best_ms_per_step) *best_ms_per_step = best / n;
     return GB_OK;
 }
 
@@ -1435,7 +1652,13 @@ extern "C" int gb_forward_static_scratch(gb_plan *P, const float *vp, const floa
         scratch = g_static_scratch_addr[dev];
     }
     // gb_forward clears every part of the scratch that must start at zero
-    // (both wavefield time levels, the energy sums, the status word)
-    return gb_forward(P, vp, rho, damp, wavelet, trace_p, trace_vx, trace_vz, energy_p, energy_vx, energy_vz,
-                      snapshot_every, snapshots, nullptr, scratch, kStaticScratchBytes, stream);
+    // (both wavefield time levels, the energy sums, the status word).  It
+    // runs with one launch per step: instantiating a CUDA graph would make
+    // the driver allocate device memory.
+    const int graph_steps = P->graph_steps;
+    P->graph_steps = 0;
+    const int rc = gb_forward(P, vp, rho, damp, wavelet, trace_p, trace_vx, trace_vz, energy_p, energy_vx, energy_vz,
+                              snapshot_every, snapshots, nullptr, scratch, kStaticScratchBytes, stream);
+    P->graph_steps = graph_steps;
+    return rc;
 }

@@ -41,7 +41,8 @@ struct StepGeom {
 
 struct FwdArgs {
     StepGeom g;
-    int it;                          // time step index
+    int it;                          // time step index (offset from *step_base when that is set)
+    const int *step_base;            // device step counter of a graph-replayed chunk, or null
     const float *a1, *k1, *a2, *k2, *k3;   // coefficient planes, Nz x pitch
     const int *tile_fast;            // per tile: 1 = no masks and no damping anywhere it reads
     float *out;                      // next state [S][3][plane]
@@ -114,6 +115,9 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
 
     const int z0 = (tile / g.tiles_x) * TZ;
     const int x0 = (tile % g.tiles_x) * TX;
+    // a CUDA graph replays the same launches for every chunk of steps; the
+    // chunk's first step comes from device memory
+    const int it = A.step_base ? *reinterpret_cast<const volatile int *>(A.step_base) + A.it : A.it;
     const int s0 = group * g.shots_per_cta;
     const int ns = min(g.n_shots - s0, g.shots_per_cta);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -228,7 +232,7 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                     if (gz == sz && sx >= gx0 && sx < gx0 + 4) {
                         // p + dt * w, rounded after the product and after the
                         // sum as the reference does (acoustic_2d.py:230-233)
-                        const float amp = __fmul_rn(g.dt, A.wavelet[(long long)s * g.nt + A.it]);
+                        const float amp = __fmul_rn(g.dt, A.wavelet[(long long)s * g.nt + it]);
                         const int q = sx - gx0;
                         if (q == 0) pv.x = __fadd_rn(pv.x, amp);
                         else if (q == 1) pv.y = __fadd_rn(pv.y, amp);
@@ -338,7 +342,7 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
             for (int e = rcv0 + threadIdx.x; e < rcv1; e += NTHR) {
                 const int4 en = A.rcv_ent[e];
                 const int rr = en.x + R, cc = en.y + 4;
-                const long long t = ((long long)s * g.nt + A.it) * g.n_rcv + en.z;
+                const long long t = ((long long)s * g.nt + it) * g.n_rcv + en.z;
                 if (A.tr_p) A.tr_p[t] = sP[rr * RW + cc];
                 if (A.tr_vx) A.tr_vx[t] = sVX[rr * VXW + cc + 4];
                 if (A.tr_vz) A.tr_vz[t] = sVZ[(en.x + 2 * R) * RW + cc];

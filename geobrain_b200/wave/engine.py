@@ -64,6 +64,9 @@ class Plan:
             raise ValueError(msg) if rc == _lib.GB_E_ARG else _lib.GbError(rc, msg)
         self.h = h
         self.tiling = (0, 0)
+        self.group_streams = True
+        self.graph_steps = 16                    # the library's default
+        self.tuned: Optional[dict] = None       # the autotuner's choice, once it ran
 
     def __del__(self):
         h = getattr(self, "h", None)
@@ -101,6 +104,35 @@ class Plan:
 
     def set_group_streams(self, enable: bool) -> None:
         _lib.check(self._lib.gb_plan_set_group_streams(self.h, int(enable)))
+        self.group_streams = bool(enable)
+
+    def set_graph_steps(self, steps: int) -> None:
+        """Plain forward as replays of a CUDA graph of `steps` steps (0 = off)."""
+        _lib.check(self._lib.gb_plan_set_graph_steps(self.h, int(steps)))
+        self.graph_steps = int(steps)
+
+    def autotune(self, vp: torch.Tensor, rho: torch.Tensor, damp: torch.Tensor, src_v: torch.Tensor,
+                 steps: int = 16) -> dict:
+        """Time `steps` forward steps for every launch configuration
+        (gb_plan_autotune) and keep the fastest on this plan."""
+        dev = vp.device
+        ws = workspace(int(self._lib.gb_plan_autotune_workspace_bytes(self.h)), dev)
+        best = ctypes.c_float(0.0)
+        with torch.cuda.device(dev):
+            rc = self._lib.gb_plan_autotune(self.h, vp.data_ptr(), rho.data_ptr(), damp.data_ptr(), src_v.data_ptr(),
+                                            ws.data_ptr(), ws.numel(), int(min(steps, self.geo.nt)),
+                                            stream_handle(dev), ctypes.byref(best))
+        _lib.check(rc)
+        self.tuned = self.config()
+        self.tuned["ms_per_step"] = float(best.value)
+        return self.tuned
+
+    def config(self) -> dict:
+        tz, spc, streams, graph = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int())
+        _lib.check(self._lib.gb_plan_get_config(self.h, ctypes.byref(tz), ctypes.byref(spc), ctypes.byref(streams),
+                                                ctypes.byref(graph)))
+        return {"tile_rows": tz.value, "shots_per_cta": spc.value, "group_streams": bool(streams.value),
+                "graph_steps": graph.value}
 
 
 def get_plan(geo: Geometry, src_x, src_z, rcv_x, rcv_z) -> Plan:

@@ -14,9 +14,14 @@ behaviour: fd_order (4 or 8); checkpoint_every, snapshot_dtype ('fp32',
 'bf16', 'fp16'), imaging_cache ('auto', a byte budget, or 0) and
 imaging_dtype ('fp32'; 'fp24', 3 bytes, gradient error about 1e-5; 'bf16',
 2 bytes, about 3e-3: more cached steps skip the recompute) for the
-gradient's memory; want_energy (skip the energy sums).
+gradient's memory; want_energy (skip the energy sums); autotune (on the
+first call for a geometry, time the launch configurations and keep the
+fastest; GEOBRAIN_B200_AUTOTUNE=1 turns it on by default).
 """
 from __future__ import annotations
+
+import os
+from typing import Optional
 
 import torch
 from torch import Tensor
@@ -47,7 +52,8 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
                             checkpoint_segments: int = 1, device: torch.device = torch.device("cpu"),
                             dtype: torch.dtype = torch.float32, snapshot_every: int = 0, *,
                             fd_order: int = 4, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
-                            want_energy: bool = True, imaging_cache="auto", imaging_dtype: str = "fp32"):
+                            want_energy: bool = True, imaging_cache="auto", imaging_dtype: str = "fp32",
+                            autotune: Optional[bool] = None):
     device = torch.device(device)
     if device.type != "cuda":
         raise ValueError(f"geobrain_b200 runs on CUDA devices only (device={device})")
@@ -81,6 +87,13 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
     for name, t in (("vp", vp), ("rho", rho)):
         if tuple(t.shape) != (int(nz), int(nx)):
             raise ValueError(f"{name} must have shape {(int(nz), int(nx))}, got {tuple(t.shape)}")
+
+    if autotune is None:
+        autotune = os.environ.get("GEOBRAIN_B200_AUTOTUNE", "0") not in ("", "0")
+    if autotune and plan.tuned is None:
+        vp_a = _as_f32(vp.detach() if torch.is_tensor(vp) else vp, device, "vp")
+        rho_a = _as_f32(rho.detach() if torch.is_tensor(rho) else rho, device, "rho")
+        plan.autotune(vp_a, rho_a, damp_t, w)
 
     needs_grad = torch.is_grad_enabled() and (getattr(vp, "requires_grad", False) or
                                               getattr(rho, "requires_grad", False))

@@ -104,6 +104,35 @@ void gb_plan_destroy(gb_plan *plan);
  * default.  Used by the autotuner. */
 int gb_plan_set_tiling(gb_plan *plan, int tile_rows, int shots_per_cta);
 
+/* Plain forward (gb_forward without a gradient store) as replays of one
+ * CUDA graph of `steps` time steps (even, at most 64; 0 = one launch per
+ * step and group; 16 by default).  The graph holds the step kernels of every shot group,
+ * with their fork and join, and a step-counter update.  It is captured on
+ * the first call, kept on the plan and replayed nt / steps times; the
+ * remaining steps launch one by one.  A call with other buffers (workspace,
+ * wavelet or trace pointers) captures it again. */
+int gb_plan_set_graph_steps(gb_plan *plan, int steps);
+
+/* Autotuner.  Times `steps` plain forward steps of this plan (no traces, no
+ * energy) for each launch configuration:
+ *   - tile rows 16 / 32;
+ *   - shots per CTA automatic, 1, 2, 4, 8 or 16;
+ *   - per-group streams on / off;
+ *   - graph chunks of 16 steps or none.
+ * It keeps the fastest on the plan and reports its time per step.  Each
+ * candidate runs three times; the first is a warm-up.  The workspace must
+ * hold gb_plan_autotune_workspace_bytes(plan); candidates that do not fit
+ * are skipped.  Blocks until done. */
+size_t gb_plan_autotune_workspace_bytes(gb_plan *plan);
+
+/* The launch configuration in use (what the autotuner chose): tile rows,
+ * effective shots per CTA, per-group streams, graph chunk steps. */
+int gb_plan_get_config(const gb_plan *plan, int *tile_rows, int *shots_per_cta, int *group_streams,
+                       int *graph_steps);
+int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const float *damp,
+                     const float *wavelet, void *workspace, size_t workspace_bytes, int32_t steps,
+                     void *stream, float *best_ms_per_step);
+
 /* Run each group of shots on its own stream (forked from and joined back to
  * the caller's stream; on by default).  Groups never interact, so their
  * kernels fill each other's tails. */
@@ -215,7 +244,9 @@ int gb_workspace_status(const void *workspace, void *stream);
  *     before any stream capture;
  *   - every call shares the one array per device: calls whose work overlaps
  *     on the GPU (other streams, other threads) race and corrupt each other;
- *   - it calls no cudaMalloc / cudaFree; inputs and outputs are the caller's. */
+ *   - it calls no cudaMalloc / cudaFree; inputs and outputs are the caller's;
+ *   - it launches one kernel per step and shot group, whatever
+ *     gb_plan_set_graph_steps says (instantiating a graph allocates). */
 size_t gb_static_scratch_bytes(void);
 int gb_forward_static_scratch(gb_plan *plan, const float *vp, const float *rho, const float *damp,
                               const float *wavelet,

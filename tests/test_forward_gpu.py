@@ -107,6 +107,70 @@ def test_tilings_are_bit_identical(cuda_device, tiling):
         assert orc.rel_l2(out[k], base[k]) < 1e-6
 
 
+def _plan_of(c, half):
+    from geobrain_b200.wave import engine
+    geo = engine.Geometry(c["nz"], c["nx"], c["nabc"], c["nt"], c["dt"], c["dx"], half, bool(c["free_surface"]))
+    return engine.get_plan(geo, c["src_x"], c["src_z"], c["rcv_x"], c["rcv_z"])
+
+
+@pytest.mark.parametrize("nt,snapshot_every,streams", [(96, 0, True), (101, 32, True), (70, 16, False)])
+def test_graph_replay_is_bit_identical(cuda_device, nt, snapshot_every, streams):
+    """Chunks of 16 steps replayed from one CUDA graph (step index from a
+    device counter; a partial last chunk runs step by step) give the same
+    traces and snapshots as one launch per step (the energy sums, added
+    with atomics, to their association order); a second call replays the
+    cached graph, a call with new buffers captures again."""
+    c = synthetic_case(60, 250, 10, nt, 5, seed=3)
+    plan = _plan_of(c, 4)
+    plan.set_tiling(16, 2)                 # three groups
+    plan.set_group_streams(streams)
+    try:
+        plan.set_graph_steps(0)
+        base = run_cuda(c, cuda_device, fd_order=8, snapshot_every=snapshot_every)
+        plan.set_graph_steps(16)
+        outs = [run_cuda(c, cuda_device, fd_order=8, snapshot_every=snapshot_every) for _ in range(3)]
+    finally:
+        plan.set_graph_steps(16)
+        plan.set_group_streams(True)
+        plan.set_tiling(16, 0)
+    for out in outs:
+        for k in ("p", "vx", "vz"):
+            np.testing.assert_array_equal(out[k], base[k])
+        for k in ("forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vz"):
+            assert orc.rel_l2(out[k], base[k]) < 1e-6
+        if snapshot_every:
+            np.testing.assert_array_equal(out["snapshots"], base["snapshots"])
+
+
+def test_graph_steps_validation(cuda_device):
+    c = synthetic_case(40, 130, 10, 20, 1, seed=2)
+    plan = _plan_of(c, 4)
+    for bad in (3, -2, 66):
+        with pytest.raises(Exception):
+            plan.set_graph_steps(bad)
+
+
+def test_autotune_picks_a_configuration_and_keeps_results(cuda_device):
+    """The autotuner only changes the launch configuration: traces after
+    tuning equal those before."""
+    c = synthetic_case(80, 300, 10, 48, 6, seed=9)
+    base = run_cuda(c, cuda_device, fd_order=8)
+    plan = _plan_of(c, 4)
+    assert plan.tuned is None
+    try:
+        tuned = run_cuda(c, cuda_device, fd_order=8, autotune=True)
+        cfg = plan.tuned
+        assert cfg is not None and cfg["ms_per_step"] > 0
+        assert cfg["tile_rows"] in (16, 32) and cfg["graph_steps"] in (0, 16)
+        assert plan.config() == {k: cfg[k] for k in ("tile_rows", "shots_per_cta", "group_streams", "graph_steps")}
+    finally:
+        plan.set_graph_steps(16)
+        plan.set_group_streams(True)
+        plan.set_tiling(16, 0)
+    for k in ("p", "vx", "vz"):
+        np.testing.assert_array_equal(tuned[k], base[k])
+
+
 def test_wavelet_scaling_is_linear(cuda_device):
     """Linearity in the source at a large grid (a size-independent check):
     doubling the wavelet doubles every trace to fp32 rounding.  Bit-exact
