@@ -345,6 +345,8 @@ def main():
     extras = {}
     if not args.no_extras and world == 1:
         extras = plain_forward_rates(torch, wave, synthetic, dev)
+        extras.update(batch_rates(torch, wave, synthetic, dev))
+        extras.update(large_gradient_rate(torch, wave, synthetic, dev))
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -403,6 +405,91 @@ def plain_forward_rates(torch, wave, synthetic, dev):
         out[name] = {"gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms,
                      "fd_order": w.fd_order, "nt": w.nt, "shots": w.n_shots}
     return out
+
+
+def _model_kwargs(torch, wave, w, dev, vp=None):
+    damp = torch.tensor(wave.bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp.max()), False),
+                        dtype=torch.float32, device=dev)
+    return dict(nx=w.nx, nz=w.nz, dx=w.dx, dz=w.dx, nt=w.nt, dt=w.dt, nabc=w.nabc, free_surface=False,
+                src_x=w.src_x, src_z=w.src_z, src_n=w.n_shots,
+                src_v=torch.tensor(np.tile(w.wavelet, (w.n_shots, 1)), device=dev), rcv_x=w.rcv_x, rcv_z=w.rcv_z,
+                rcv_n=w.rcv_x.size, damp=damp, vp=vp if vp is not None else torch.tensor(w.vp, device=dev),
+                rho=torch.tensor(w.rho, device=dev))
+
+
+def _timed(torch, fn, reps=1):
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def batch_rates(torch, wave, synthetic, dev):
+    """Batched engine (one launch per time step for all models): the 50
+    particles of 256 x 512 (8 shots, 2000 steps) and the 24 uneven models
+    (128 x 256 .. 512 x 1024, 1000 .. 3000 steps, 4 .. 16 shots), forward
+    and gradient (fwd + adjoint of 0.5 ||p||^2, fp24 imaging cache within
+    the free memory, checkpoints for the rest)."""
+    out = {}
+    for name, ws in (("ensemble_256x512_50particles", synthetic.ensemble_256x512()),
+                     ("uneven_batch_24models", synthetic.uneven_batch())):
+        units = sum(w.cell_updates() for w in ws)
+
+        def fwd():
+            with torch.no_grad():
+                wave.acoustic_forward_batched([_model_kwargs(torch, wave, w, dev) for w in ws], fd_order=8,
+                                              want_energy=False, device=dev)
+
+        def grad():
+            ms = [_model_kwargs(torch, wave, w, dev, torch.tensor(w.vp, device=dev, requires_grad=True)) for w in ws]
+            outs = wave.acoustic_forward_batched(ms, fd_order=8, want_energy=False, device=dev, imaging_dtype="fp24")
+            loss = sum(0.5 * (o["p"] * o["p"]).sum() for o in outs)
+            loss.backward()
+            return [m["vp"].grad for m in ms]
+
+        ms_f = _timed(torch, fwd)
+        ms_g = _timed(torch, grad)
+        out[name] = {"forward_gcell_updates_per_s": units / (ms_f * 1e-3) / 1e9, "forward_ms": ms_f,
+                     "gradient_gcell_updates_per_s": units / (ms_g * 1e-3) / 1e9, "gradient_ms": ms_g,
+                     "models": len(ws), "cell_updates": units, "launch": "batched (one launch per step)"}
+    return out
+
+
+def large_gradient_rate(torch, wave, synthetic, dev, cap_bytes=60 * 10**9):
+    """1000 x 3000 (1080 x 3080 padded), 16 shots, 8000 steps, 8th order:
+    gradient within a 60 GB device-memory cap, with bf16 checkpoints (one
+    scale per snapshot), fp24 imaging fields, and as many cached steps as the
+    cap leaves room for."""
+    w = synthetic.large_1000x3000()
+    kw = _model_kwargs(torch, wave, w, dev)
+    kw.pop("vp")
+    vp0 = torch.tensor(w.vp, device=dev)
+    from geobrain_b200.wave import engine
+    torch.cuda.synchronize()
+    base = torch.cuda.memory_allocated(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+
+    def grad():
+        vp = vp0.detach().requires_grad_(True)
+        out = wave.acoustic_forward_kernel(vp=vp, **kw, device=dev, fd_order=8, want_energy=False,
+                                           snapshot_dtype="bf16", imaging_dtype="fp24", memory_budget=cap_bytes)
+        (0.5 * (out["p"] * out["p"]).sum()).backward()
+        return vp.grad
+
+    ms = _timed(torch, grad)
+    peak = torch.cuda.max_memory_allocated(dev) - base
+    geo = engine.Geometry(w.nz, w.nx, w.nabc, w.nt, float(w.dt), float(w.dx), 4, False)
+    plan = engine.get_plan(geo, w.src_x, w.src_z, w.rcv_x, w.rcv_z)
+    K = engine.choose_checkpoint_every(plan, 1, 0, "bf16", False, "fp24")
+    return {"large_1000x3000_16shots_gradient": {
+        "gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms, "nt": w.nt, "shots": w.n_shots,
+        "memory_cap_bytes": cap_bytes, "peak_bytes_above_inputs": int(peak), "checkpoint_every": K,
+        "checkpoints": "bf16, one scale per (checkpoint, shot, field)", "imaging": "fp24"}}
 
 
 if __name__ == "__main__":

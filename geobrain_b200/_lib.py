@@ -55,6 +55,7 @@ SIGNATURES = {
     "gb_plan_destroy": (None, [_P]),
     "gb_plan_set_tiling": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_workspace_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
+    "gb_plan_gradient_workspace_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gb_plan_checkpoint_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_imaging_bytes": (_SZ, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "gb_plan_set_group_streams": (ctypes.c_int, [_P, ctypes.c_int]),

@@ -268,8 +268,12 @@ struct Layout {
     int n_img;
 };
 
-// with_gradient: 0 forward only, 1 velocity gradient, 2 velocity and density.
-Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0)
+size_t img_esize(int f);
+
+// with_gradient: 0 forward only, 1 velocity gradient, 2 velocity and density;
+// checkpoint_every: steps of the recompute segment buffer, whose imaging
+// fields are stored in img_fmt.
+Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0, int img_fmt = GB_IMG_F32)
 {
     Layout L{};
     size_t o = 0;
@@ -288,7 +292,7 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0)
         const size_t K = std::max(1, std::min(checkpoint_every, p->d.nt));
         const size_t G = p->n_groups;
         L.mu = o; o = align256(o + 2 * S * 3 * p->plane * 4);
-        L.img = o; o = align256(o + K * L.n_img * S * p->plane * 4);
+        L.img = o; o = align256(o + K * L.n_img * S * p->plane * img_esize(img_fmt));
         L.g1 = o; o = align256(o + G * p->plane * 4);
         L.c1 = o; o = align256(o + G * p->plane * 4);
         if (with_gradient >= 2) {
@@ -774,6 +778,12 @@ size_t gb_plan_workspace_bytes(const gb_plan *p, int with_gradient, int checkpoi
     return layout(p, with_gradient, checkpoint_every).total + 256;
 }
 
+size_t gb_plan_gradient_workspace_bytes(const gb_plan *p, int with_rho, int segment_steps, int imaging_format)
+{
+    if (!p || !img_format_ok(imaging_format)) return 0;
+    return layout(p, with_rho ? 2 : 1, segment_steps, imaging_format).total + 256;
+}
+
 size_t gb_plan_checkpoint_bytes(const gb_plan *p, int checkpoint_every, int ckpt_format)
 {
     if (!p || checkpoint_every < 1) return 0;
@@ -1033,7 +1043,8 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     const int with_grad = rho_fields ? 2 : 1;
     // recompute segments lie in [0, nt - cached_steps): the segment buffer
     // holds at most that many steps
-    const Layout L = layout(P, with_grad, std::max(1, std::min(K, d.nt - store->cached_steps)));
+    const int ifmt = store->imaging_format;
+    const Layout L = layout(P, with_grad, std::max(1, std::min(K, d.nt - store->cached_steps)), ifmt);
     char *ws = aligned_ws(workspace);
     if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
         return fail(GB_E_WORKSPACE, "workspace too small");
@@ -1044,7 +1055,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     const size_t state_fl = (size_t)S * 3 * P->plane;
     float *fb[2] = {reinterpret_cast<float *>(ws + L.fields), reinterpret_cast<float *>(ws + L.fields) + state_fl};
     float *mu[2] = {reinterpret_cast<float *>(ws + L.mu), reinterpret_cast<float *>(ws + L.mu) + state_fl};
-    float *wimg = reinterpret_cast<float *>(ws + L.img);
+    void *wimg = ws + L.img;      // imaging fields of one recompute segment, in the store's format
     float *G1 = reinterpret_cast<float *>(ws + L.g1), *C1 = reinterpret_cast<float *>(ws + L.c1);
     float *G2 = rho_fields ? reinterpret_cast<float *>(ws + L.g2) : nullptr;
     float *C2 = rho_fields ? reinterpret_cast<float *>(ws + L.c2) : nullptr;
@@ -1063,11 +1074,10 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
 
     const bool fs = d.free_surface != 0;
     const StepKernel KF = fwd_kernel(P->R, P->tz, fs, false, rho_fields ? 2 : 1);
-    const StepKernel KA = adj_kernel(P->R, P->tz, fs, rho_fields, GB_IMG_F32);            // recomputed segments
-    const StepKernel KC = adj_kernel(P->R, P->tz, fs, rho_fields, store->imaging_format);  // cached steps
+    // cached and recomputed imaging fields share the store's format
+    const StepKernel KA = adj_kernel(P->R, P->tz, fs, rho_fields, ifmt);
     if (int rc = prepare_kernel(KF)) return rc;
     if (int rc = prepare_kernel(KA)) return rc;
-    if (int rc = prepare_kernel(KC)) return rc;
     Maps fmaps[2], amaps[2];
     for (int b = 0; b < 2; ++b) {
         if (int rc = make_maps(P, fb[b], Su.a1, Su.a2, &fmaps[b])) return rc;
@@ -1084,6 +1094,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     F.rcv_ptr = Su.d_rptr; F.rcv_ent = Su.d_rent;
     F.err = Su.err;
     F.img_field_stride = (long long)S * P->plane;
+    F.img_fmt = ifmt;
     AdjArgs A{};
     A.g = g;
     A.a1 = Su.a1; A.k1 = Su.k1; A.a2 = Su.a2; A.k2 = Su.k2; A.k3 = Su.k3;
@@ -1113,8 +1124,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
             for (int i = 0; i < gs.n; ++i) {
                 int g0, gc;
                 launch_groups(gs, i, P->n_groups, &g0, &gc);
-                if (int rc = launch_step(P, img_fmt == GB_IMG_F32 ? KA : KC, amaps[cur], A, g0, gc, gs.at(i)))
-                    return rc;
+                if (int rc = launch_step(P, KA, amaps[cur], A, g0, gc, gs.at(i))) return rc;
             }
             cur ^= 1;
         }
@@ -1145,7 +1155,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
             const int b = (it - t0) & 1;
             F.it = it;
             F.out = fb[b ^ 1];
-            F.imaging = wimg + (size_t)(it - t0) * step_img;
+            F.imaging = img_at(wimg, (size_t)(it - t0) * step_img, img_esize(ifmt));
             for (int i = 0; i < gs.n; ++i) {
                 int g0, gc;
                 launch_groups(gs, i, P->n_groups, &g0, &gc);
@@ -1154,7 +1164,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
         }
         if (int rc = join(gs)) return rc;
         P->mark(1, false, st);
-        if (int rc = adjoint_sweep(t0, t1, wimg, GB_IMG_F32)) return rc;
+        if (int rc = adjoint_sweep(t0, t1, wimg, ifmt)) return rc;
     }
     grad_finish_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, G1, C1, G2, C2, P->n_groups, P->plane, d.nz, d.nx, d.nabc,
                                                 P->pitch, grad_vp, grad_rho);

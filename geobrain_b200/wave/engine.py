@@ -95,6 +95,10 @@ class Plan:
     def workspace_bytes(self, with_gradient: bool = False, checkpoint_every: int = 0) -> int:
         return int(self._lib.gb_plan_workspace_bytes(self.h, int(with_gradient), int(checkpoint_every)))
 
+    def gradient_workspace_bytes(self, with_rho: bool, segment_steps: int, imaging_fmt: str = "fp32") -> int:
+        return int(self._lib.gb_plan_gradient_workspace_bytes(self.h, int(bool(with_rho)), int(segment_steps),
+                                                              _lib.IMAGING_FORMATS[imaging_fmt]))
+
     def checkpoint_bytes(self, checkpoint_every: int, fmt: str) -> int:
         return int(self._lib.gb_plan_checkpoint_bytes(self.h, int(checkpoint_every), _lib.CKPT_FORMATS[fmt]))
 
@@ -209,7 +213,7 @@ def pack_output(plan: Plan, p, vx, vz, energies, snaps) -> dict:
 # Gradient: checkpointed forward + hand-written adjoint behind autograd
 # ---------------------------------------------------------------------------
 def choose_checkpoint_every(plan: Plan, checkpoint_segments: int = 1, checkpoint_every: int = 0,
-                            fmt: str = "fp32", with_rho: bool = False) -> int:
+                            fmt: str = "fp32", with_rho: bool = False, imaging_fmt: str = "fp32") -> int:
     """Segment length K: explicit checkpoint_every wins; otherwise the K that
     minimises checkpoint storage + one segment of imaging fields
     (K ~ sqrt(nt * state_bytes / imaging_bytes_per_step)), and never fewer
@@ -218,21 +222,22 @@ def choose_checkpoint_every(plan: Plan, checkpoint_segments: int = 1, checkpoint
     if checkpoint_every > 0:
         return min(int(checkpoint_every), nt)
     state = plan.checkpoint_bytes(nt, fmt)                             # one stored state
-    img_step = plan.imaging_bytes(1, with_rho)                         # imaging fields of one step
+    img_step = plan.imaging_bytes(1, with_rho, imaging_fmt)            # imaging fields of one step
     k = int(max(1, round(math.sqrt(nt * state / max(img_step, 1.0)))))
     k = min(k, max(1, -(-nt // max(1, checkpoint_segments))))
     return max(1, min(k, nt))
 
 
 def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device, imaging_fmt: str = "fp32",
-                        checkpoint_every: int = 1, ckpt_fmt: str = "fp32") -> int:
+                        checkpoint_every: int = 1, ckpt_fmt: str = "fp32", memory_budget: Optional[int] = None) -> int:
     """How many of the last time steps keep their imaging fields from the
     forward (those steps skip the recompute).  imaging_cache: a byte budget,
     0, or 'auto': the most steps for which the cache, the checkpoints of the
     remaining steps, the workspaces, the trace gradients and a margin (2 GiB
     + 5 %) fit in the device memory available right now, counting blocks the
     caching allocator holds unused (GEOBRAIN_B200_IMAGING_CACHE_BYTES
-    overrides it with a byte budget)."""
+    overrides it with a byte budget).  memory_budget caps that available
+    memory (bytes the whole gradient may hold beyond what is allocated now)."""
     nt = plan.geo.nt
     per = max(plan.imaging_bytes(1, with_rho, imaging_fmt), 1)
     if imaging_cache in (None, 0, False):
@@ -245,6 +250,8 @@ def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device, imagi
     free, _ = torch.cuda.mem_get_info(device)
     # blocks torch's allocator holds but does not use are free for this too
     avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+    if memory_budget is not None:
+        avail = min(avail, int(memory_budget))
     K = max(1, min(int(checkpoint_every), nt))
     one_ck = plan.checkpoint_bytes(nt, ckpt_fmt)                      # one stored state
     fixed = 3 * plan.n_shots * nt * plan.n_rcv * 4 + (2 << 30) + avail // 20
@@ -252,7 +259,7 @@ def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device, imagi
     def need(c: int) -> int:
         rest = nt - c
         seg = max(1, min(K, rest))
-        return (c * per + -(-rest // K) * one_ck + plan.workspace_bytes(2 if with_rho else 1, seg) +
+        return (c * per + -(-rest // K) * one_ck + plan.gradient_workspace_bytes(with_rho, seg, imaging_fmt) +
                 plan.workspace_bytes(0, 0) + fixed)
 
     if need(nt) <= avail:                # no recompute at all (no segment buffer either)
@@ -276,7 +283,8 @@ def run_backward(plan: Plan, vp, rho, damp, src_v, res_p, res_vx, res_vz, store:
     grad_vp = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32)
     grad_rho = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32) if want_rho else None
     seg = max(1, min(store.checkpoint_every, g.nt - store.cached_steps))    # steps of one recompute segment
-    ws = workspace(plan.workspace_bytes(2 if store.with_rho else 1, seg), dev)
+    ifmt = {v: k for k, v in _lib.IMAGING_FORMATS.items()}[store.imaging_format]
+    ws = workspace(plan.gradient_workspace_bytes(bool(store.with_rho), seg, ifmt), dev)
     with torch.cuda.device(dev):
         rc = plan._lib.gb_backward(plan.h, vp.data_ptr(), rho.data_ptr(), damp.data_ptr(), src_v.data_ptr(),
                                    _lib.ptr(res_p), _lib.ptr(res_vx), _lib.ptr(res_vz), ctypes.byref(store),
@@ -338,7 +346,8 @@ class AcousticFunction(torch.autograd.Function):
 
 def differentiable_forward(plan: Plan, vp, rho, damp, src_v, *, device, snapshot_every: int = 0,
                            checkpoint_segments: int = 1, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
-                           want_energy: bool = True, imaging_cache="auto", imaging_dtype: str = "fp32") -> dict:
+                           want_energy: bool = True, imaging_cache="auto", imaging_dtype: str = "fp32",
+                           memory_budget: Optional[int] = None) -> dict:
     if snapshot_dtype not in _lib.CKPT_FORMATS:
         raise ValueError(f"snapshot_dtype must be one of {sorted(_lib.CKPT_FORMATS)}")
     if imaging_dtype not in _lib.IMAGING_FORMATS:
@@ -349,8 +358,9 @@ def differentiable_forward(plan: Plan, vp, rho, damp, src_v, *, device, snapshot
     for name, t in (("vp", vp_t), ("rho", rho_t)):
         if t.device != device:
             raise ValueError(f"{name} is on {t.device}, expected {device}")
-    K = choose_checkpoint_every(plan, checkpoint_segments, checkpoint_every, snapshot_dtype, need_rho)
-    cached = choose_cached_steps(plan, imaging_cache, need_rho, device, imaging_dtype, K, snapshot_dtype)
+    K = choose_checkpoint_every(plan, checkpoint_segments, checkpoint_every, snapshot_dtype, need_rho, imaging_dtype)
+    cached = choose_cached_steps(plan, imaging_cache, need_rho, device, imaging_dtype, K, snapshot_dtype,
+                                 memory_budget)
     opts = dict(checkpoint_every=K, fmt=snapshot_dtype, want_energy=want_energy, snapshot_every=snapshot_every,
                 with_rho=need_rho, cached_steps=cached, imaging_fmt=imaging_dtype)
     p, vx, vz, e0, e1, e2, snaps = AcousticFunction.apply(vp_t, rho_t, plan, damp, src_v, opts)

@@ -14,7 +14,9 @@ behaviour: fd_order (4 or 8); checkpoint_every, snapshot_dtype ('fp32',
 'bf16', 'fp16'), imaging_cache ('auto', a byte budget, or 0) and
 imaging_dtype ('fp32'; 'fp24', 3 bytes, gradient error about 1e-5; 'bf16',
 2 bytes, about 3e-3: more cached steps skip the recompute) for the
-gradient's memory; want_energy (skip the energy sums); autotune (on the
+gradient's memory, and memory_budget (bytes the gradient's store and
+workspaces may take, for the 'auto' cache); want_energy (skip the energy
+sums); autotune (on the
 first call for a geometry, time the launch configurations and keep the
 fastest; GEOBRAIN_B200_AUTOTUNE=1 turns it on by default).
 """
@@ -53,7 +55,7 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
                             dtype: torch.dtype = torch.float32, snapshot_every: int = 0, *,
                             fd_order: int = 4, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
                             want_energy: bool = True, imaging_cache="auto", imaging_dtype: str = "fp32",
-                            autotune: Optional[bool] = None):
+                            autotune: Optional[bool] = None, memory_budget: Optional[int] = None):
     device = torch.device(device)
     if device.type != "cuda":
         raise ValueError(f"geobrain_b200 runs on CUDA devices only (device={device})")
@@ -103,7 +105,8 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
                                              checkpoint_segments=int(checkpoint_segments),
                                              checkpoint_every=int(checkpoint_every),
                                              snapshot_dtype=snapshot_dtype, want_energy=want_energy,
-                                             imaging_cache=imaging_cache, imaging_dtype=imaging_dtype)
+                                             imaging_cache=imaging_cache, imaging_dtype=imaging_dtype,
+                                             memory_budget=memory_budget)
     vp_t = _as_f32(vp.detach() if torch.is_tensor(vp) else vp, device, "vp")
     rho_t = _as_f32(rho.detach() if torch.is_tensor(rho) else rho, device, "rho")
     p, vx, vz, en, snaps = engine.run_forward(plan, vp_t, rho_t, damp_t, w, want_energy=want_energy,

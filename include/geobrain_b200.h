@@ -144,6 +144,14 @@ int gb_plan_set_group_streams(gb_plan *plan, int enable);
  * gradient's.  The workspace is used from its first 256-byte boundary. */
 size_t gb_plan_workspace_bytes(const gb_plan *plan, int with_gradient, int checkpoint_every);
 
+/* The exact workspace gb_backward needs for a store: its recompute segment
+ * buffer holds segment_steps = max(1, min(checkpoint_every, nt -
+ * cached_steps)) steps of imaging fields in the store's imaging_format (the
+ * recomputed fields are rounded like the cached ones).  gb_plan_workspace_bytes
+ * with with_gradient > 0 is the fp32 upper bound of it. */
+size_t gb_plan_gradient_workspace_bytes(const gb_plan *plan, int with_rho, int segment_steps,
+                                        int imaging_format);
+
 /* Bytes of checkpoint storage for a given segment length and format. */
 size_t gb_plan_checkpoint_bytes(const gb_plan *plan, int checkpoint_every, int ckpt_format);
 
@@ -177,9 +185,9 @@ int gb_forward(gb_plan *plan, const float *vp, const float *rho, const float *da
  * over shots and time with compensated fp32 summation and folds the padding
  * back into the edge cells (the adjoint of pad_model).  grad_vp / grad_rho
  * are (nz, nx) float32 and are overwritten; grad_rho may be NULL (it needs a
- * store made with with_rho).  Workspace: gb_plan_workspace_bytes(plan,
- * with_rho ? 2 : 1, min(checkpoint_every, nt - cached_steps)) (at least 1
- * step: the recompute segments only cover the uncached steps). */
+ * store made with with_rho).  Workspace: gb_plan_gradient_workspace_bytes
+ * (the recompute segments only cover the uncached steps, and their imaging
+ * fields are kept in the store's imaging_format). */
 int gb_backward(gb_plan *plan, const float *vp, const float *rho, const float *damp,
                 const float *wavelet,
                 const float *res_p, const float *res_vx, const float *res_vz,
