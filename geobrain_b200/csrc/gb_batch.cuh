@@ -30,17 +30,18 @@ struct BatchModel {
     float *fld[2];           // forward state levels
     float *mu[2];            // adjoint state levels
     float *cache;            // imaging cache of steps >= t_cache, or null
-    float *segimg;           // imaging fields of the segment being recomputed (fp32)
+    float *segimg;           // imaging fields of the segment being recomputed (cache_fmt)
     long long step_img;      // elements per step of imaging fields
     int nt, t_cache, K;
     int cache_fmt;           // storage format of the cache (kImg*)
 };
 
-// Step `j` of the imaging cache (elements of 2, 3 or 4 bytes).
-__device__ __forceinline__ float *cache_step(const BatchModel &M, int j)
+// Step `j` of an imaging buffer in the model's format (elements of 2, 3 or
+// 4 bytes): the cache, or the recompute segment's buffer.
+__device__ __forceinline__ float *img_step(const BatchModel &M, float *base, int j)
 {
     const int es = M.cache_fmt == kImgBF16 ? 2 : M.cache_fmt == kImgF24 ? 3 : 4;
-    return reinterpret_cast<float *>(reinterpret_cast<char *>(M.cache) + (long long)j * M.step_img * es);
+    return reinterpret_cast<float *>(reinterpret_cast<char *>(base) + (long long)j * M.step_img * es);
 }
 
 constexpr int kBatchForward = 0;
@@ -62,11 +63,11 @@ fwd_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ 
         A.it = tau;
         A.out = M.fld[par ^ 1];
         if (mode == kBatchForward) {
-            A.imaging = (M.cache && tau >= M.t_cache) ? cache_step(M, tau - M.t_cache) : nullptr;
+            A.imaging = (M.cache && tau >= M.t_cache) ? img_step(M, M.cache, tau - M.t_cache) : nullptr;
             A.img_fmt = M.cache_fmt;
         } else {
-            A.imaging = M.segimg + (long long)(tau - t0) * M.step_img;
-            A.img_fmt = 0;
+            A.imaging = img_step(M, M.segimg, tau - t0);
+            A.img_fmt = M.cache_fmt;
             A.energy = nullptr;
             A.tr_p = A.tr_vx = A.tr_vz = nullptr;
         }
@@ -92,8 +93,8 @@ adj_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ 
         A.it = tau;
         A.out = M.mu[par ^ 1];
         const bool cached = M.cache && tau >= M.t_cache;
-        A.img = cached ? cache_step(M, tau - M.t_cache) : M.segimg + (long long)(tau - (tau / M.K) * M.K) * M.step_img;
-        A.img_fmt = cached ? M.cache_fmt : 0;
+        A.img = cached ? img_step(M, M.cache, tau - M.t_cache) : img_step(M, M.segimg, tau - (tau / M.K) * M.K);
+        A.img_fmt = M.cache_fmt;
     }
     __syncthreads();
     const BatchMaps &mp = maps[item.x];

@@ -1484,7 +1484,9 @@ int gb_batch_backward(gb_plan *const *plans, int n, const gb_model_io *io, void 
         gb_plan *P = plans[m];
         const gb_model_io &x = io[m];
         const int Km = std::min<int>(K, P->d.nt);
-        const Layout L = layout(P, rho ? 2 : 1, Km);
+        // the segment buffer holds at most the uncached steps, in the store's format
+        const int seg = std::max(1, std::min(Km, P->d.nt - x.store->cached_steps));
+        const Layout L = layout(P, rho ? 2 : 1, seg, x.store->imaging_format);
         Ls.push_back(L);
         char *ws = aligned_ws(x.workspace);
         if (x.workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(x.workspace)))

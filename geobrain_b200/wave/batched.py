@@ -58,7 +58,6 @@ class _Prepared:
                                   float(m["dx"]), engine.FD_ORDERS[fd_order], fs0)
             plan = engine.get_plan(geo, engine._i64(m["src_x"])[:src_n], engine._i64(m["src_z"])[:src_n],
                                    engine._i64(m["rcv_x"])[:rcv_n], engine._i64(m["rcv_z"])[:rcv_n])
-            plan.set_tiling(BATCH_TILE_ROWS, min(plan.n_shots, 8))
             w = _as_f32(m["src_v"], device, "src_v")
             if w.dim() == 1:
                 w = w.unsqueeze(0).expand(src_n, -1)
@@ -66,6 +65,10 @@ class _Prepared:
             damp = _as_f32(m["damp"], device, "damp")
             self.plans.append(plan)
             self.inputs.append((m["vp"], m["rho"], damp, w))
+        for plan in self.plans:
+            # up to 8 shots per CTA: fewer, longer CTAs measured faster than
+            # more, shorter ones even for small models
+            plan.set_tiling(BATCH_TILE_ROWS, min(plan.n_shots, 8))
         self.plan_arr = (ctypes.c_void_p * len(self.plans))(*[p.h.value for p in self.plans])
 
 
@@ -147,7 +150,8 @@ class _BatchFunction(torch.autograd.Function):
             gvp = torch.empty((g.nz, g.nx), device=dev)
             grho = torch.empty((g.nz, g.nx), device=dev) if (need_rho and ctx.stores[i].with_rho) else None
             st = ctx.stores[i]
-            ws = engine.workspace(plan.workspace_bytes(2 if st.with_rho else 1, st.checkpoint_every), dev)
+            seg = max(1, min(st.checkpoint_every, g.nt - st.cached_steps))
+            ws = engine.workspace(plan.gradient_workspace_bytes(bool(st.with_rho), seg, ctx.opts["imaging_fmt"]), dev)
             _, _, damp, w = prep.inputs[i]
             io = ios[i]
             io.vp, io.rho, io.damp, io.wavelet = vps[i].data_ptr(), rhos[i].data_ptr(), damp.data_ptr(), w.data_ptr()
@@ -166,6 +170,42 @@ class _BatchFunction(torch.autograd.Function):
         out_vp = [g if ctx.needs_input_grad[2 + i] else None for i, g in enumerate(gv)]
         out_rho = [g if ctx.needs_input_grad[2 + n + i] else None for i, g in enumerate(gr)]
         return (None, None, *out_vp, *out_rho)
+
+
+def _auto_cache_fraction(prep: _Prepared, per_step, K: int, fmt: str, imaging_fmt: str, with_rho: bool,
+                         device) -> float:
+    """The largest fraction f of every model's steps whose imaging fields the
+    forward can keep: the caches, the checkpoints of the other steps, the
+    workspaces, the traces and their gradients and a margin (2 GiB + 5 %)
+    must fit in the device memory available now."""
+    free, _ = torch.cuda.mem_get_info(device)
+    avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+    traces = sum(4 * p.n_shots * p.geo.nt * p.n_rcv * 4 for p in prep.plans)   # 3 trace fields + one gradient
+    fixed = traces + (2 << 30) + avail // 20 + sum(p.workspace_bytes(False, 0) for p in prep.plans)
+
+    def need(f: float) -> int:
+        tot = fixed
+        for p, per in zip(prep.plans, per_step):
+            nt = p.geo.nt
+            c = int(f * nt)
+            rest = nt - c
+            k = max(1, min(K, nt))
+            tot += (c * per + -(-rest // k) * p.checkpoint_bytes(nt, fmt) +
+                    p.gradient_workspace_bytes(with_rho, max(1, min(k, rest)), imaging_fmt))
+        return tot
+
+    if need(1.0) <= avail:
+        return 1.0
+    lo, hi = 0.0, 1.0
+    if need(0.0) > avail:
+        return 0.0
+    for _ in range(24):
+        mid = 0.5 * (lo + hi)
+        if need(mid) <= avail:
+            lo = mid
+        else:
+            hi = mid
+    return lo
 
 
 def acoustic_forward_batched(models: Sequence[dict], *, fd_order: int = 8, device=None, want_energy: bool = True,
@@ -194,7 +234,8 @@ def acoustic_forward_batched(models: Sequence[dict], *, fd_order: int = 8, devic
             outs.append(engine.pack_output(plan, tr[0], tr[1], tr[2], en, None))
         return outs
     with_rho = any(r.requires_grad for r in rhos)
-    K = max(engine.choose_checkpoint_every(p, 1, checkpoint_every, snapshot_dtype, with_rho) for p in prep.plans)
+    K = max(engine.choose_checkpoint_every(p, 1, checkpoint_every, snapshot_dtype, with_rho, imaging_dtype)
+            for p in prep.plans)
     # split the imaging-cache budget over the models in proportion to their steps
     if imaging_cache in (0, None, False):
         cached = [0] * len(prep.plans)
@@ -203,13 +244,10 @@ def acoustic_forward_batched(models: Sequence[dict], *, fd_order: int = 8, devic
             raise ValueError(f"imaging_dtype must be one of {sorted(_lib.IMAGING_FORMATS)}")
         per_step = [p.imaging_bytes(1, with_rho, imaging_dtype) for p in prep.plans]
         if imaging_cache == "auto":
-            free, _ = torch.cuda.mem_get_info(device)
-            avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
-            budget = int(avail * 0.5)
+            frac = _auto_cache_fraction(prep, per_step, K, snapshot_dtype, imaging_dtype, with_rho, device)
         else:
-            budget = int(imaging_cache)
-        total = sum(p.geo.nt * b for p, b in zip(prep.plans, per_step))
-        frac = min(1.0, budget / max(total, 1))
+            total = sum(p.geo.nt * b for p, b in zip(prep.plans, per_step))
+            frac = min(1.0, int(imaging_cache) / max(total, 1))
         cached = [int(frac * p.geo.nt) for p in prep.plans]
     opts = dict(K=K, fmt=snapshot_dtype, with_rho=with_rho, want_energy=want_energy, cached=cached,
                 imaging_fmt=imaging_dtype)
