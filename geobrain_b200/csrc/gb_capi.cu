@@ -5,6 +5,7 @@
 #include "gb_adj.cuh"
 #include "gb_aux.cuh"
 #include "gb_batch.cuh"
+#include "gb_misfit.cuh"
 #include "gb_fwd.cuh"
 
 #include <cudaTypedefs.h>
@@ -929,6 +930,22 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
             ++P->launches;
         }
     P->mark(0, false, st);
+    return GB_OK;
+}
+
+int gb_trace_misfit(const float *pred, const float *obs, int32_t n_shots, int32_t nt, int32_t n_rcv, float *adj,
+                    float *per_trace, float *loss, void *stream)
+{
+    g_last_error.clear();
+    if (!pred || !obs || !per_trace || !loss) return fail(GB_E_ARG, "null argument");
+    if (n_shots < 1 || nt < 1 || n_rcv < 1) return fail(GB_E_ARG, "n_shots, nt and n_rcv must be >= 1");
+    if (n_shots > 65535) return fail(GB_E_ARG, "at most 65535 shots per call");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    dim3 grid((n_rcv + 127) / 128, n_shots);
+    trace_misfit_kernel<<<grid, 128, 0, st>>>(pred, obs, nt, n_rcv, adj, per_trace);
+    GB_CUDA(cudaGetLastError());
+    trace_misfit_sum_kernel<<<1, 1024, 0, st>>>(per_trace, (long long)n_shots * n_rcv, loss);
+    GB_CUDA(cudaGetLastError());
     return GB_OK;
 }
 

@@ -17,7 +17,7 @@ create_wavelet, bc_pml, create_boundary and kernels.acoustic_forward_kernel /
 kernels.pad_model; the compute runs in hand-written sm_100a CUDA kernels.
 """
 from . import kernel as kernels
-from . import sharding
+from . import misfit, sharding
 from .batched import AcousticBatch, acoustic_forward_batched
 from .boundary import bc_pml, create_boundary
 from .config import BoundaryConfig, GridConfig, SolverConfig, TimeConfig, WaveletConfig
@@ -34,5 +34,5 @@ __all__ = [
     "WaveletGenerator", "RickerWavelet", "GaussianWavelet", "create_wavelet",
     "bc_pml", "create_boundary", "Source", "Receiver", "Survey", "AcousticPropagator",
     "numpy2tensor", "kernels", "acoustic_forward_kernel", "pad_model",
-    "AcousticBatch", "acoustic_forward_batched", "sharding",
+    "AcousticBatch", "acoustic_forward_batched", "sharding", "misfit",
 ]

@@ -232,6 +232,23 @@ int gb_batch_forward(gb_plan *const *plans, int n_models, const gb_model_io *io,
 int gb_batch_backward(gb_plan *const *plans, int n_models, const gb_model_io *io,
                       void *batch_workspace, size_t batch_workspace_bytes, void *stream);
 
+/* Trace-normalised L2 misfit and its adjoint source, on the device.  It
+ * replaces the misfit of examples/09_acoustic_fwi.py:290-319:
+ * normalize_traces, per_trace_l2, active_mask.  For pred and obs of shape
+ * (n_shots, nt, n_rcv), float32:
+ *   - each trace is divided by its max |value| (clamped to 1e-30);
+ *   - the per-trace L2 norm of obs_n - pred_n is summed over the traces
+ *     that are not silent in both.
+ * Outputs:
+ *   - loss: one float32 on the device, summed in fp64 in a fixed order;
+ *   - per_trace: (n_shots, n_rcv) float32, the L_j, 0 for silent traces;
+ *   - adj: same shape as pred, may be NULL; d loss / d pred, including the
+ *     gradient of each trace's max.  It is the residual gb_backward takes.
+ *     Silent traces and traces with L_j = 0 get zeros; autograd through the
+ *     example's expression gives NaN there. */
+int gb_trace_misfit(const float *pred, const float *obs, int32_t n_shots, int32_t nt, int32_t n_rcv,
+                    float *adj, float *per_trace, float *loss, void *stream);
+
 /* Synchronises `stream` and reports the device-side status word of a
  * workspace after gb_forward / gb_backward: GB_OK, or GB_E_TIMEOUT if a
  * bounded wait inside a kernel gave up. */
