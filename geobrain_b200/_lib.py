@@ -63,7 +63,9 @@ SIGNATURES = {
     "gb_trace_misfit": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P, _P, _P]),
     "gb_plan_autotune_workspace_bytes": (_SZ, [_P]),
     "gb_plan_get_config": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
-                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+                                          ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int)]),
+    "gb_plan_set_streaming": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_autotune": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _I32, _P, ctypes.POINTER(ctypes.c_float)]),
     "gb_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P, _P, _SZ, _P]),
     "gb_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),

@@ -6,6 +6,7 @@
 #include "gb_aux.cuh"
 #include "gb_batch.cuh"
 #include "gb_misfit.cuh"
+#include "gb_stream.cuh"
 #include "gb_fwd.cuh"
 
 #include <cudaTypedefs.h>
@@ -128,6 +129,20 @@ struct gb_plan {
     long long phase_steps[3] = {0, 0, 0};                     // time steps run per phase
     // plain forward as replays of a CUDA graph of graph_steps steps (0 = off)
     int graph_steps = 16;
+    // forward steps by the streaming kernel (gb_stream.cuh): off, or on with
+    // stream_chunks 16-row chunks per z-segment (0 = automatic)
+    bool stream = false;
+    int stream_chunks = 0;
+    bool stream_usable() const { return stream && !d.free_surface && tz == 16; }
+    int seg_chunks() const
+    {
+        if (stream_chunks > 0) return stream_chunks;
+        // enough segments for four waves of two CTAs per SM over all shots
+        const long long want = 4LL * 2 * 148;
+        const long long per_seg = (long long)tiles_x * d.n_shots;
+        const int n_seg = (int)std::max<long long>(1, (want + per_seg - 1) / per_seg);
+        return std::max(2, (tiles_z + n_seg - 1) / n_seg);
+    }
     cudaStream_t cap_stream = nullptr;                         // capture origin (never the legacy stream)
     cudaGraphExec_t gexec = nullptr;
     std::vector<uintptr_t> gkey;                               // what the instantiated graph baked in
@@ -330,7 +345,28 @@ void *fwd_pick3(bool fs, bool en, int img)
 struct StepKernel {
     void *fn;
     size_t smem;
+    bool stream = false;    // fwd_stream_kernel: launched over (strip, segment, shot)
 };
+
+template <int R>
+void *fwd_stream_pick(bool en, int img)
+{
+    if (img == 1) return en ? (void *)&fwd_stream_kernel<R, true, 1> : (void *)&fwd_stream_kernel<R, false, 1>;
+    if (img == 2) return en ? (void *)&fwd_stream_kernel<R, true, 2> : (void *)&fwd_stream_kernel<R, false, 2>;
+    return en ? (void *)&fwd_stream_kernel<R, true, 0> : (void *)&fwd_stream_kernel<R, false, 0>;
+}
+
+// The plan's forward step kernel: the streaming one when the plan asks for it
+// (no free surface, 16-row tiles), else the tile kernel.
+StepKernel fwd_kernel(int R, int tz, bool fs, bool en, int im);
+StepKernel fwd_kernel_for(const gb_plan *P, bool en, int im)
+{
+    if (P->stream_usable()) {
+        StepKernel k{P->R == 2 ? fwd_stream_pick<2>(en, im) : fwd_stream_pick<4>(en, im), kStreamSmemBytes, true};
+        return k;
+    }
+    return fwd_kernel(P->R, P->tz, P->d.free_surface != 0, en, im);
+}
 
 StepKernel fwd_kernel(int R, int tz, bool fs, bool en, int im)
 {
@@ -385,6 +421,7 @@ int box_rows_vz(int R, int tz) { return tz + 4 * R; }
 
 struct Maps {
     CUtensorMap p, vx, vz, a1, a2;
+    CUtensorMap sp, svx, svz, sa1, sa2;   // 16-row blocks for the streaming kernel (when the plan uses it)
 };
 
 // Field maps over one state buffer plus the a1 / a2 coefficient maps.
@@ -395,6 +432,13 @@ int make_maps(const gb_plan *P, const float *buf, const float *a1, const float *
     if (int rc = make_map(&m->vx, buf, P->Nx, P->Nz, P->pitch, n_planes, VXW, box_rows_p(P->R, P->tz))) return rc;
     if (int rc = make_map(&m->vz, buf, P->Nx, P->Nz, P->pitch, n_planes, RW, box_rows_vz(P->R, P->tz))) return rc;
     if (int rc = make_map2d(&m->a1, a1, P->Nx, P->Nz, P->pitch, RW, box_rows_p(P->R, P->tz))) return rc;
+    if (P->stream_usable()) {
+        if (int rc = make_map(&m->sp, buf, P->Nx, P->Nz, P->pitch, n_planes, RW, SCH)) return rc;
+        if (int rc = make_map(&m->svx, buf, P->Nx, P->Nz, P->pitch, n_planes, VXW, SCH)) return rc;
+        if (int rc = make_map(&m->svz, buf, P->Nx, P->Nz, P->pitch, n_planes, RW, SCH)) return rc;
+        if (int rc = make_map2d(&m->sa1, a1, P->Nx, P->Nz, P->pitch, RW, SCH)) return rc;
+        if (int rc = make_map2d(&m->sa2, a2, P->Nx, P->Nz, P->pitch, RW, SCH)) return rc;
+    }
     return make_map2d(&m->a2, a2, P->Nx, P->Nz, P->pitch, RW, P->tz);
 }
 
@@ -420,6 +464,25 @@ int launch_step(gb_plan *P, const StepKernel &K, const Maps &maps, Args A, int g
     void *args[] = {(void *)&maps.p, (void *)&maps.vx, (void *)&maps.vz, (void *)&maps.a1, (void *)&maps.a2,
                     (void *)&A};
     dim3 grid(P->n_tiles * grp_count), block(NTHR);
+    GB_CUDA(cudaLaunchKernel(K.fn, grid, block, args, K.smem, st));
+    ++P->launches;
+    return GB_OK;
+}
+
+// Forward launches: the tile kernel as above, or the streaming kernel over
+// (strip, segment, shot) for the shots of groups [grp0, grp0 + grp_count).
+int launch_step(gb_plan *P, const StepKernel &K, const Maps &maps, FwdArgs A, int grp0, int grp_count,
+                cudaStream_t st)
+{
+    if (!K.stream) return launch_step<FwdArgs>(P, K, maps, A, grp0, grp_count, st);
+    StreamArgs SA;
+    SA.shot0 = P->group_first(grp0);
+    SA.n_shots = std::min(P->d.n_shots, P->group_first(grp0 + grp_count)) - SA.shot0;
+    SA.seg_chunks = P->seg_chunks();
+    SA.n_seg = (P->tiles_z + SA.seg_chunks - 1) / SA.seg_chunks;
+    void *args[] = {(void *)&maps.sp,  (void *)&maps.svx, (void *)&maps.svz, (void *)&maps.sa1,
+                    (void *)&maps.sa2, (void *)&A,         (void *)&SA};
+    dim3 grid((unsigned)P->tiles_x * SA.n_seg * SA.n_shots), block(NTHR);
     GB_CUDA(cudaLaunchKernel(K.fn, grid, block, args, K.smem, st));
     ++P->launches;
     return GB_OK;
@@ -753,13 +816,25 @@ int gb_plan_set_group_streams(gb_plan *p, int enable)
     return GB_OK;
 }
 
-int gb_plan_get_config(const gb_plan *p, int *tile_rows, int *shots_per_cta, int *group_streams, int *graph_steps)
+int gb_plan_get_config(const gb_plan *p, int *tile_rows, int *shots_per_cta, int *group_streams, int *graph_steps,
+                       int *stream_chunks)
 {
     if (!p) return fail(GB_E_ARG, "null plan");
     if (tile_rows) *tile_rows = p->tz;
     if (shots_per_cta) *shots_per_cta = p->spc_eff;
     if (group_streams) *group_streams = p->group_streams ? 1 : 0;
     if (graph_steps) *graph_steps = p->graph_steps;
+    if (stream_chunks) *stream_chunks = p->stream_usable() ? p->seg_chunks() : 0;
+    return GB_OK;
+}
+
+int gb_plan_set_streaming(gb_plan *p, int enable, int seg_chunks)
+{
+    if (!p) return fail(GB_E_ARG, "null plan");
+    if (seg_chunks < 0) return fail(GB_E_ARG, "seg_chunks must be >= 0");
+    p->stream = enable != 0;
+    p->stream_chunks = seg_chunks;
+    p->release_graph();
     return GB_OK;
 }
 
@@ -830,8 +905,8 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
     if (want_energy) GB_CUDA(cudaMemsetAsync(energy, 0, 3 * P->plane * 4, st));
 
     const bool fs = d.free_surface != 0;
-    const StepKernel K0 = fwd_kernel(P->R, P->tz, fs, want_energy, 0);
-    const StepKernel KI = fwd_kernel(P->R, P->tz, fs, want_energy, n_img == 3 ? 2 : 1);
+    const StepKernel K0 = fwd_kernel_for(P, want_energy, 0);
+    const StepKernel KI = fwd_kernel_for(P, want_energy, n_img == 3 ? 2 : 1);
     if (int rc = prepare_kernel(K0)) return rc;
     if (store && store->cached_steps > 0)
         if (int rc = prepare_kernel(KI)) return rc;
@@ -975,8 +1050,9 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         int tz, spc;
         bool streams;
         int graph;
+        bool stream;
     };
-    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps};
+    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps, P->stream};
     const bool prof = P->prof;
     const int nt = P->d.nt;
     const long long launches = P->launches;
@@ -984,14 +1060,17 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
     const int C = 16;
     const int n = steps >= C ? steps / C * C : steps;       // whole graph chunks when graphs are tried
     std::vector<Config> cands;
-    for (int tz : {16, 32})
-        for (int spc : {0, 1, 2, 4, 8, 16}) {
-            if (spc > S) continue;
-            for (int streams = 1; streams >= 0; --streams)
-                for (int graph : {0, C}) {
-                    if (graph > n) continue;
-                    cands.push_back({tz, spc, streams != 0, graph});
-                }
+    for (int stream = 0; stream <= (P->d.free_surface ? 0 : 1); ++stream)
+        for (int tz : {16, 32}) {
+            if (stream && tz != 16) continue;      // the streaming kernel walks 16-row chunks
+            for (int spc : {0, 1, 2, 4, 8, 16}) {
+                if (spc > S) continue;
+                for (int streams = 1; streams >= 0; --streams)
+                    for (int graph : {0, C}) {
+                        if (graph > n) continue;
+                        cands.push_back({tz, spc, streams != 0, graph, stream != 0});
+                    }
+            }
         }
     cudaEvent_t e0, e1;
     GB_CUDA(cudaEventCreate(&e0));
@@ -1007,6 +1086,7 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         P->retile();
         P->group_streams = k.streams;
         P->graph_steps = k.graph;
+        P->stream = k.stream;
         P->release_graph();
         if (gb_plan_workspace_bytes(P, 0, 0) > workspace_bytes) continue;
         if (k.streams && P->n_groups == 1) continue;      // same as without
@@ -1038,6 +1118,7 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
     P->retile();
     P->group_streams = win.streams;
     P->graph_steps = win.graph;
+    P->stream = win.stream;
     P->release_graph();                // captured with the shortened step count
     if (rc != GB_OK) return rc;
     if (best < 0) return fail(GB_E_WORKSPACE, "no candidate fits the workspace");
@@ -1090,7 +1171,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     }
 
     const bool fs = d.free_surface != 0;
-    const StepKernel KF = fwd_kernel(P->R, P->tz, fs, false, rho_fields ? 2 : 1);
+    const StepKernel KF = fwd_kernel_for(P, false, rho_fields ? 2 : 1);
     // cached and recomputed imaging fields share the store's format
     const StepKernel KA = adj_kernel(P->R, P->tz, fs, rho_fields, ifmt);
     if (int rc = prepare_kernel(KF)) return rc;

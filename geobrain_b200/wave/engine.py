@@ -132,11 +132,15 @@ class Plan:
         return self.tuned
 
     def config(self) -> dict:
-        tz, spc, streams, graph = (ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int())
+        tz, spc, streams, graph, chunks = (ctypes.c_int() for _ in range(5))
         _lib.check(self._lib.gb_plan_get_config(self.h, ctypes.byref(tz), ctypes.byref(spc), ctypes.byref(streams),
-                                                ctypes.byref(graph)))
+                                                ctypes.byref(graph), ctypes.byref(chunks)))
         return {"tile_rows": tz.value, "shots_per_cta": spc.value, "group_streams": bool(streams.value),
-                "graph_steps": graph.value}
+                "graph_steps": graph.value, "stream_chunks": chunks.value}
+
+    def set_streaming(self, enable: bool, seg_chunks: int = 0) -> None:
+        """Forward steps by the streaming kernel (0 chunks = automatic)."""
+        _lib.check(self._lib.gb_plan_set_streaming(self.h, int(bool(enable)), int(seg_chunks)))
 
 
 def get_plan(geo: Geometry, src_x, src_z, rcv_x, rcv_z) -> Plan:

@@ -118,7 +118,8 @@ int gb_plan_set_graph_steps(gb_plan *plan, int steps);
  *   - tile rows 16 / 32;
  *   - shots per CTA automatic, 1, 2, 4, 8 or 16;
  *   - per-group streams on / off;
- *   - graph chunks of 16 steps or none.
+ *   - graph chunks of 16 steps or none;
+ *   - the streaming forward kernel or the tile kernel.
  * It keeps the fastest on the plan and reports its time per step.  Each
  * candidate runs three times; the first is a warm-up.  The workspace must
  * hold gb_plan_autotune_workspace_bytes(plan); candidates that do not fit
@@ -126,9 +127,19 @@ int gb_plan_set_graph_steps(gb_plan *plan, int steps);
 size_t gb_plan_autotune_workspace_bytes(gb_plan *plan);
 
 /* The launch configuration in use (what the autotuner chose): tile rows,
- * effective shots per CTA, per-group streams, graph chunk steps. */
+ * effective shots per CTA, per-group streams, graph chunk steps, and the
+ * streaming kernel's chunks per z-segment (0 when the tile kernel runs). */
 int gb_plan_get_config(const gb_plan *plan, int *tile_rows, int *shots_per_cta, int *group_streams,
-                       int *graph_steps);
+                       int *graph_steps, int *stream_chunks);
+
+/* Forward (and recompute) steps by the streaming kernel: one CTA walks a
+ * 120-column strip of one shot down a z-segment of seg_chunks 16-row chunks
+ * (0 = automatic), keeping the rows it has in shared-memory rings, so that
+ * each pressure row is updated once instead of once per tile plus a halo.
+ * Same results as the tile kernel, bit for bit.  Used when enabled, the
+ * tiles are 16 rows and the model has no free surface; otherwise the tile
+ * kernel runs.  Off by default; the autotuner tries it. */
+int gb_plan_set_streaming(gb_plan *plan, int enable, int seg_chunks);
 int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const float *damp,
                      const float *wavelet, void *workspace, size_t workspace_bytes, int32_t steps,
                      void *stream, float *best_ms_per_step);

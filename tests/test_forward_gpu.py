@@ -162,9 +162,11 @@ def test_autotune_picks_a_configuration_and_keeps_results(cuda_device):
         cfg = plan.tuned
         assert cfg is not None and cfg["ms_per_step"] > 0
         assert cfg["tile_rows"] in (16, 32) and cfg["graph_steps"] in (0, 16)
-        assert plan.config() == {k: cfg[k] for k in ("tile_rows", "shots_per_cta", "group_streams", "graph_steps")}
+        assert plan.config() == {k: cfg[k] for k in ("tile_rows", "shots_per_cta", "group_streams", "graph_steps",
+                                                     "stream_chunks")}
     finally:
         plan.set_graph_steps(16)
+        plan.set_streaming(False)
         plan.set_group_streams(True)
         plan.set_tiling(16, 0)
     for k in ("p", "vx", "vz"):
@@ -217,3 +219,42 @@ def test_cpu_device_is_rejected():
                                 rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"]),
                                 vp=torch.as_tensor(c["vp"]), rho=torch.as_tensor(c["rho"]),
                                 device=torch.device("cpu"))
+
+
+@pytest.mark.parametrize("shape,chunks,order", [((60, 250, 10, 70, 5), 0, 8), ((90, 121, 12, 50, 3), 1, 8),
+                                                 ((45, 250, 8, 60, 2), 2, 8), ((300, 900, 20, 40, 4), 3, 8),
+                                                 ((70, 200, 10, 60, 3), 2, 4)])
+def test_streaming_kernel_is_bit_identical(cuda_device, shape, chunks, order):
+    """The streaming forward kernel (each CTA walks a column strip of one
+    shot down a z-segment) gives the tile kernel's traces and snapshots bit
+    for bit, on ragged grids with sources and receivers on the padded border
+    and for every segment length (the energy sums, added in another order,
+    to 1e-6)."""
+    c = synthetic_case(*shape, seed=21)
+    plan = _plan_of(c, order // 2)
+    plan.set_tiling(16, 0)
+    base = run_cuda(c, cuda_device, fd_order=order, snapshot_every=16)
+    plan.set_streaming(True, chunks)
+    try:
+        assert plan.config()["stream_chunks"] > 0
+        out = run_cuda(c, cuda_device, fd_order=order, snapshot_every=16)
+    finally:
+        plan.set_streaming(False)
+    for k in ("p", "vx", "vz"):
+        np.testing.assert_array_equal(out[k], base[k])
+    np.testing.assert_array_equal(out["snapshots"], base["snapshots"])
+    for k in ("forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vz"):
+        assert orc.rel_l2(out[k], base[k]) < 1e-6
+
+
+def test_streaming_kernel_is_not_used_with_a_free_surface(cuda_device):
+    c = dict(synthetic_case(60, 250, 10, 30, 2, seed=4), free_surface=True)
+    plan = _plan_of(c, 4)
+    plan.set_streaming(True, 0)
+    try:
+        assert plan.config()["stream_chunks"] == 0          # the tile kernel runs
+        out = run_cuda(c, cuda_device, fd_order=8)
+    finally:
+        plan.set_streaming(False)
+    base = run_cuda(c, cuda_device, fd_order=8)
+    np.testing.assert_array_equal(out["p"], base["p"])

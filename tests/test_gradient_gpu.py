@@ -157,6 +157,25 @@ def test_shot_subsets_sum_to_the_full_gradient(cuda_device):
     assert float(z_l) == 0.0 and not z_g.any()
 
 
+@pytest.mark.parametrize("want_rho", [False, True])
+def test_streaming_recompute_is_bit_identical(cuda_device, want_rho):
+    """Recompute segments (and the forward) through the streaming kernel
+    write the same imaging fields, so the gradient is bit-identical."""
+    from geobrain_b200.wave import engine
+    c = load_case("small_nofs")
+    geo = engine.Geometry(c["nz"], c["nx"], c["nabc"], c["nt"], c["dt"], c["dx"], 4, False)
+    plan = engine.get_plan(geo, c["src_x"], c["src_z"], c["rcv_x"], c["rcv_z"])
+    base = cuda_grad(c, cuda_device, fd_order=8, want_rho=want_rho, checkpoint_every=17, imaging_cache=0)
+    plan.set_streaming(True, 2)
+    try:
+        got = cuda_grad(c, cuda_device, fd_order=8, want_rho=want_rho, checkpoint_every=17, imaging_cache=0)
+    finally:
+        plan.set_streaming(False)
+    np.testing.assert_array_equal(got[0], base[0])
+    if want_rho:
+        np.testing.assert_array_equal(got[1], base[1])
+
+
 def test_velocity_only_gradient_matches_full(cuda_device):
     c = load_case("small_fs")
     g1, _, _ = cuda_grad(c, cuda_device, want_rho=False)
