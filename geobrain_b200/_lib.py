@@ -39,6 +39,11 @@ class ModelDesc(ctypes.Structure):
     ]
 
 
+class Desc3(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in ("nz", "ny", "nx", "nabc", "nt", "n_shots", "n_rcv", "free_surface")] + [
+        (n, ctypes.c_float) for n in ("dt", "dx", "dy", "dz")]
+
+
 class GradStore(ctypes.Structure):
     _fields_ = [("checkpoints", ctypes.c_void_p), ("checkpoint_every", ctypes.c_int32), ("format", ctypes.c_int32),
                 ("imaging", ctypes.c_void_p), ("cached_steps", ctypes.c_int32), ("with_rho", ctypes.c_int32),
@@ -61,6 +66,8 @@ SIGNATURES = {
     "gb_plan_set_group_streams": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_plan_set_graph_steps": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_trace_misfit": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P, _P, _P]),
+    "gb3_workspace_bytes": (_SZ, [ctypes.POINTER(Desc3)]),
+    "gb3_forward": (ctypes.c_int, [ctypes.POINTER(Desc3)] + [_P] * 6 + [_P] * 4 + [_P] * 8 + [_P, _SZ, _P]),
     "gb_plan_autotune_workspace_bytes": (_SZ, [_P]),
     "gb_plan_get_config": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),

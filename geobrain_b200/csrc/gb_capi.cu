@@ -7,6 +7,7 @@
 #include "gb_batch.cuh"
 #include "gb_misfit.cuh"
 #include "gb_stream.cuh"
+#include "gb_3d.cuh"
 #include "gb_fwd.cuh"
 
 #include <cudaTypedefs.h>
@@ -904,7 +905,6 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
     GB_CUDA(cudaMemsetAsync(buf[1], 0, (size_t)S * 3 * P->plane * 4, st));
     if (want_energy) GB_CUDA(cudaMemsetAsync(energy, 0, 3 * P->plane * 4, st));
 
-    const bool fs = d.free_surface != 0;
     const StepKernel K0 = fwd_kernel_for(P, want_energy, 0);
     const StepKernel KI = fwd_kernel_for(P, want_energy, n_img == 3 ? 2 : 1);
     if (int rc = prepare_kernel(K0)) return rc;
@@ -1021,6 +1021,127 @@ int gb_trace_misfit(const float *pred, const float *obs, int32_t n_shots, int32_
     GB_CUDA(cudaGetLastError());
     trace_misfit_sum_kernel<<<1, 1024, 0, st>>>(per_trace, (long long)n_shots * n_rcv, loss);
     GB_CUDA(cudaGetLastError());
+    return GB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// 3-D acoustic forward (gb_3d.cuh)
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Layout3 {
+    size_t state, coef, src, rcv, total;
+};
+
+bool geo3_of(const gb3_model_desc *d, Geo3 *g)
+{
+    if (!d || d->nz < 1 || d->ny < 1 || d->nx < 1 || d->nabc < 0 || d->nt < 1 || d->n_shots < 1 || d->n_rcv < 0)
+        return false;
+    g->nz = d->nz; g->ny = d->ny; g->nx = d->nx; g->pml = d->nabc;
+    g->Nz = d->nz + 2 * d->nabc; g->Ny = d->ny + 2 * d->nabc; g->Nx = d->nx + 2 * d->nabc;
+    g->pitch = (g->Nx + 31) / 32 * 32;
+    g->fs = d->free_surface ? d->nabc : 1;
+    g->n_shots = d->n_shots; g->nt = d->nt; g->n_rcv = d->n_rcv;
+    g->dt = d->dt;
+    g->plane = (long long)g->Ny * g->pitch;
+    g->vol = (long long)g->Nz * g->plane;
+    return true;
+}
+
+Layout3 layout3(const Geo3 &g)
+{
+    Layout3 L{};
+    size_t o = 0;
+    L.state = o; o = align256(o + (size_t)g.n_shots * 4 * g.vol * 4);
+    L.coef = o; o = align256(o + 6 * (size_t)g.vol * 4);
+    L.src = o; o = align256(o + 3 * (size_t)g.n_shots * 4);
+    L.rcv = o; o = align256(o + 3 * (size_t)std::max(g.n_rcv, 1) * 4);
+    L.total = o;
+    return L;
+}
+
+}  // namespace
+
+size_t gb3_workspace_bytes(const gb3_model_desc *desc)
+{
+    Geo3 g;
+    if (!geo3_of(desc, &g)) return 0;
+    return layout3(g).total + 256;
+}
+
+int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t *src_y, const int64_t *src_z,
+                const int64_t *rcv_x, const int64_t *rcv_y, const int64_t *rcv_z, const float *vp, const float *rho,
+                const float *damp, const float *wavelet, float *trace_p, float *trace_vx, float *trace_vy,
+                float *trace_vz, float *energy_p, float *energy_vx, float *energy_vy, float *energy_vz,
+                void *workspace, size_t workspace_bytes, void *stream)
+{
+    g_last_error.clear();
+    Geo3 g;
+    if (!geo3_of(desc, &g)) return fail(GB_E_ARG, "invalid 3-D model description");
+    if (!vp || !rho || !damp || !wavelet || !src_x || !src_y || !src_z) return fail(GB_E_ARG, "null argument");
+    if (g.n_rcv > 0 && (!rcv_x || !rcv_y || !rcv_z)) return fail(GB_E_ARG, "null receiver positions");
+    if (!(desc->dt > 0.f) || !(desc->dz > 0.f)) return fail(GB_E_ARG, "dt and dz must be positive");
+    if (g.Nz > 65535) return fail(GB_E_ARG, "at most 65535 padded z planes");
+    // positions: unpadded indices, as the reference takes them (it adds nabc,
+    // acoustic_3d.py:398-403); sources anywhere in the padded grid, receivers
+    // where vx / vy / vz exist too (the reference indexes all four fields)
+    std::vector<int> hs(3 * g.n_shots), hr(3 * std::max(g.n_rcv, 1));
+    for (int s = 0; s < g.n_shots; ++s) {
+        const long long z = src_z[s] + g.pml, y = src_y[s] + g.pml, x = src_x[s] + g.pml;
+        if (z < 0 || z >= g.Nz || y < 0 || y >= g.Ny || x < 0 || x >= g.Nx)
+            return fail(GB_E_ARG, "source " + std::to_string(s) + " lies outside the padded grid");
+        hs[s] = (int)z; hs[g.n_shots + s] = (int)y; hs[2 * g.n_shots + s] = (int)x;
+    }
+    for (int r = 0; r < g.n_rcv; ++r) {
+        const long long z = rcv_z[r] + g.pml, y = rcv_y[r] + g.pml, x = rcv_x[r] + g.pml;
+        if (z < 0 || z > g.Nz - 2 || y < 0 || y > g.Ny - 2 || x < 0 || x > g.Nx - 2)
+            return fail(GB_E_ARG, "receiver " + std::to_string(r) + " lies outside the velocity grids");
+        hr[r] = (int)z; hr[g.n_rcv + r] = (int)y; hr[2 * g.n_rcv + r] = (int)x;
+    }
+    const Layout3 L = layout3(g);
+    char *ws = aligned_ws(workspace);
+    if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
+        return fail(GB_E_WORKSPACE, "workspace too small");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    float *state = reinterpret_cast<float *>(ws + L.state);
+    float *coef = reinterpret_cast<float *>(ws + L.coef);
+    int *d_src = reinterpret_cast<int *>(ws + L.src), *d_rcv = reinterpret_cast<int *>(ws + L.rcv);
+    GB_CUDA(cudaMemsetAsync(state, 0, (size_t)g.n_shots * 4 * g.vol * 4, st));
+    GB_CUDA(cudaMemsetAsync(coef, 0, 6 * (size_t)g.vol * 4, st));
+    GB_CUDA(cudaMemcpyAsync(d_src, hs.data(), hs.size() * 4, cudaMemcpyHostToDevice, st));
+    if (g.n_rcv) GB_CUDA(cudaMemcpyAsync(d_rcv, hr.data(), 3 * (size_t)g.n_rcv * 4, cudaMemcpyHostToDevice, st));
+    float *eout[4] = {energy_p, energy_vx, energy_vy, energy_vz};
+    const bool want_energy = energy_p && energy_vx && energy_vy && energy_vz;
+    if ((energy_p || energy_vx || energy_vy || energy_vz) && !want_energy)
+        return fail(GB_E_ARG, "give all four energy outputs or none");
+    for (int f = 0; f < 4 && want_energy; ++f)
+        GB_CUDA(cudaMemsetAsync(eout[f], 0, (size_t)g.nz * g.ny * g.nx * 4, st));
+
+    Args3 A{};
+    A.g = g;
+    A.state = state;
+    A.a1 = coef; A.k1 = coef + g.vol; A.a2 = coef + 2 * g.vol;
+    A.k2 = coef + 3 * g.vol; A.k3 = coef + 4 * g.vol; A.k4 = coef + 5 * g.vol;
+    A.src = d_src;
+    A.wavelet = wavelet;
+    for (int f = 0; f < 4; ++f) A.energy[f] = want_energy ? eout[f] : nullptr;
+    coef3_kernel<<<4 * 148, 256, 0, st>>>(g, vp, rho, damp, desc->dz, coef, coef + g.vol, coef + 2 * g.vol,
+                                          coef + 3 * g.vol, coef + 4 * g.vol, coef + 5 * g.vol);
+    GB_CUDA(cudaGetLastError());
+    const dim3 block(32, 4), grid((g.Nx + 127) / 128, (g.Ny + 3) / 4, g.Nz);
+    const bool fs = desc->free_surface != 0;
+    const bool want_tr = g.n_rcv > 0 && (trace_p || trace_vx || trace_vy || trace_vz);
+    for (int it = 0; it < g.nt; ++it) {
+        A.it = it;
+        p3_kernel<<<grid, block, 0, st>>>(A);
+        if (fs) mirror3_kernel<<<148, 256, 0, st>>>(g, state, 0, 2, -1.f);
+        v3_kernel<<<grid, block, 0, st>>>(A);
+        if (fs) mirror3_kernel<<<148, 256, 0, st>>>(g, state, 3, 1, 1.f);
+        if (want_tr)
+            rec3_kernel<<<(g.n_shots * g.n_rcv + 255) / 256, 256, 0, st>>>(g, state, d_rcv, trace_p, trace_vx,
+                                                                          trace_vy, trace_vz, it, nullptr);
+        GB_CUDA(cudaGetLastError());
+    }
     return GB_OK;
 }
 

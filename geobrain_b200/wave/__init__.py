@@ -19,9 +19,10 @@ kernels.pad_model; the compute runs in hand-written sm_100a CUDA kernels.
 from . import kernel as kernels
 from . import misfit, sharding
 from .batched import AcousticBatch, acoustic_forward_batched
-from .boundary import bc_pml, create_boundary
+from .boundary import bc_pml, bc_pml_3d, create_boundary
 from .config import BoundaryConfig, GridConfig, SolverConfig, TimeConfig, WaveletConfig
 from .kernel import acoustic_forward_kernel, pad_model
+from .kernel3d import acoustic_forward_kernel_3d, pad_model_3d
 from .model import UNITS, AbstractModel, AcousticModel, numpy2tensor
 from .propagator import AbstractPropagator, AcousticPropagator
 from .result import WaveResult
@@ -35,4 +36,5 @@ __all__ = [
     "bc_pml", "create_boundary", "Source", "Receiver", "Survey", "AcousticPropagator",
     "numpy2tensor", "kernels", "acoustic_forward_kernel", "pad_model",
     "AcousticBatch", "acoustic_forward_batched", "sharding", "misfit",
+    "acoustic_forward_kernel_3d", "pad_model_3d", "bc_pml_3d",
 ]

@@ -47,12 +47,46 @@ def bc_pml(nx: int, nz: int, dx: float, dz: float, pml: int, vmax: float, free_s
     return out
 
 
+def bc_pml_3d(nx: int, ny: int, nz: int, dx: float, dy: float, dz: float, pml: int, vmax: float,
+              free_surface: bool = True) -> np.ndarray:
+    """3-D quadratic damping (geobrain/physics/wave/boundary/pml.py:101-196):
+    the 1-D profile kappa (i dx / a)^2, kappa = -3 vmax ln(1e-6) / (2 a),
+    a = (pml - 1) dx, laid on all six faces (the top one only without a free
+    surface), the maximum where faces meet.  With a free surface the grid has
+    only the bottom PML in z, as in the reference."""
+    nxp, nyp = nx + 2 * pml, ny + 2 * pml
+    nzp = nz + pml if free_surface else nz + 2 * pml
+    a = (pml - 1) * dx
+    kappa = -3.0 * vmax * np.log(1e-6) / (2.0 * a)
+    prof = np.array([kappa * (i * dx / a) * (i * dx / a) for i in range(pml)], dtype=np.float64)
+
+    def dist(n, lo):
+        d = np.full(n, -1, dtype=np.int64)
+        if lo:
+            d[:pml] = np.arange(pml - 1, -1, -1)
+        d[n - pml:] = np.arange(pml)
+        return d
+    dz_, dy_, dx_ = dist(nzp, not free_surface), dist(nyp, True), dist(nxp, True)
+    out = np.zeros((nzp, nyp, nxp), dtype=np.float64)
+    for d, shape in ((dx_, (1, 1, nxp)), (dy_, (1, nyp, 1)), (dz_, (nzp, 1, 1))):
+        vals = np.where(d >= 0, prof[np.maximum(d, 0)], 0.0).reshape(shape)
+        out = np.maximum(out, vals)
+    return out
+
+
 def create_boundary(bc_type: str, nx: int, nz: int, dx: float, dz: float, n_layers: int, vmax: float = None,
                     alpha: float = 0.0053, free_surface: bool = False, ny: int = None, dy: float = None):
     """Factory with the signature of geobrain/physics/wave/boundary/__init__.py:23-116."""
     bc_type = bc_type.lower()
     if ny is not None:
-        raise NotImplementedError("3-D boundaries are outside the 2-D acoustic path")
+        if bc_type != "pml":
+            raise NotImplementedError(f"3-D boundary type '{bc_type}' is not yet supported. "
+                                      f"Only 'pml' is available for 3-D.")
+        if vmax is None:
+            raise ValueError("vmax is required for PML boundary")
+        if dy is None:
+            raise ValueError("dy is required for 3-D PML boundary")
+        return bc_pml_3d(nx, ny, nz, dx, dy, dz, n_layers, vmax, free_surface)
     if bc_type == "pml":
         if vmax is None:
             raise ValueError("vmax is required for PML boundary")

@@ -112,3 +112,7 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
     p, vx, vz, en, snaps = engine.run_forward(plan, vp_t, rho_t, damp_t, w, want_energy=want_energy,
                                               snapshot_every=int(snapshot_every))
     return engine.pack_output(plan, p, vx, vz, en, snaps)
+
+
+# the 3-D kernel lives beside it, under the reference's kernels namespace
+from .kernel3d import acoustic_forward_kernel_3d, pad_model_3d  # noqa: E402,F401

@@ -18,6 +18,7 @@ import torch
 
 from .boundary import create_boundary
 from .kernel import acoustic_forward_kernel
+from .kernel3d import acoustic_forward_kernel_3d
 from .model import AbstractModel, AcousticModel, numpy2tensor
 from .result import WaveResult
 from .survey import Survey
@@ -53,8 +54,8 @@ class AcousticPropagator(AbstractPropagator):
             raise TypeError(f"Expected AcousticModel, got {type(model).__name__}")
         if not isinstance(survey, Survey):
             raise TypeError(f"Expected Survey, got {type(survey).__name__}")
-        if model.ndim != 2:
-            raise NotImplementedError("geobrain_b200 implements the 2-D acoustic propagator")
+        if model.ndim == 3 and fd_order != 4:
+            raise ValueError("the 3-D acoustic kernel is 4th order")
         self.survey = survey
         self.nt, self.dt, self.f0 = survey.nt, survey.dt, survey.f0
         self.fd_order = fd_order
@@ -64,20 +65,26 @@ class AcousticPropagator(AbstractPropagator):
         src = self.source.get_loc()
         self.src_n = self.source.num
         self.wavelet = numpy2tensor(self.source.get_wavelet(), dtype).to(device)
+        # locations are (x, z) in 2-D and (x, y, z) in 3-D (acoustic.py:90-116)
         self.src_x = numpy2tensor(src[:, 0], torch.long).to(device)
-        self.src_z = numpy2tensor(src[:, 1], torch.long).to(device)
+        self.src_z = numpy2tensor(src[:, -1], torch.long).to(device)
+        if model.ndim == 3:
+            self.src_y = numpy2tensor(src[:, 1], torch.long).to(device)
         self.receiver = survey.receiver
         rcv = self.receiver.get_loc()
         self.rcv_n = self.receiver.num
         self.rcv_x = numpy2tensor(rcv[:, 0], torch.long).to(device)
-        self.rcv_z = numpy2tensor(rcv[:, 1], torch.long).to(device)
+        self.rcv_z = numpy2tensor(rcv[:, -1], torch.long).to(device)
+        if model.ndim == 3:
+            self.rcv_y = numpy2tensor(rcv[:, 1], torch.long).to(device)
         self.receiver_masks = survey.receiver_masks
 
     def _init_boundary(self, vmax: Optional[float] = None) -> None:
         if vmax is None:
             vmax = float(self.model.vp.detach().cpu().max())
+        extra = dict(ny=self.ny, dy=self.dy) if self.model.ndim == 3 else {}
         damp = create_boundary(self.abc_type, nx=self.nx, nz=self.nz, dx=self.dx, dz=self.dz, n_layers=self.nabc,
-                               vmax=vmax, alpha=self.model.abc_alpha, free_surface=False)
+                               vmax=vmax, alpha=self.model.abc_alpha, free_surface=False, **extra)
         self.damp = numpy2tensor(damp, self.dtype).to(self.device)
 
     def forward(self, model: Optional[AcousticModel] = None, shot_index: Optional[int] = None,
@@ -93,6 +100,15 @@ class AcousticPropagator(AbstractPropagator):
             src_x, src_z, src_n, wavelet = self.src_x[sl], self.src_z[sl], 1, self.wavelet[sl]
         else:
             src_x, src_z, src_n, wavelet = self.src_x, self.src_z, self.src_n, self.wavelet
+        if self.model.ndim == 3:
+            src_y = self.src_y[sl] if shot_index is not None else self.src_y
+            result = acoustic_forward_kernel_3d(
+                nx=self.nx, ny=self.ny, nz=self.nz, dx=self.dx, dy=self.dy, dz=self.dz, nt=self.nt, dt=self.dt,
+                nabc=self.nabc, free_surface=self.free_surface, src_x=src_x, src_y=src_y, src_z=src_z,
+                src_n=src_n, src_v=wavelet, rcv_x=self.rcv_x, rcv_y=self.rcv_y, rcv_z=self.rcv_z,
+                rcv_n=self.rcv_n, damp=self.damp, vp=model.vp, rho=model.rho,
+                checkpoint_segments=checkpoint_segments, device=torch.device(self.device), dtype=self.dtype)
+            return WaveResult.from_dict(result)
         result = acoustic_forward_kernel(
             nx=self.nx, nz=self.nz, dx=self.dx, dz=self.dz, nt=self.nt, dt=self.dt, nabc=self.nabc,
             free_surface=self.free_surface, src_x=src_x, src_z=src_z, src_n=src_n, src_v=wavelet,

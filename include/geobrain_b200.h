@@ -290,6 +290,33 @@ int gb_forward_static_scratch(gb_plan *plan, const float *vp, const float *rho, 
                               float *energy_p, float *energy_vx, float *energy_vz,
                               int32_t snapshot_every, float *snapshots, void *stream);
 
+/* ---------------------------------------------------------------------
+ * 3-D acoustic forward modelling (4th order), a drop-in for
+ * acoustic_forward_kernel_3d (geobrain/physics/wave/kernels/acoustic_3d.py
+ * :303-476): padding, coefficients and every time step on the device.
+ * -------------------------------------------------------------------- */
+typedef struct gb3_model_desc {
+    int32_t nz, ny, nx, nabc, nt;
+    int32_t n_shots, n_rcv, free_surface;
+    float dt, dx, dy, dz;      /* the reference scales every derivative by 1/dz */
+} gb3_model_desc;
+
+size_t gb3_workspace_bytes(const gb3_model_desc *desc);
+
+/* vp, rho: (nz, ny, nx); damp: (nz+2nabc, ny+2nabc, nx+2nabc); wavelet:
+ * (n_shots, nt); positions: host int64 arrays of unpadded indices.  A source
+ * may sit anywhere in the padded grid; a receiver must lie where vx, vy and
+ * vz exist (padded index <= N-2 on each axis), since all four fields are
+ * recorded.  Traces: (n_shots, nt, n_rcv), any may be NULL.  Energies:
+ * (nz, ny, nx), all four or none (overwritten).  Device pointers;
+ * asynchronous on `stream`. */
+int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t *src_y, const int64_t *src_z,
+                const int64_t *rcv_x, const int64_t *rcv_y, const int64_t *rcv_z,
+                const float *vp, const float *rho, const float *damp, const float *wavelet,
+                float *trace_p, float *trace_vx, float *trace_vy, float *trace_vz,
+                float *energy_p, float *energy_vx, float *energy_vy, float *energy_vz,
+                void *workspace, size_t workspace_bytes, void *stream);
+
 /* Message of the last failure on this thread ("" if none). */
 const char *gb_last_error(void);
 

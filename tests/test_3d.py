@@ -1,0 +1,144 @@
+"""3-D acoustic path (geobrain/physics/wave/kernels/acoustic_3d.py): the
+NumPy oracle against the reference's own outputs (golden fixtures from
+tests/golden/make_golden_3d.py), then the CUDA kernel through the C ABI
+against the fixtures and the oracle.  Tolerance: 1e-5 relative L2 in fp32."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import acoustic3d as o3
+from oracle import oracle as orc
+
+CASES = ["small_3d_nofs", "small_3d_fs"]
+KEYS = ("p", "vx", "vy", "vz", "forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vy",
+        "forward_wavefield_vz")
+
+
+def load3(name):
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    with np.load(os.path.join(here, "golden", f"{name}.npz")) as z:
+        c = {k: z[k] for k in z.files}
+    for k in ("nz", "ny", "nx", "nabc", "nt"):
+        c[k] = int(c[k])
+    c["dx"], c["dt"], c["free_surface"] = float(c["dx"]), float(c["dt"]), bool(c["free_surface"])
+    return c
+
+
+def kw3(c):
+    return dict(nz=c["nz"], ny=c["ny"], nx=c["nx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+                free_surface=c["free_surface"], src_x=c["src_x"], src_y=c["src_y"], src_z=c["src_z"],
+                src_v=c["src_v"], rcv_x=c["rcv_x"], rcv_y=c["rcv_y"], rcv_z=c["rcv_z"], damp=c["damp"], vp=c["vp"],
+                rho=c["rho"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matches_reference_golden(name):
+    c = load3(name)
+    r64 = o3.forward(**kw3(c), dtype=np.float64)
+    r32 = o3.forward(**kw3(c), dtype=np.float32)
+    for k in KEYS:
+        assert orc.rel_l2(r64[k], c[f"ref64_{k}"]) < 1e-12, k
+        assert orc.rel_l2(r32[k], c[f"ref32_{k}"]) < 1e-6, k
+
+
+def test_bc_pml_3d_matches_golden_damping():
+    from geobrain_b200.wave import bc_pml_3d, create_boundary
+    c = load3("small_3d_nofs")
+    d = create_boundary("pml", nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], n_layers=c["nabc"],
+                        vmax=float(c["vp"].max()), free_surface=False, ny=c["ny"], dy=c["dx"])
+    np.testing.assert_array_equal(d.astype(np.float32), c["damp"])
+    assert bc_pml_3d(16, 14, 12, 10.0, 10.0, 10.0, 6, 3000.0, free_surface=True).shape == (18, 26, 28)
+
+
+def test_pad_model_3d_replicates_edges():
+    from geobrain_b200.wave import pad_model_3d
+    v = torch.arange(2 * 3 * 4, dtype=torch.float32).reshape(2, 3, 4)
+    np.testing.assert_array_equal(pad_model_3d(v, 2, 2, 3, 4).numpy(), np.pad(v.numpy(), 2, mode="edge"))
+
+
+def run3(c, device, **kw):
+    from geobrain_b200.wave import acoustic_forward_kernel_3d
+    out = acoustic_forward_kernel_3d(
+        nx=c["nx"], ny=c["ny"], nz=c["nz"], dx=c["dx"], dy=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"],
+        nabc=c["nabc"], free_surface=c["free_surface"], src_x=torch.as_tensor(c["src_x"]),
+        src_y=torch.as_tensor(c["src_y"]), src_z=torch.as_tensor(c["src_z"]), src_n=len(c["src_x"]),
+        src_v=torch.as_tensor(c["src_v"], device=device), rcv_x=torch.as_tensor(c["rcv_x"]),
+        rcv_y=torch.as_tensor(c["rcv_y"]), rcv_z=torch.as_tensor(c["rcv_z"]), rcv_n=len(c["rcv_x"]),
+        damp=torch.as_tensor(c["damp"], device=device), vp=torch.as_tensor(c["vp"], device=device),
+        rho=torch.as_tensor(c["rho"], device=device), device=device, **kw)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_cuda_3d_matches_reference(cuda_device, name):
+    c = load3(name)
+    out = run3(c, cuda_device)
+    for k in KEYS:
+        assert orc.rel_l2(out[k], c[f"ref32_{k}"]) < 1e-5, (k, orc.rel_l2(out[k], c[f"ref32_{k}"]))
+        assert orc.rel_l2(out[k], c[f"ref64_{k}"]) < 1e-5, k
+
+
+@pytest.mark.gpu
+def test_cuda_3d_larger_grid_against_oracle(cuda_device):
+    """A ragged grid (sizes no multiple of the 128-column blocks) with more
+    shots, a source in the padded border and receivers on the last valid
+    planes, against the float64 oracle."""
+    rng = np.random.default_rng(7)
+    nz, ny, nx, nabc, nt = 23, 19, 61, 7, 60
+    vp = (2000 + 800 * rng.random((nz, ny, nx))).astype(np.float32)
+    rho = (1900 + 300 * rng.random((nz, ny, nx))).astype(np.float32)
+    from geobrain_b200.wave import bc_pml_3d, RickerWavelet
+    damp = bc_pml_3d(nx, ny, nz, 10.0, 10.0, 10.0, nabc, float(vp.max()), free_surface=False).astype(np.float32)
+    w, _ = RickerWavelet()(f0=20.0, dt=1e-3)
+    w = np.pad(w.numpy(), (0, nt))[:nt].astype(np.float32)
+    c = dict(nz=nz, ny=ny, nx=nx, nabc=nabc, nt=nt, dx=10.0, dt=1e-3, free_surface=False, vp=vp, rho=rho,
+             damp=damp, src_x=np.array([3, 30, -nabc, 50]), src_y=np.array([2, 9, -nabc, 17]),
+             src_z=np.array([1, 11, -nabc, 20]), src_v=np.tile(w, (4, 1)),
+             rcv_x=np.array([0, 10, 40, nx + nabc - 2, -nabc]), rcv_y=np.array([1, 5, 18, ny + nabc - 2, -nabc]),
+             rcv_z=np.array([0, 3, 22, nz + nabc - 2, -nabc]))
+    out = run3(c, cuda_device)
+    ref = o3.forward(**kw3(c), dtype=np.float64)
+    for k in KEYS:
+        assert orc.rel_l2(out[k], ref[k]) < 1e-5, k
+
+
+@pytest.mark.gpu
+def test_cuda_3d_rejects_what_the_reference_cannot_index(cuda_device):
+    c = load3("small_3d_nofs")
+    bad = dict(c, rcv_x=np.array([c["nx"] + c["nabc"] - 1]), rcv_y=np.array([0]), rcv_z=np.array([0]))
+    with pytest.raises(ValueError):
+        run3(bad, cuda_device)
+    with pytest.raises(NotImplementedError):
+        from geobrain_b200.wave import acoustic_forward_kernel_3d
+        acoustic_forward_kernel_3d(
+            nx=c["nx"], ny=c["ny"], nz=c["nz"], dx=10, dy=10, dz=10, nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+            free_surface=False, src_x=c["src_x"], src_y=c["src_y"], src_z=c["src_z"], src_n=2,
+            src_v=torch.as_tensor(c["src_v"], device=cuda_device), rcv_x=c["rcv_x"], rcv_y=c["rcv_y"],
+            rcv_z=c["rcv_z"], rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=cuda_device),
+            vp=torch.tensor(c["vp"], device=cuda_device, requires_grad=True),
+            rho=torch.as_tensor(c["rho"], device=cuda_device), device=cuda_device)
+
+
+@pytest.mark.gpu
+def test_propagator_runs_3d_models(cuda_device):
+    """AcousticPropagator on a 3-D AcousticModel and Survey dispatches to the
+    3-D kernel (propagators/acoustic.py:220-247), with the survey's (x, y, z)
+    locations."""
+    from geobrain_b200.wave import (AcousticModel, AcousticPropagator, BoundaryConfig, GridConfig, Receiver,
+                                    Source, Survey)
+    c = load3("small_3d_nofs")
+    grid = GridConfig(nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], ny=c["ny"], dy=c["dx"])
+    model = AcousticModel(grid, BoundaryConfig(n_layers=c["nabc"]), vp=c["vp"], rho=c["rho"], auto_update_rho=False,
+                          device=str(cuda_device))
+    src = Source(nt=c["nt"], dt=c["dt"], f0=25.0)
+    src.add_sources(x=c["src_x"], z=c["src_z"], y=c["src_y"], wavelet=c["src_v"][0])
+    rcv = Receiver(nt=c["nt"], dt=c["dt"])
+    rcv.add_receivers(x=c["rcv_x"], z=c["rcv_z"], y=c["rcv_y"], rcv_type="pr")
+    prop = AcousticPropagator(model, Survey(src, rcv), device=str(cuda_device))
+    res = prop.forward()
+    assert res.vy is not None
+    for k in ("p", "vx", "vy", "vz"):
+        assert orc.rel_l2(getattr(res, k).cpu().numpy(), c[f"ref32_{k}"]) < 1e-5, k
