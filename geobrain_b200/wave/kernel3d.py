@@ -6,12 +6,15 @@ arguments (positions are unpadded grid indices; damp is the padded 3-D
 array) and returns the same dict: traces p / vx / vy / vz (src_n, nt, rcv_n)
 and energy maps forward_wavefield_{p,vx,vy,vz} (nz, ny, nx).  The CUDA
 library (gb3_forward) computes them.  As in the reference, every derivative
-is scaled by 1/dz.  The path is forward-only: a vp or rho that requires grad
-raises.
+is scaled by 1/dz.  When vp or rho requires grad, the traces are
+differentiable: the forward keeps checkpoints and the backward runs the
+hand-written adjoint (gb3_backward) in place of autograd through the
+reference's time loop.
 """
 from __future__ import annotations
 
 import ctypes
+import math
 
 import torch
 from torch import Tensor
@@ -31,6 +34,75 @@ def pad_model_3d(v: Tensor, pml: int, nz: int, ny: int, nx: int, device: torch.d
     return v[iz][:, iy][:, :, ix].to(device)
 
 
+class _Run3:
+    """Validated inputs of one 3-D call, bound to the C ABI."""
+
+    def __init__(self, desc, pos, rpos, damp, w, device):
+        self.desc, self.pos, self.rpos, self.damp, self.w, self.device = desc, pos, rpos, damp, w, device
+        self.L = _lib.load()
+
+    def check(self, rc):
+        if rc == _lib.GB_E_ARG:
+            raise ValueError(self.L.gb_last_error().decode())
+        _lib.check(rc)
+
+    def forward(self, vp, rho, ckpt=None, K=0):
+        d, dev = self.desc, self.device
+        ws = engine.workspace(int(self.L.gb3_workspace_bytes(ctypes.byref(d))), dev)
+        f32 = dict(device=dev, dtype=torch.float32)
+        tr = [torch.empty((d.n_shots, d.nt, d.n_rcv), **f32) for _ in range(4)]
+        en = [torch.empty((d.nz, d.ny, d.nx), **f32) for _ in range(4)]
+        with torch.cuda.device(dev):
+            rc = self.L.gb3_forward(ctypes.byref(d), *[p.ctypes.data for p in self.pos],
+                                    *[p.ctypes.data for p in self.rpos], vp.data_ptr(), rho.data_ptr(),
+                                    self.damp.data_ptr(), self.w.data_ptr(), *[t.data_ptr() for t in tr],
+                                    *[e.data_ptr() for e in en], _lib.ptr(ckpt), int(K), ws.data_ptr(), ws.numel(),
+                                    engine.stream_handle(dev))
+        self.check(rc)
+        return tr, en
+
+    def backward(self, vp, rho, res, ckpt, K, want_rho):
+        d, dev = self.desc, self.device
+        ws = engine.workspace(int(self.L.gb3_backward_workspace_bytes(ctypes.byref(d), int(K), int(want_rho))), dev)
+        gvp = torch.empty((d.nz, d.ny, d.nx), device=dev, dtype=torch.float32)
+        grho = torch.empty_like(gvp) if want_rho else None
+        with torch.cuda.device(dev):
+            rc = self.L.gb3_backward(ctypes.byref(d), *[p.ctypes.data for p in self.pos],
+                                     *[p.ctypes.data for p in self.rpos], vp.data_ptr(), rho.data_ptr(),
+                                     self.damp.data_ptr(), self.w.data_ptr(), *[_lib.ptr(r) for r in res],
+                                     ckpt.data_ptr(), int(K), gvp.data_ptr(), _lib.ptr(grho), ws.data_ptr(),
+                                     ws.numel(), engine.stream_handle(dev))
+        self.check(rc)
+        return gvp, grho
+
+
+class _Function3D(torch.autograd.Function):
+    """3-D traces as a differentiable function of (vp, rho): checkpoints every
+    K steps in the forward, the hand-written adjoint in the backward
+    (replaces autograd through acoustic_3d.py:446-460)."""
+
+    @staticmethod
+    def forward(ctx, vp, rho, run, K):
+        vp32 = vp.detach().to(torch.float32).contiguous()
+        rho32 = rho.detach().to(torch.float32).contiguous()
+        ckpt = torch.empty(int(run.L.gb3_checkpoint_bytes(ctypes.byref(run.desc), int(K))) // 4,
+                           device=run.device, dtype=torch.float32)
+        tr, en = run.forward(vp32, rho32, ckpt, K)
+        ctx.run, ctx.K, ctx.ckpt = run, K, ckpt
+        ctx.save_for_backward(vp32, rho32)
+        ctx.mark_non_differentiable(*en)
+        return (*tr, *en)
+
+    @staticmethod
+    def backward(ctx, gp, gvx, gvy, gvz, *unused):
+        vp32, rho32 = ctx.saved_tensors
+        need_vp, need_rho = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        res = [None if t is None else t.to(torch.float32).contiguous() for t in (gp, gvx, gvy, gvz)]
+        gvp, grho = ctx.run.backward(vp32, rho32, res, ctx.ckpt, ctx.K, need_rho)
+        ctx.ckpt = None
+        return (gvp if need_vp else None), (grho if need_rho else None), None, None
+
+
 def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, dz: float, nt: int, dt: float,
                                nabc: int, free_surface: bool, src_x: Tensor, src_y: Tensor, src_z: Tensor,
                                src_n: int, src_v: Tensor, rcv_x: Tensor, rcv_y: Tensor, rcv_z: Tensor, rcv_n: int,
@@ -43,8 +115,6 @@ def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, 
         raise TypeError(f"geobrain_b200 computes in float32 (dtype={dtype})")
     if checkpoint_segments < 1:
         raise ValueError(f"checkpoint_segments must be >= 1, got {checkpoint_segments}")
-    if torch.is_grad_enabled() and (getattr(vp, "requires_grad", False) or getattr(rho, "requires_grad", False)):
-        raise NotImplementedError("the 3-D path of geobrain_b200 is forward-only (no gradient)")
     nx, ny, nz, nt, nabc, src_n, rcv_n = (int(v) for v in (nx, ny, nz, nt, nabc, src_n, rcv_n))
     pos = [engine._i64(a) for a in (src_x, src_y, src_z)]
     rpos = [engine._i64(a) for a in (rcv_x, rcv_y, rcv_z)]
@@ -62,26 +132,29 @@ def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, 
     damp_t = _as_f32(damp, device, "damp")
     if tuple(damp_t.shape) != shape:
         raise ValueError(f"damp must have shape {shape}, got {tuple(damp_t.shape)}")
-    vp_t = _as_f32(vp.detach() if torch.is_tensor(vp) else vp, device, "vp")
-    rho_t = _as_f32(rho.detach() if torch.is_tensor(rho) else rho, device, "rho")
-    for name, t in (("vp", vp_t), ("rho", rho_t)):
+    for name, t in (("vp", vp), ("rho", rho)):
         if tuple(t.shape) != (nz, ny, nx):
             raise ValueError(f"{name} must have shape {(nz, ny, nx)}, got {tuple(t.shape)}")
     desc = _lib.Desc3(nz, ny, nx, nabc, nt, src_n, rcv_n, int(bool(free_surface)), float(dt), float(dx), float(dy),
                       float(dz))
-    L = _lib.load()
-    ws = engine.workspace(int(L.gb3_workspace_bytes(ctypes.byref(desc))), device)
-    f32 = dict(device=device, dtype=torch.float32)
-    tr = [torch.empty((src_n, nt, rcv_n), **f32) for _ in range(4)]
-    en = [torch.empty((nz, ny, nx), **f32) for _ in range(4)]
-    with torch.cuda.device(device):
-        rc = L.gb3_forward(ctypes.byref(desc), *[p.ctypes.data for p in pos], *[p.ctypes.data for p in rpos],
-                           vp_t.data_ptr(), rho_t.data_ptr(), damp_t.data_ptr(), w.data_ptr(),
-                           *[t.data_ptr() for t in tr], *[e.data_ptr() for e in en], ws.data_ptr(), ws.numel(),
-                           engine.stream_handle(device))
-    if rc == _lib.GB_E_ARG:
-        raise ValueError(L.gb_last_error().decode())
-    _lib.check(rc)
+    run = _Run3(desc, pos, rpos, damp_t, w, device)
+    needs_grad = torch.is_grad_enabled() and (getattr(vp, "requires_grad", False) or
+                                              getattr(rho, "requires_grad", False))
+    if needs_grad:
+        vp_g = vp if torch.is_tensor(vp) else torch.as_tensor(vp)
+        rho_g = rho if torch.is_tensor(rho) else torch.as_tensor(rho)
+        for name, t in (("vp", vp_g), ("rho", rho_g)):
+            if t.device != device:
+                raise ValueError(f"{name} is on {t.device}, expected {device}")
+        # segments of about sqrt(nt) steps, and never fewer than the caller's checkpoint_segments
+        n_seg = max(int(checkpoint_segments), int(math.ceil(math.sqrt(nt))))
+        K = max(1, -(-nt // n_seg))
+        outs = _Function3D.apply(vp_g, rho_g, run, K)
+        tr, en = list(outs[:4]), list(outs[4:])
+    else:
+        vp_t = _as_f32(vp.detach() if torch.is_tensor(vp) else vp, device, "vp")
+        rho_t = _as_f32(rho.detach() if torch.is_tensor(rho) else rho, device, "rho")
+        tr, en = run.forward(vp_t, rho_t)
     keys = ("p", "vx", "vy", "vz")
     out = {k: t for k, t in zip(keys, tr)}
     out.update({f"forward_wavefield_{k}": e for k, e in zip(keys, en)})

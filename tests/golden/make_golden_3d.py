@@ -10,7 +10,9 @@ builds it (propagators/acoustic.py:119-148, boundary/pml.py:101-196), and the
 traces (p, vx, vy, vz) and energy maps of
 geobrain/physics/wave/kernels/acoustic_3d.py:303-476 in float32 and in
 float64 (torch.set_default_dtype(float64) + dtype=float64, because
-pad_model_3d allocates with the default dtype).
+pad_model_3d allocates with the default dtype), and the float64 autograd
+gradients dL/dvp, dL/drho (checkpoint_segments=3) of a loss linear in all
+four traces, L = sum_k <lin_k, trace_k>.
 """
 from __future__ import annotations
 
@@ -62,6 +64,24 @@ def main(ref_root: str) -> None:
             torch.set_default_dtype(torch.float32)
             for k, v in res.items():
                 out[f"{tag}_{k}"] = v.numpy()
+        rng_l = np.random.default_rng(seed + 100)
+        lin = {k: rng_l.standard_normal((2, nt, rcv_x.size)) for k in ("p", "vx", "vy", "vz")}
+        torch.set_default_dtype(torch.float64)
+        vp_t = torch.tensor(vp, dtype=torch.float64, requires_grad=True)
+        rho_t = torch.tensor(rho, dtype=torch.float64, requires_grad=True)
+        res = acoustic_forward_kernel_3d(
+            nx=nx, ny=ny, nz=nz, dx=dx, dy=dx, dz=dx, nt=nt, dt=dt, nabc=nabc, free_surface=fs,
+            src_x=torch.tensor(src_x), src_y=torch.tensor(src_y), src_z=torch.tensor(src_z), src_n=2,
+            src_v=torch.tensor(src_v, dtype=torch.float64), rcv_x=torch.tensor(rcv_x), rcv_y=torch.tensor(rcv_y),
+            rcv_z=torch.tensor(rcv_z), rcv_n=rcv_x.size, damp=torch.tensor(damp, dtype=torch.float64), vp=vp_t,
+            rho=rho_t, checkpoint_segments=3, dtype=torch.float64)
+        loss = sum((torch.tensor(lin[k]) * res[k]).sum() for k in lin)
+        loss.backward()
+        torch.set_default_dtype(torch.float32)
+        out["ref64_grad_vp"] = vp_t.grad.numpy()
+        out["ref64_grad_rho"] = rho_t.grad.numpy()
+        for k, v in lin.items():
+            out[f"lin_{k}"] = v
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print(name, {k: v.shape for k, v in out.items() if hasattr(v, "shape") and k.startswith("ref32")})
 
