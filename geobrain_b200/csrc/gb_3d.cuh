@@ -338,6 +338,14 @@ __device__ __forceinline__ float at3(const Geo3 &g, const float *F, int z, int y
     return F[(long long)z * g.plane + (long long)y * g.pitch + x];
 }
 
+// float4 of field F at (z, y, x4), 0 outside the grid rows / planes; x4 is a
+// multiple of 4 and x4 - 4 >= 0 is checked by the caller's guard
+__device__ __forceinline__ float4 row4(const Geo3 &g, const float *F, int z, int y, int x4)
+{
+    if (z < 0 || z >= g.Nz || y < 0 || y >= g.Ny || x4 < 0 || x4 >= g.pitch) return make_float4(0.f, 0.f, 0.f, 0.f);
+    return *reinterpret_cast<const float4 *>(F + (long long)z * g.plane + (long long)y * g.pitch + x4);
+}
+
 __global__ void __launch_bounds__(128) adj_v3_kernel(const AdjArgs3 A)
 {
     const Geo3 &g = A.g;
@@ -346,47 +354,76 @@ __global__ void __launch_bounds__(128) adj_v3_kernel(const AdjArgs3 A)
     const int z = blockIdx.z;
     if (x0 >= g.Nx || y >= g.Ny) return;
     const long long o = (long long)z * g.plane + (long long)y * g.pitch + x0;
+    // a2 times the mask of each velocity component at the neighbours the
+    // transposed gradient reads: x-1 .. x+1 (vx), rows y-2 .. y+1 (vy),
+    // planes z-2 .. z+1 (vz); the same for every shot
+    float mx[12], my[4][4], mz[4][4];
+    {
+        const float4 l = row4(g, A.a2, z, y, x0 - 4), c = row4(g, A.a2, z, y, x0), r = row4(g, A.a2, z, y, x0 + 4);
+        const float v[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 12; ++i) mx[i] = in_vx(g, z, y, x0 - 4 + i) ? v[i] : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 ay = row4(g, A.a2, z, y + k - 2, x0), az = row4(g, A.a2, z + k - 2, y, x0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            my[k][q] = in_vy(g, z, y + k - 2, x0 + q) ? f4(ay, q) : 0.f;
+            mz[k][q] = in_vz(g, z + k - 2, y, x0 + q) ? f4(az, q) : 0.f;
+        }
+    }
+    const float4 k2 = row4(g, A.k2, z, y, x0), k3 = row4(g, A.k3, z, y, x0), k4 = row4(g, A.k4, z, y, x0);
     float g2[4] = {0.f, 0.f, 0.f, 0.f};
     for (int s = 0; s < g.n_shots; ++s) {
         const float *L = A.lam_in + (long long)s * 4 * g.vol;
         float *O = A.lam_out + (long long)s * 4 * g.vol;
+        const float *LX = L + g.vol, *LY = L + 2 * g.vol, *LZ = L + 3 * g.vol;
+        const float4 xl = row4(g, LX, z, y, x0 - 4), xc = row4(g, LX, z, y, x0), xr = row4(g, LX, z, y, x0 + 4);
+        const float lxs[12] = {xl.x, xl.y, xl.z, xl.w, xc.x, xc.y, xc.z, xc.w, xr.x, xr.y, xr.z, xr.w};
+        float4 ly[4], lz[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            ly[k] = row4(g, LY, z, y + k - 2, x0);
+            lz[k] = row4(g, LZ, z + k - 2, y, x0);
+        }
+        const float4 lp = *reinterpret_cast<const float4 *>(L + o);
+        float4 jx = make_float4(0.f, 0.f, 0.f, 0.f), jy = jx, jz = jx;
+        if (A.G2) {
+            const long long jo = (long long)s * g.vol + o, js = (long long)g.n_shots * g.vol;
+            jx = *reinterpret_cast<const float4 *>(A.img_j + jo);
+            jy = *reinterpret_cast<const float4 *>(A.img_j + js + jo);
+            jz = *reinterpret_cast<const float4 *>(A.img_j + 2 * js + jo);
+        }
+        float op[4], ox[4], oy[4], oz[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
+            // w = a2 lam on the component's mask; lp' = lp - sum_c G_c^T w
+            const float wx_m1 = mx[q + 3] * lxs[q + 3], wx_0 = mx[q + 4] * lxs[q + 4];
+            const float wx_m2 = mx[q + 2] * lxs[q + 2], wx_p1 = mx[q + 5] * lxs[q + 5];
+            const float wy_m2 = my[0][q] * f4(ly[0], q), wy_m1 = my[1][q] * f4(ly[1], q);
+            const float wy_0 = my[2][q] * f4(ly[2], q), wy_p1 = my[3][q] * f4(ly[3], q);
+            const float wz_m2 = mz[0][q] * f4(lz[0], q), wz_m1 = mz[1][q] * f4(lz[1], q);
+            const float wz_0 = mz[2][q] * f4(lz[2], q), wz_p1 = mz[3][q] * f4(lz[3], q);
+            const float gt = kC1 * (wx_m1 - wx_0) + kC2 * (wx_m2 - wx_p1) + kC1 * (wy_m1 - wy_0) +
+                             kC2 * (wy_m2 - wy_p1) + kC1 * (wz_m1 - wz_0) + kC2 * (wz_m2 - wz_p1);
+            op[q] = f4(lp, q) - gt;
             const int x = x0 + q;
-            if (x >= g.Nx) break;
-            // lp' = lp - sum_c G_c^T w_c, w_c = a2 lam_c on M_c
-            float acc = L[o + q];
-            float gt = 0.f;
-            {   // vx: w at x-1, x, x-2, x+1
-                const float *W = L + g.vol;
-                auto w = [&](int xx) { return in_vx(g, z, y, xx) ? at3(g, A.a2, z, y, xx) * at3(g, W, z, y, xx) : 0.f; };
-                gt += kC1 * (w(x - 1) - w(x)) + kC2 * (w(x - 2) - w(x + 1));
-            }
-            {   // vy: rows y-1, y, y-2, y+1
-                const float *W = L + 2 * g.vol;
-                auto w = [&](int yy) { return in_vy(g, z, yy, x) ? at3(g, A.a2, z, yy, x) * at3(g, W, z, yy, x) : 0.f; };
-                gt += kC1 * (w(y - 1) - w(y)) + kC2 * (w(y - 2) - w(y + 1));
-            }
-            {   // vz: planes z-1, z, z-2, z+1
-                const float *W = L + 3 * g.vol;
-                auto w = [&](int zz) { return in_vz(g, zz, y, x) ? at3(g, A.a2, zz, y, x) * at3(g, W, zz, y, x) : 0.f; };
-                gt += kC1 * (w(z - 1) - w(z)) + kC2 * (w(z - 2) - w(z + 1));
-            }
-            acc -= gt;
-            O[o + q] = acc;
-            // own velocity cells
-            const float lx = L[g.vol + o + q], ly = L[2 * g.vol + o + q], lz = L[3 * g.vol + o + q];
-            const bool mx = in_vx(g, z, y, x), my = in_vy(g, z, y, x), mz = in_vz(g, z, y, x);
-            O[g.vol + o + q] = mx ? (1.f - A.k2[o + q]) * lx : lx;
-            O[2 * g.vol + o + q] = my ? (1.f - A.k3[o + q]) * ly : ly;
-            O[3 * g.vol + o + q] = mz ? (1.f - A.k4[o + q]) * lz : lz;
+            const float lxq = lxs[q + 4], lyq = f4(ly[2], q), lzq = f4(lz[2], q);
+            const bool bx = in_vx(g, z, y, x), by = in_vy(g, z, y, x), bz = in_vz(g, z, y, x);
+            ox[q] = bx ? (1.f - f4(k2, q)) * lxq : lxq;
+            oy[q] = by ? (1.f - f4(k3, q)) * lyq : lyq;
+            oz[q] = bz ? (1.f - f4(k4, q)) * lzq : lzq;
             if (A.G2) {
-                const long long jo = (long long)s * g.vol + o + q, js = (long long)g.n_shots * g.vol;
-                if (mx) g2[q] -= lx * A.img_j[jo];
-                if (my) g2[q] -= ly * A.img_j[js + jo];
-                if (mz) g2[q] -= lz * A.img_j[2 * js + jo];
+                if (bx) g2[q] -= lxq * f4(jx, q);
+                if (by) g2[q] -= lyq * f4(jy, q);
+                if (bz) g2[q] -= lzq * f4(jz, q);
             }
         }
+        *reinterpret_cast<float4 *>(O + o) = make_float4(op[0], op[1], op[2], op[3]);
+        *reinterpret_cast<float4 *>(O + g.vol + o) = make_float4(ox[0], ox[1], ox[2], ox[3]);
+        *reinterpret_cast<float4 *>(O + 2 * g.vol + o) = make_float4(oy[0], oy[1], oy[2], oy[3]);
+        *reinterpret_cast<float4 *>(O + 3 * g.vol + o) = make_float4(oz[0], oz[1], oz[2], oz[3]);
     }
     if (A.G2) {
 #pragma unroll
@@ -403,29 +440,62 @@ __global__ void __launch_bounds__(128) adj_p3_kernel(const AdjArgs3 A)
     const int z = blockIdx.z;
     if (x0 >= g.Nx || y >= g.Ny) return;
     const long long o = (long long)z * g.plane + (long long)y * g.pitch + x0;
+    // a1 times the p mask at the neighbours the transposed divergence reads:
+    // x-1 .. x+2, rows y-1 .. y+2, planes z-1 .. z+2 (the same for every shot)
+    float ux[12], uy[4][4], uz[4][4];
+    {
+        const float4 l = row4(g, A.a1, z, y, x0 - 4), c = row4(g, A.a1, z, y, x0), r = row4(g, A.a1, z, y, x0 + 4);
+        const float v[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
+#pragma unroll
+        for (int i = 0; i < 12; ++i) ux[i] = in_p(g, z, y, x0 - 4 + i) ? v[i] : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 ay = row4(g, A.a1, z, y + k - 1, x0), az = row4(g, A.a1, z + k - 1, y, x0);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uy[k][q] = in_p(g, z, y + k - 1, x0 + q) ? f4(ay, q) : 0.f;
+            uz[k][q] = in_p(g, z + k - 1, y, x0 + q) ? f4(az, q) : 0.f;
+        }
+    }
+    const float4 k1 = row4(g, A.k1, z, y, x0);
     float g1[4] = {0.f, 0.f, 0.f, 0.f};
     for (int s = 0; s < g.n_shots; ++s) {
         const float *L = A.lam_in + (long long)s * 4 * g.vol;     // lp' and lam_c'
         float *O = A.lam_out + (long long)s * 4 * g.vol;
-        auto u = [&](int zz, int yy, int xx) {
-            return in_p(g, zz, yy, xx) ? at3(g, A.a1, zz, yy, xx) * at3(g, L, zz, yy, xx) : 0.f;
-        };
+        const float4 pl = row4(g, L, z, y, x0 - 4), pc = row4(g, L, z, y, x0), pr = row4(g, L, z, y, x0 + 4);
+        const float ps[12] = {pl.x, pl.y, pl.z, pl.w, pc.x, pc.y, pc.z, pc.w, pr.x, pr.y, pr.z, pr.w};
+        float4 py[4], pz[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            py[k] = k == 1 ? pc : row4(g, L, z, y + k - 1, x0);
+            pz[k] = k == 1 ? pc : row4(g, L, z + k - 1, y, x0);
+        }
+        const float4 lvx = *reinterpret_cast<const float4 *>(L + g.vol + o);
+        const float4 lvy = *reinterpret_cast<const float4 *>(L + 2 * g.vol + o);
+        const float4 lvz = *reinterpret_cast<const float4 *>(L + 3 * g.vol + o);
+        const float4 im = *reinterpret_cast<const float4 *>(A.img_i + (long long)s * g.vol + o);
+        float op[4], ox[4], oy[4], oz[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int x = x0 + q;
-            if (x >= g.Nx) break;
-            const float lp = L[o + q];
+            const float lp = ps[q + 4];
             const bool mp = in_p(g, z, y, x);
-            O[o + q] = mp ? (1.f - A.k1[o + q]) * lp : lp;
-            if (mp) g1[q] += lp * A.img_i[(long long)s * g.vol + o + q];
-            // lam_c = lam_c' - D_c^T u
-            O[g.vol + o + q] = L[g.vol + o + q] -
-                               (kC1 * (u(z, y, x) - u(z, y, x + 1)) + kC2 * (u(z, y, x - 1) - u(z, y, x + 2)));
-            O[2 * g.vol + o + q] = L[2 * g.vol + o + q] -
-                                   (kC1 * (u(z, y, x) - u(z, y + 1, x)) + kC2 * (u(z, y - 1, x) - u(z, y + 2, x)));
-            O[3 * g.vol + o + q] = L[3 * g.vol + o + q] -
-                                   (kC1 * (u(z, y, x) - u(z + 1, y, x)) + kC2 * (u(z - 1, y, x) - u(z + 2, y, x)));
+            op[q] = mp ? (1.f - f4(k1, q)) * lp : lp;
+            if (mp) g1[q] += lp * f4(im, q);
+            // u = a1 lp' on the p mask; lam_c = lam_c' - D_c^T u
+            const float u0 = ux[q + 4] * ps[q + 4], uxp1 = ux[q + 5] * ps[q + 5];
+            const float uxm1 = ux[q + 3] * ps[q + 3], uxp2 = ux[q + 6] * ps[q + 6];
+            ox[q] = f4(lvx, q) - (kC1 * (u0 - uxp1) + kC2 * (uxm1 - uxp2));
+            const float uym1 = uy[0][q] * f4(py[0], q), uyp1 = uy[2][q] * f4(py[2], q), uyp2 = uy[3][q] * f4(py[3], q);
+            oy[q] = f4(lvy, q) - (kC1 * (u0 - uyp1) + kC2 * (uym1 - uyp2));
+            const float uzm1 = uz[0][q] * f4(pz[0], q), uzp1 = uz[2][q] * f4(pz[2], q), uzp2 = uz[3][q] * f4(pz[3], q);
+            oz[q] = f4(lvz, q) - (kC1 * (u0 - uzp1) + kC2 * (uzm1 - uzp2));
         }
+        *reinterpret_cast<float4 *>(O + o) = make_float4(op[0], op[1], op[2], op[3]);
+        *reinterpret_cast<float4 *>(O + g.vol + o) = make_float4(ox[0], ox[1], ox[2], ox[3]);
+        *reinterpret_cast<float4 *>(O + 2 * g.vol + o) = make_float4(oy[0], oy[1], oy[2], oy[3]);
+        *reinterpret_cast<float4 *>(O + 3 * g.vol + o) = make_float4(oz[0], oz[1], oz[2], oz[3]);
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
