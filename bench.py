@@ -347,6 +347,7 @@ def main():
         extras = plain_forward_rates(torch, wave, synthetic, dev)
         extras.update(batch_rates(torch, wave, synthetic, dev))
         extras.update(large_gradient_rate(torch, wave, synthetic, dev))
+        extras.update(rates_3d(torch, wave, dev))
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -490,6 +491,39 @@ def large_gradient_rate(torch, wave, synthetic, dev, cap_bytes=60 * 10**9):
         "gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms, "nt": w.nt, "shots": w.n_shots,
         "memory_cap_bytes": cap_bytes, "peak_bytes_above_inputs": int(peak), "checkpoint_every": K,
         "checkpoints": "bf16, one scale per (checkpoint, shot, field)", "imaging": "fp24"}}
+
+
+def rates_3d(torch, wave, dev, nz=200, ny=200, nx=200, shots=4, nt=200, nabc=20):
+    """The 3-D path (acoustic_forward_kernel_3d, 4th order): forward and
+    gradient (forward + adjoint of 0.5 ||p||^2, checkpointed recompute) on a
+    200^3 model with a 20-cell PML and 4 shots, seeded random velocities."""
+    rng = np.random.default_rng(0)
+    vp = torch.tensor((2000 + 1000 * rng.random((nz, ny, nx))).astype(np.float32), device=dev)
+    rho = torch.full((nz, ny, nx), 2000.0, device=dev)
+    damp = torch.tensor(wave.bc_pml_3d(nx, ny, nz, 10.0, 10.0, 10.0, nabc, 3000.0, free_surface=False)
+                        .astype(np.float32), device=dev)
+    w, _ = wave.RickerWavelet()(f0=15.0, dt=1e-3)
+    w = torch.tensor(np.pad(w.numpy(), (0, nt))[:nt], device=dev)
+    kw = dict(nx=nx, ny=ny, nz=nz, dx=10.0, dy=10.0, dz=10.0, nt=nt, dt=1e-3, nabc=nabc, free_surface=False,
+              src_x=np.linspace(10, nx - 10, shots).astype(np.int64), src_y=np.full(shots, ny // 2),
+              src_z=np.ones(shots, np.int64), src_n=shots, src_v=w, rcv_x=np.arange(0, nx, 2),
+              rcv_y=np.full(nx // 2, ny // 2), rcv_z=np.ones(nx // 2, np.int64), rcv_n=nx // 2, damp=damp,
+              rho=rho, device=dev)
+    units = shots * (nz + 2 * nabc) * (ny + 2 * nabc) * (nx + 2 * nabc) * nt
+
+    def fwd():
+        with torch.no_grad():
+            wave.acoustic_forward_kernel_3d(vp=vp, **kw)
+
+    def grad():
+        v = vp.detach().requires_grad_(True)
+        out = wave.acoustic_forward_kernel_3d(vp=v, **kw)
+        (0.5 * (out["p"] * out["p"]).sum()).backward()
+
+    ms_f, ms_g = _timed(torch, fwd, 2), _timed(torch, grad, 1)
+    return {"3d_200x200x200_4shots": {"forward_gcell_updates_per_s": units / (ms_f * 1e-3) / 1e9,
+                                      "forward_ms": ms_f, "gradient_gcell_updates_per_s": units / (ms_g * 1e-3) / 1e9,
+                                      "gradient_ms": ms_g, "nt": nt, "fd_order": 4}}
 
 
 if __name__ == "__main__":
