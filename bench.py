@@ -380,18 +380,20 @@ def main():
 
 def plain_forward_rates(torch, wave, synthetic, dev):
     """Plain forward kernel rates beside the gradient: the 400 x 1200 grid
-    with one shot and with 32 shots, and the 100 x 200 4th-order workload."""
+    with one shot and with 32 shots (damping layers, and the CPML option),
+    and the 100 x 200 4th-order workload."""
     out = {}
-    for name, w, shots in (("fwd_400x1200_1shot", synthetic.fwi_400x1200(nt=3000, n_shots=1), 1),
-                           ("fwd_400x1200_32shots", synthetic.fwi_400x1200(nt=1000), 32),
-                           ("fwd_100x200_1shot", synthetic.plain_forward_100x200(), 1)):
+    for name, w, absorbing in (("fwd_400x1200_1shot", synthetic.fwi_400x1200(nt=3000, n_shots=1), "damping"),
+                               ("fwd_400x1200_32shots", synthetic.fwi_400x1200(nt=1000), "damping"),
+                               ("fwd_400x1200_32shots_cpml", synthetic.fwi_400x1200(nt=1000), "cpml"),
+                               ("fwd_100x200_1shot", synthetic.plain_forward_100x200(), "damping")):
         damp = torch.tensor(wave.bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp.max()), False),
                             dtype=torch.float32, device=dev)
         kw = dict(nx=w.nx, nz=w.nz, dx=w.dx, dz=w.dx, nt=w.nt, dt=w.dt, nabc=w.nabc, free_surface=False,
                   src_x=w.src_x, src_z=w.src_z, src_n=w.n_shots,
                   src_v=torch.tensor(np.tile(w.wavelet, (w.n_shots, 1)), device=dev), rcv_x=w.rcv_x,
                   rcv_z=w.rcv_z, rcv_n=w.rcv_x.size, damp=damp, vp=torch.tensor(w.vp, device=dev),
-                  rho=torch.tensor(w.rho, device=dev), device=dev, fd_order=w.fd_order)
+                  rho=torch.tensor(w.rho, device=dev), device=dev, fd_order=w.fd_order, absorbing=absorbing)
         for _ in range(2):
             wave.acoustic_forward_kernel(**kw)
         torch.cuda.synchronize()
@@ -404,7 +406,7 @@ def plain_forward_rates(torch, wave, synthetic, dev):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
         out[name] = {"gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms,
-                     "fd_order": w.fd_order, "nt": w.nt, "shots": w.n_shots}
+                     "fd_order": w.fd_order, "nt": w.nt, "shots": w.n_shots, "absorbing": absorbing}
     return out
 
 

@@ -78,6 +78,7 @@ SIGNATURES = {
                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int)]),
     "gb_plan_set_streaming": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
+    "gb_plan_set_absorbing": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_float]),
     "gb_plan_autotune": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _I32, _P, ctypes.POINTER(ctypes.c_float)]),
     "gb_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P, _P, _SZ, _P]),
     "gb_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),

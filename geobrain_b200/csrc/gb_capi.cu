@@ -134,7 +134,13 @@ struct gb_plan {
     // stream_chunks 16-row chunks per z-segment (0 = automatic)
     bool stream = false;
     int stream_chunks = 0;
-    bool stream_usable() const { return stream && !d.free_surface && tz == 16; }
+    bool stream_usable() const { return stream && !d.free_surface && tz == 16 && !cpml; }
+    // CPML absorbing layers in place of the damping (gb_plan_set_absorbing):
+    // profiles [bz, az, bz_half, az_half][Nz] + [bx, ax, bx_half, ax_half][pitch]
+    bool cpml = false;
+    float cpml_vmax = 0.f;
+    std::vector<float> cpml_prof;
+    int4 cpml_still{0, 0, 0, 0};   // rows [x, y] x cols [z, w] where the profiles vanish
     int seg_chunks() const
     {
         if (stream_chunks > 0) return stream_chunks;
@@ -279,7 +285,7 @@ namespace {
 
 // Workspace layout (offsets in bytes from the 256-aligned base).
 struct Layout {
-    size_t err, coef, fields, energy, src, rcv_ptr, rcv_ent, tile_fast, amax, total;
+    size_t err, coef, fields, energy, src, rcv_ptr, rcv_ent, tile_fast, amax, cpml, psi, total;
     // gradient only
     size_t mu, img, g1, c1, g2, c2, arcv_ptr, arcv_ent;
     int n_img;
@@ -304,6 +310,10 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
     L.rcv_ent = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 16);
     L.tile_fast = o; o = align256(o + (size_t)p->n_tiles * 4);
     L.amax = o; o = align256(o + S * 3 * 4);
+    if (p->cpml) {
+        L.cpml = o; o = align256(o + (4 * (size_t)p->Nz + 4 * (size_t)p->pitch) * 4);
+        L.psi = o; o = align256(o + 2 * S * 4 * p->plane * 4);   // two levels of the memory variables
+    }
     L.n_img = with_gradient >= 2 ? 3 : 1;
     if (with_gradient > 0) {
         const size_t K = std::max(1, std::min(checkpoint_every, p->d.nt));
@@ -447,10 +457,11 @@ int make_maps(const gb_plan *P, const float *buf, const float *a1, const float *
 int launch_tile_flags(gb_plan *P, const StepGeom &g, const float *k1, const float *k2, const float *k3, int *flags,
                       cudaStream_t st)
 {
-    if (P->R == 2 && P->tz == 16) tile_fast_kernel<2, 16><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags);
-    if (P->R == 2 && P->tz == 32) tile_fast_kernel<2, 32><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags);
-    if (P->R == 4 && P->tz == 16) tile_fast_kernel<4, 16><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags);
-    if (P->R == 4 && P->tz == 32) tile_fast_kernel<4, 32><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags);
+    const int4 still = P->cpml ? P->cpml_still : int4{-(1 << 24), 1 << 24, -(1 << 24), 1 << 24};
+    if (P->R == 2 && P->tz == 16) tile_fast_kernel<2, 16><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags, still);
+    if (P->R == 2 && P->tz == 32) tile_fast_kernel<2, 32><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags, still);
+    if (P->R == 4 && P->tz == 16) tile_fast_kernel<4, 16><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags, still);
+    if (P->R == 4 && P->tz == 32) tile_fast_kernel<4, 32><<<P->n_tiles, 256, 0, st>>>(g, k1, k2, k3, flags, still);
     GB_CUDA(cudaGetLastError());
     ++P->launches;
     return GB_OK;
@@ -563,7 +574,7 @@ inline void launch_groups(const GroupStreams &gs, int i, int n_groups, int *g0, 
 constexpr int kMaxGraphSteps = 64;
 
 int capture_forward_chunk(gb_plan *P, const StepKernel &K, const Maps (&maps)[2], float *const (&buf)[2],
-                          FwdArgs A, int C, int *step_ctr, cudaGraphExec_t *out)
+                          float *const (&psi)[2], FwdArgs A, int C, int *step_ctr, cudaGraphExec_t *out)
 {
     GroupStreams gs;
     if (int rc = group_streams(P, nullptr, &gs)) return rc;      // (re)creating the group streams drops cap_stream
@@ -576,6 +587,10 @@ int capture_forward_chunk(gb_plan *P, const StepKernel &K, const Maps (&maps)[2]
     for (int j = 0; j < C && rc == GB_OK; ++j) {
         A.it = j;
         A.out = buf[(j & 1) ^ 1];
+        if (A.cpml) {
+            A.psi_in = psi[j & 1];
+            A.psi_out = psi[(j & 1) ^ 1];
+        }
         for (int i = 0; i < gs.n && rc == GB_OK; ++i) {
             int g0, gc;
             launch_groups(gs, i, P->n_groups, &g0, &gc);
@@ -667,6 +682,7 @@ struct Setup {
     int *d_src, *d_rptr, *tile_fast;
     int4 *d_rent;
     unsigned int *amax;
+    float *cpml = nullptr, *psi[2] = {nullptr, nullptr};
 };
 
 int common_setup(gb_plan *P, const Layout &L, char *ws, const float *vp, const float *rho, const float *damp,
@@ -694,6 +710,16 @@ int common_setup(gb_plan *P, const Layout &L, char *ws, const float *vp, const f
                                          S->a1, S->k1, S->a2, S->k2, S->k3);
     GB_CUDA(cudaGetLastError());
     ++P->launches;
+    if (P->cpml) {
+        // the CPML layers replace the damping: no k terms, profiles and memory variables instead
+        GB_CUDA(cudaMemsetAsync(S->k1, 0, P->plane * 4, st));       // k1, then k2 and k3 (a2 sits between)
+        GB_CUDA(cudaMemsetAsync(S->k2, 0, 2 * P->plane * 4, st));
+        S->cpml = reinterpret_cast<float *>(ws + L.cpml);
+        S->psi[0] = reinterpret_cast<float *>(ws + L.psi);
+        S->psi[1] = S->psi[0] + (size_t)d.n_shots * 4 * P->plane;
+        GB_CUDA(cudaMemcpyAsync(S->cpml, P->cpml_prof.data(), P->cpml_prof.size() * 4, cudaMemcpyHostToDevice, st));
+        GB_CUDA(cudaMemsetAsync(S->psi[0], 0, 2 * (size_t)d.n_shots * 4 * P->plane * 4, st));
+    }
     return launch_tile_flags(P, P->geom(), S->k1, S->k2, S->k3, S->tile_fast, st);
 }
 
@@ -829,6 +855,47 @@ int gb_plan_get_config(const gb_plan *p, int *tile_rows, int *shots_per_cta, int
     return GB_OK;
 }
 
+int gb_plan_set_absorbing(gb_plan *p, int mode, float vmax)
+{
+    if (!p) return fail(GB_E_ARG, "null plan");
+    if (mode != GB_ABSORB_DAMPING && mode != GB_ABSORB_CPML) return fail(GB_E_ARG, "unknown absorbing mode");
+    if (mode == GB_ABSORB_CPML && !(vmax > 0.f)) return fail(GB_E_ARG, "CPML needs vmax > 0");
+    if ((mode == GB_ABSORB_CPML) == p->cpml && (!p->cpml || vmax == p->cpml_vmax)) return GB_OK;   // unchanged
+    p->release_graph();
+    p->cpml = mode == GB_ABSORB_CPML;
+    p->cpml_vmax = vmax;
+    p->cpml_prof.clear();
+    if (!p->cpml) return GB_OK;
+    const int pml = p->d.nabc;
+    if (pml < 1) return fail(GB_E_ARG, "CPML needs nabc >= 1");
+    // quadratic profile d(r) = d0 r^2, r = depth into the layer / nabc, d0 for
+    // a 1e-6 reflection; b = exp(-d dt), a = b - 1 (no kappa / alpha terms)
+    const double d0 = -3.0 * vmax * std::log(1e-6) / (2.0 * pml * p->d.dx), dt = p->d.dt;
+    auto depth = [&](double c, int N, bool lo) {
+        double r = 0.0;
+        if (lo && c < pml) r = (pml - c) / pml;
+        else if (c > N - 1 - pml) r = (c - (N - 1 - pml)) / pml;
+        return std::min(r, 1.0);
+    };
+    p->cpml_prof.assign(4 * (size_t)p->Nz + 4 * (size_t)p->pitch, 0.f);
+    float *z = p->cpml_prof.data(), *x = z + 4 * p->Nz;
+    const bool top = !p->d.free_surface;   // a free surface has no layer above it
+    for (int i = 0; i < p->Nz; ++i)
+        for (int h = 0; h < 2; ++h) {
+            const double r = depth(i + 0.5 * h, p->Nz, top), b = std::exp(-d0 * r * r * dt);
+            z[(2 * h) * p->Nz + i] = (float)b;
+            z[(2 * h + 1) * p->Nz + i] = (float)(b - 1.0);
+        }
+    for (int j = 0; j < p->pitch; ++j)
+        for (int h = 0; h < 2; ++h) {
+            const double r = j < p->Nx ? depth(j + 0.5 * h, p->Nx, true) : 0.0, b = std::exp(-d0 * r * r * dt);
+            x[(2 * h) * p->pitch + j] = (float)b;
+            x[(2 * h + 1) * p->pitch + j] = (float)(b - 1.0);
+        }
+    p->cpml_still = int4{top ? pml : -(1 << 24), p->Nz - 2 - pml, pml, p->Nx - 2 - pml};
+    return GB_OK;
+}
+
 int gb_plan_set_streaming(gb_plan *p, int enable, int seg_chunks)
 {
     if (!p) return fail(GB_E_ARG, "null plan");
@@ -926,6 +993,7 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
     A.img_field_stride = (long long)S * P->plane;
     A.img_fmt = store ? store->imaging_format : GB_IMG_F32;
     A.err = Su.err;
+    A.cpml = Su.cpml;
     const size_t img_es = store ? img_esize(store->imaging_format) : 4;
 
     GroupStreams gs;
@@ -949,7 +1017,7 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
             (uintptr_t)P->n_groups, (uintptr_t)gs.n, (uintptr_t)K0.fn};
         if (!P->gexec || P->gkey != key) {
             P->release_graph();
-            if (int rc = capture_forward_chunk(P, K0, maps, buf, A, C, step_ctr, &P->gexec)) return rc;
+            if (int rc = capture_forward_chunk(P, K0, maps, buf, Su.psi, A, C, step_ctr, &P->gexec)) return rc;
             P->gkey = key;
         }
         step_set_kernel<<<1, 1, 0, st>>>(step_ctr, 0);
@@ -974,6 +1042,10 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
         const int b = it & 1;
         A.it = it;
         A.out = buf[b ^ 1];
+        if (Su.cpml) {
+            A.psi_in = Su.psi[b];
+            A.psi_out = Su.psi[b ^ 1];
+        }
         const bool keep = store && it >= t_cache;
         A.imaging = keep ? img_at(store->imaging, (size_t)(it - t_cache) * step_img, img_es) : nullptr;
         for (int i = 0; i < gs.n; ++i) {
@@ -1415,6 +1487,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     if (!P || !vp || !rho || !damp || !wavelet || !store || !grad_vp) return fail(GB_E_ARG, "null argument");
     if (int rc = check_store(P, store)) return rc;
     if (grad_rho && !store->with_rho) return fail(GB_E_ARG, "density gradient needs a store made with with_rho");
+    if (P->cpml) return fail(GB_E_UNSUPPORTED, "the CPML option has no adjoint: gradients need the damping layers");
     const gb_model_desc &d = P->d;
     const int S = d.n_shots;
     const int K = std::min<int>(store->checkpoint_every, d.nt);
@@ -1677,6 +1750,7 @@ int check_batch(gb_plan *const *plans, int n, const gb_model_io *io, bool gradie
         if (P->R != plans[0]->R || (P->d.free_surface != 0) != (plans[0]->d.free_surface != 0))
             return fail(GB_E_ARG, "a batch needs one stencil order and one free-surface setting");
         if (P->tz != 16) return fail(GB_E_ARG, "batched plans use 16-row tiles (gb_plan_set_tiling(plan, 16, ...))");
+        if (P->cpml) return fail(GB_E_UNSUPPORTED, "batched runs use the damping layers, not CPML");
         const gb_model_io &x = io[m];
         if (!x.vp || !x.rho || !x.damp || !x.wavelet || !x.workspace) return fail(GB_E_ARG, "null model input");
         if (gradient) {

@@ -57,6 +57,13 @@ struct FwdArgs {
     int img_fmt;                     // storage format of the imaging fields (kImg*)
     int grp0, grp_count;             // shot groups this launch covers
     int *err;
+    // CPML option (null otherwise): profiles [bz, az (integer rows), bz, az
+    // (half rows)][Nz] then [bx, ax (integer cols), bx, ax (half cols)][pitch],
+    // and the memory variables [S][psi_px, psi_pz, psi_vx, psi_vz][plane],
+    // read from psi_in and written to psi_out (two levels, as the state)
+    const float *cpml;
+    const float *psi_in;
+    float *psi_out;
 };
 
 template <int R>
@@ -214,16 +221,43 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                     } else {
                         const bool row_in = gz >= g.p_r0 && gz <= g.p_r1;
                         if (row_in && (gx0 + 3 >= g.p_c0) && (gx0 <= g.p_c1)) {
-                            divergence4<R>(sVX + r * VXW, lane, wz, u, g.c, D);
                             const long long o = (long long)gz * g.pitch + gx0;
-                            const float4 k1 = ldg4(A.k1 + o);
                             float4 img;
+                            if (A.cpml) {
+                                // psi' = b psi + a d, p' = p - a1 ((Dx + psi_x') + (Dz + psi_z'))
+                                float Dx[4], Dz[4];
+                                divergence4_split<R>(sVX + r * VXW, lane, wz, u, g.c, Dx, Dz);
+                                const float bz = A.cpml[gz], az = A.cpml[g.Nz + gz];
+                                const float *xp = A.cpml + 4 * g.Nz;
+                                const float4 bx = ldg4(xp + gx0), ax = ldg4(xp + g.pitch + gx0);
+                                const long long po = (long long)s * 4 * g.plane + o;
+                                const float4 ox = ldg4(A.psi_in + po), oz = ldg4(A.psi_in + po + g.plane);
+                                float4 nx = ox, nz = oz;
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                const int gx = gx0 + q;
-                                const bool m = gx >= g.p_c0 && gx <= g.p_c1;
-                                at(img, q) = m ? -D[q] : 0.f;
-                                if (m) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], (1.f - at(k1, q)) * at(pv, q));
+                                for (int q = 0; q < 4; ++q) {
+                                    const int gx = gx0 + q;
+                                    const bool m = gx >= g.p_c0 && gx <= g.p_c1;
+                                    at(img, q) = 0.f;
+                                    if (m) {
+                                        at(nx, q) = __fadd_rn(__fmul_rn(at(bx, q), at(ox, q)), __fmul_rn(at(ax, q), Dx[q]));
+                                        at(nz, q) = __fadd_rn(__fmul_rn(bz, at(oz, q)), __fmul_rn(az, Dz[q]));
+                                        const float sd = __fadd_rn(__fadd_rn(Dx[q], at(nx, q)), __fadd_rn(Dz[q], at(nz, q)));
+                                        at(pv, q) = __fsub_rn(at(pv, q), __fmul_rn(at(a1, q), sd));
+                                        at(img, q) = -sd;
+                                    }
+                                }
+                                stg4(A.psi_out + po, nx);
+                                stg4(A.psi_out + po + g.plane, nz);
+                            } else {
+                                divergence4<R>(sVX + r * VXW, lane, wz, u, g.c, D);
+                                const float4 k1 = ldg4(A.k1 + o);
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    const int gx = gx0 + q;
+                                    const bool m = gx >= g.p_c0 && gx <= g.p_c1;
+                                    at(img, q) = m ? -D[q] : 0.f;
+                                    if (m) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], (1.f - at(k1, q)) * at(pv, q));
+                                }
                             }
                             if (tile_cell && A.imaging)
                                 store_img4(A.imaging, (long long)s * g.plane + o, A.img_fmt, img);
@@ -290,7 +324,31 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                             const bool vz_row = gz >= g.vz_r0 && gz <= g.vz_r1;
                             const bool need = (vx_row && gx0 + 3 >= g.vx_c0 && gx0 <= g.vx_c1) ||
                                               (vz_row && gx0 + 3 >= g.vz_c0 && gx0 <= g.vz_c1);
-                            if (need) {
+                            if (need && A.cpml) {
+                                // psi' = b psi + a G, v' = v - a2 (G + psi')
+                                const float bz = A.cpml[2 * g.Nz + gz], az = A.cpml[3 * g.Nz + gz];
+                                const float *xp = A.cpml + 4 * g.Nz;
+                                const float4 bx = ldg4(xp + 2 * g.pitch + gx0), ax = ldg4(xp + 3 * g.pitch + gx0);
+                                const long long po = (long long)s * 4 * g.plane + o;
+                                const float4 ox = ldg4(A.psi_in + po + 2 * g.plane), oz = ldg4(A.psi_in + po + 3 * g.plane);
+                                float4 nx = ox, nz = oz;
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    const int gx = gx0 + q;
+                                    if (vx_row && gx >= g.vx_c0 && gx <= g.vx_c1) {
+                                        at(nx, q) = __fadd_rn(__fmul_rn(at(bx, q), at(ox, q)), __fmul_rn(at(ax, q), Dx[q]));
+                                        at(jx, q) = __fadd_rn(Dx[q], at(nx, q));
+                                        at(vx, q) = __fsub_rn(at(vx, q), __fmul_rn(at(a2, q), at(jx, q)));
+                                    }
+                                    if (vz_row && gx >= g.vz_c0 && gx <= g.vz_c1) {
+                                        at(nz, q) = __fadd_rn(__fmul_rn(bz, at(oz, q)), __fmul_rn(az, Dz[q]));
+                                        at(jz, q) = __fadd_rn(Dz[q], at(nz, q));
+                                        at(vz, q) = __fsub_rn(at(vz, q), __fmul_rn(at(a2, q), at(jz, q)));
+                                    }
+                                }
+                                stg4(A.psi_out + po + 2 * g.plane, nx);
+                                stg4(A.psi_out + po + 3 * g.plane, nz);
+                            } else if (need) {
                                 const float4 k2 = ldg4(A.k2 + o);
                                 const float4 k3 = ldg4(A.k3 + o);
 #pragma unroll
@@ -392,11 +450,13 @@ constexpr size_t fwd_smem_bytes()
 // see no damping (k1 on the p rectangle, k2 / k3 on the tile all zero).
 template <int R, int TZ>
 __global__ void tile_fast_kernel(const StepGeom g, const float *__restrict__ k1, const float *__restrict__ k2,
-                                 const float *__restrict__ k3, int *flags)
+                                 const float *__restrict__ k3, int *flags, int4 still)
 {
     const int tile = blockIdx.x;
     const int z0 = (tile / g.tiles_x) * TZ, x0 = (tile % g.tiles_x) * TX;
-    bool ok = tile_is_interior<R, TZ>(g, z0, x0);
+    // still: rows [x, y] x cols [z, w] where the CPML profiles vanish (the whole grid without CPML)
+    bool ok = tile_is_interior<R, TZ>(g, z0, x0) && z0 - R >= still.x && z0 + TZ + R - 1 <= still.y &&
+              x0 - 4 >= still.z && x0 + TX + 3 <= still.w;
     bool damped = false;
     if (ok) {
         for (int i = threadIdx.x; i < (TZ + 2 * R) * RW; i += blockDim.x) {

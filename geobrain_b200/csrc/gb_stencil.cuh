@@ -38,6 +38,34 @@ __device__ __forceinline__ void divergence4(const float *vxr, int lane, const fl
     }
 }
 
+// The two parts of divergence4 kept apart (the CPML option needs each one):
+//   Dx[q] = sum_k c_k (vx[j+k] - vx[j-1-k]),  Dz[q] = sum_k c_k (vz[i+k] - vz[i-1-k])
+template <int R>
+__device__ __forceinline__ void divergence4_split(const float *vxr, int lane, const float4 *wz, int u,
+                                                  const float (&c)[4], float (&Dx)[4], float (&Dz)[4])
+{
+    float e[12];
+    {
+        const float4 e0 = lds4(vxr + 4 * lane);
+        const float4 e1 = lds4(vxr + 4 * lane + 4);
+        const float4 e2 = lds4(vxr + 4 * lane + 8);
+        e[0] = e0.x; e[1] = e0.y; e[2] = e0.z; e[3] = e0.w;
+        e[4] = e1.x; e[5] = e1.y; e[6] = e1.z; e[7] = e1.w;
+        e[8] = e2.x; e[9] = e2.y; e[10] = e2.z; e[11] = e2.w;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        float dx = 0.f, dz = 0.f;
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            dx = __fmaf_rn(c[k], e[q + 4 + k] - e[q + 3 - k], dx);
+            dz = __fmaf_rn(c[k], at(wz[u + R + k], q) - at(wz[u + R - 1 - k], q), dz);
+        }
+        Dx[q] = dx;
+        Dz[q] = dz;
+    }
+}
+
 // x-derivative of p at the staggered vx points of 4 adjacent cells:
 //   D[q] = sum_k c_k (p[j+1+k] - p[j-k])        (acoustic_2d.py:248-252)
 // pr: the row of the p rectangle (128 wide, column 0 = x0 - 4); the lane's

@@ -138,6 +138,14 @@ class Plan:
         return {"tile_rows": tz.value, "shots_per_cta": spc.value, "group_streams": bool(streams.value),
                 "graph_steps": graph.value, "stream_chunks": chunks.value}
 
+    def set_absorbing(self, mode: str = "damping", vmax: float = 0.0) -> None:
+        """'damping' (the reference's damping PML) or 'cpml' (memory-variable
+        CPML with a profile for vmax; forward only)."""
+        modes = {"damping": 0, "cpml": 1}
+        if mode not in modes:
+            raise ValueError(f"absorbing must be one of {sorted(modes)}, got {mode!r}")
+        _lib.check(self._lib.gb_plan_set_absorbing(self.h, modes[mode], float(vmax)))
+
     def set_streaming(self, enable: bool, seg_chunks: int = 0) -> None:
         """Forward steps by the streaming kernel (0 chunks = automatic)."""
         _lib.check(self._lib.gb_plan_set_streaming(self.h, int(bool(enable)), int(seg_chunks)))

@@ -15,7 +15,9 @@ behaviour: fd_order (4 or 8); checkpoint_every, snapshot_dtype ('fp32',
 imaging_dtype ('fp32'; 'fp24', 3 bytes, gradient error about 1e-5; 'bf16',
 2 bytes, about 3e-3: more cached steps skip the recompute) for the
 gradient's memory, and memory_budget (bytes the gradient's store and
-workspaces may take, for the 'auto' cache); want_energy (skip the energy
+workspaces may take, for the 'auto' cache); absorbing ('damping', the
+reference's PML driven by damp, or 'cpml': memory-variable convolutional
+PML layers, forward only, damp unused); want_energy (skip the energy
 sums); autotune (on the
 first call for a geometry, time the launch configurations and keep the
 fastest; GEOBRAIN_B200_AUTOTUNE=1 turns it on by default).
@@ -55,7 +57,8 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
                             dtype: torch.dtype = torch.float32, snapshot_every: int = 0, *,
                             fd_order: int = 4, checkpoint_every: int = 0, snapshot_dtype: str = "fp32",
                             want_energy: bool = True, imaging_cache="auto", imaging_dtype: str = "fp32",
-                            autotune: Optional[bool] = None, memory_budget: Optional[int] = None):
+                            autotune: Optional[bool] = None, memory_budget: Optional[int] = None,
+                            absorbing: str = "damping"):
     device = torch.device(device)
     if device.type != "cuda":
         raise ValueError(f"geobrain_b200 runs on CUDA devices only (device={device})")
@@ -90,6 +93,15 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
         if tuple(t.shape) != (int(nz), int(nx)):
             raise ValueError(f"{name} must have shape {(int(nz), int(nx))}, got {tuple(t.shape)}")
 
+    needs_grad_now = torch.is_grad_enabled() and (getattr(vp, "requires_grad", False) or
+                                                  getattr(rho, "requires_grad", False))
+    if absorbing == "cpml":
+        if needs_grad_now:
+            raise NotImplementedError("the CPML option is forward-only; gradients use absorbing='damping'")
+        vmax = float(vp.detach().max()) if torch.is_tensor(vp) else float(torch.as_tensor(vp).max())
+        plan.set_absorbing("cpml", vmax)
+    else:
+        plan.set_absorbing(absorbing)
     if autotune is None:
         autotune = os.environ.get("GEOBRAIN_B200_AUTOTUNE", "0") not in ("", "0")
     if autotune and plan.tuned is None:

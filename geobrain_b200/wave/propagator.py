@@ -90,7 +90,8 @@ class AcousticPropagator(AbstractPropagator):
     def forward(self, model: Optional[AcousticModel] = None, shot_index: Optional[int] = None,
                 checkpoint_segments: int = 1, snapshot_every: int = 0, *, checkpoint_every: int = 0,
                 snapshot_dtype: str = "fp32", want_energy: bool = True, imaging_cache="auto",
-                imaging_dtype: str = "fp32", memory_budget: Optional[int] = None) -> WaveResult:
+                imaging_dtype: str = "fp32", memory_budget: Optional[int] = None,
+                absorbing: str = "damping") -> WaveResult:
         model = model if model is not None else self.model
         model.forward()
         if checkpoint_segments > 1 and not any(p.requires_grad for p in model.parameters()):
@@ -116,7 +117,7 @@ class AcousticPropagator(AbstractPropagator):
             checkpoint_segments=checkpoint_segments, device=torch.device(self.device), dtype=self.dtype,
             snapshot_every=snapshot_every, fd_order=self.fd_order, checkpoint_every=checkpoint_every,
             snapshot_dtype=snapshot_dtype, want_energy=want_energy, imaging_cache=imaging_cache,
-            imaging_dtype=imaging_dtype, memory_budget=memory_budget)
+            imaging_dtype=imaging_dtype, memory_budget=memory_budget, absorbing=absorbing)
         return WaveResult.from_dict(result)
 
     def __call__(self, model: Optional[AcousticModel] = None, shot_index: Optional[int] = None,

@@ -140,6 +140,22 @@ int gb_plan_get_config(const gb_plan *plan, int *tile_rows, int *shots_per_cta, 
  * tiles are 16 rows and the model has no free surface; otherwise the tile
  * kernel runs.  Off by default; the autotuner tries it. */
 int gb_plan_set_streaming(gb_plan *plan, int enable, int seg_chunks);
+
+/* Absorbing layers.  GB_ABSORB_DAMPING (default) is the reference's
+ * damping PML, driven by the damp array (boundary/pml.py).
+ * GB_ABSORB_CPML is an opt-in convolutional PML with memory variables, an
+ * extension the reference does not have; the damp array is not used:
+ *   - per axis, a quadratic profile d = d0 (depth / nabc)^2 with
+ *     d0 = -3 vmax ln(1e-6) / (2 nabc dx), on both sides (not above a free
+ *     surface); b = exp(-d dt), a = b - 1, at integer and half points;
+ *   - every derivative g entering an update becomes g + psi, with
+ *     psi' = b psi + a g (psi_px, psi_pz for p; psi_vx, psi_vz for the
+ *     velocities), and the k damping terms are dropped.
+ * Forward only (gb_backward and batched runs reject CPML plans); the
+ * streaming kernel is not used with it. */
+#define GB_ABSORB_DAMPING 0
+#define GB_ABSORB_CPML    1
+int gb_plan_set_absorbing(gb_plan *plan, int mode, float vmax);
 int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const float *damp,
                      const float *wavelet, void *workspace, size_t workspace_bytes, int32_t steps,
                      void *stream, float *best_ms_per_step);

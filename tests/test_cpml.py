@@ -1,0 +1,120 @@
+"""The CPML absorbing option of the 2-D forward (absorbing='cpml'): the
+NumPy oracle's structure against the C oracle, the CUDA path against the
+oracle (1e-5 relative L2), and the reason for the option: less reflection
+from the grid edges than the damping PML at the same layer width."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_case, oracle_kwargs
+from oracle import cpml as ocp
+from oracle import oracle as orc
+
+
+@pytest.mark.parametrize("name", ["small_nofs", "small_fs"])
+@pytest.mark.parametrize("half", [2, 4])
+def test_oracle_without_profiles_is_the_undamped_scheme(name, half):
+    """With vanishing profiles the CPML scheme is the reference's leapfrog
+    without damping: the oracle reproduces the C oracle run with damp = 0."""
+    c = load_case(name)
+    kw = oracle_kwargs(c)
+    kw.pop("damp")
+    a = ocp.forward(**kw, half=half, vmax=1e-30)
+    b = orc.forward(**dict(oracle_kwargs(c), damp=np.zeros_like(c["damp"])), half=half, dtype=np.float64)
+    for k in ("p", "vx", "vz", "forward_wavefield_p"):
+        assert orc.rel_l2(a[k], b[k]) < 1e-12, k
+
+
+def test_profiles():
+    bi, ai, bh, ah = ocp.profiles(60, 10, 10.0, 1e-3, 3000.0, lo=True)
+    assert np.all((bi > 0) & (bi <= 1)) and np.allclose(ai, bi - 1)
+    assert np.all(ai[10:50] == 0) and np.all(ah[10:49] == 0)       # interior: no absorption
+    assert ai[0] < ai[5] < 0 and ai[-1] < ai[-5] < 0               # deeper into the layer: stronger
+    bi, ai, _, _ = ocp.profiles(60, 10, 10.0, 1e-3, 3000.0, lo=False)
+    assert np.all(ai[:50] == 0)                                    # free surface: no layer on top
+
+
+def run(c, device, fd_order, **kw):
+    from geobrain_b200.wave import acoustic_forward_kernel
+    out = acoustic_forward_kernel(
+        nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+        free_surface=c["free_surface"], src_x=c["src_x"], src_z=c["src_z"], src_n=len(c["src_x"]),
+        src_v=torch.as_tensor(c["src_v"], device=device), rcv_x=c["rcv_x"], rcv_z=c["rcv_z"],
+        rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=device),
+        vp=torch.as_tensor(c["vp"], device=device), rho=torch.as_tensor(c["rho"], device=device), device=device,
+        fd_order=fd_order, **kw)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small_nofs", "small_fs"])
+@pytest.mark.parametrize("fd_order", [4, 8])
+def test_cuda_cpml_matches_oracle(cuda_device, name, fd_order):
+    c = load_case(name)
+    out = run(c, cuda_device, fd_order, absorbing="cpml")
+    kw = oracle_kwargs(c)
+    kw.pop("damp")
+    ref = ocp.forward(**kw, half=fd_order // 2)
+    for k in ("p", "vx", "vz", "forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vz"):
+        assert orc.rel_l2(out[k], ref[k]) < 1e-5, (k, orc.rel_l2(out[k], ref[k]))
+    # the damping path on the same plan is untouched
+    damped = run(c, cuda_device, fd_order)
+    assert orc.rel_l2(damped["p"], orc.forward(**oracle_kwargs(c), half=fd_order // 2, dtype=np.float64)["p"]) < 1e-5
+
+
+@pytest.mark.gpu
+def test_cuda_cpml_graph_replay_and_tilings_are_bit_identical(cuda_device):
+    from geobrain_b200.wave import engine
+    c = load_case("small_nofs")
+    geo = engine.Geometry(c["nz"], c["nx"], c["nabc"], c["nt"], c["dt"], c["dx"], 4, False)
+    plan = engine.get_plan(geo, c["src_x"], c["src_z"], c["rcv_x"], c["rcv_z"])
+    base = run(c, cuda_device, 8, absorbing="cpml")
+    try:
+        plan.set_graph_steps(0)
+        plan.set_tiling(16, 1)
+        other = run(c, cuda_device, 8, absorbing="cpml")
+    finally:
+        plan.set_graph_steps(16)
+        plan.set_tiling(16, 0)
+    for k in ("p", "vx", "vz"):
+        np.testing.assert_array_equal(other[k], base[k])
+
+
+@pytest.mark.gpu
+def test_cpml_reflects_less_than_the_damping_layers(cuda_device):
+    """A homogeneous model with a source near one edge: traces along a line
+    close to the edges, against the same model on a grid large enough that
+    nothing comes back within nt.  The CPML's edge reflections are a fraction
+    of the damping PML's at the same 20-cell width."""
+    from geobrain_b200.wave import RickerWavelet, bc_pml
+    nz, nx, nabc, nt, dx, dt = 80, 160, 20, 900, 10.0, 1e-3
+    w, _ = RickerWavelet()(f0=15.0, dt=dt)
+    w = np.pad(w.numpy(), (0, nt))[:nt].astype(np.float32)
+
+    def case(nz_, nx_, off):
+        vp = np.full((nz_, nx_), 2500.0, np.float32)
+        return dict(nz=nz_, nx=nx_, nabc=nabc, nt=nt, dx=dx, dt=dt, free_surface=False, vp=vp,
+                    rho=np.full_like(vp, 2000.0), src_x=np.array([20 + off]), src_z=np.array([40 + off]),
+                    src_v=w[None, :], rcv_x=np.arange(0, nx, 4) + off, rcv_z=np.full(nx // 4, 5 + off),
+                    damp=bc_pml(nx_, nz_, dx, dx, nabc, 2500.0, False).astype(np.float32))
+    small = case(nz, nx, 0)
+    big = case(nz + 2 * 400, nx + 2 * 400, 400)          # edges 400 cells away: no return within 0.9 s
+    ref = run(big, cuda_device, 8)["p"]
+    err_damp = orc.rel_l2(run(small, cuda_device, 8)["p"], ref)
+    err_cpml = orc.rel_l2(run(small, cuda_device, 8, absorbing="cpml")["p"], ref)
+    assert err_cpml < 0.5 * err_damp, (err_cpml, err_damp)
+
+
+@pytest.mark.gpu
+def test_cpml_is_forward_only(cuda_device):
+    from geobrain_b200.wave import acoustic_forward_kernel
+    c = load_case("small_nofs")
+    with pytest.raises(NotImplementedError):
+        acoustic_forward_kernel(
+            nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+            free_surface=False, src_x=c["src_x"], src_z=c["src_z"], src_n=3,
+            src_v=torch.as_tensor(c["src_v"], device=cuda_device), rcv_x=c["rcv_x"], rcv_z=c["rcv_z"],
+            rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=cuda_device),
+            vp=torch.tensor(c["vp"], device=cuda_device, requires_grad=True),
+            rho=torch.as_tensor(c["rho"], device=cuda_device), device=cuda_device, absorbing="cpml")
