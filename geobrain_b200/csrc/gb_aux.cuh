@@ -118,6 +118,28 @@ __global__ void unpack16_kernel(const H *__restrict__ in, const float *__restric
         o[i] = from_h(p[i]) * scale;
 }
 
+// Self-test of the bounded waits.  One CTA waits on an mbarrier of arrival
+// count 2.  The second arrival is made only when `complete` is set, so
+// otherwise the phase never completes: the wait gives up after max_polls
+// polls and the CTA sets the status word to the timeout code, as every step
+// kernel does when its TMA loads never land.  Nothing is in flight when it
+// returns.
+__global__ void bounded_wait_selftest_kernel(int *err, int complete, uint32_t max_polls)
+{
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 2);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_arrive(&bar);
+        if (complete) mbar_arrive(&bar);
+    }
+    __syncthreads();
+    if (!__syncthreads_and(mbar_wait_bounded(&bar, 0, max_polls)) && threadIdx.x == 0) atomicExch(err, -4);
+}
+
 // Step counter of graph-replayed forward chunks.
 __global__ void step_set_kernel(int *ctr, int value) { *ctr = value; }
 __global__ void step_advance_kernel(int *ctr, int by) { *ctr += by; }

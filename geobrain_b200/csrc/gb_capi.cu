@@ -1639,6 +1639,21 @@ int gb_workspace_status(const void *workspace, void *stream)
     return GB_OK;
 }
 
+int gb_selftest_bounded_wait(void *workspace, size_t workspace_bytes, int32_t complete, int32_t max_polls,
+                             void *stream)
+{
+    g_last_error.clear();
+    if (!workspace) return fail(GB_E_ARG, "null workspace");
+    char *ws = reinterpret_cast<char *>(align256(reinterpret_cast<uintptr_t>(workspace)));
+    if (ws + 4 > reinterpret_cast<char *>(workspace) + workspace_bytes) return fail(GB_E_WORKSPACE, "workspace too small");
+    if (max_polls < 1 || (uint32_t)max_polls > kMaxPolls) return fail(GB_E_ARG, "max_polls out of [1, 2^22]");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    GB_CUDA(cudaMemsetAsync(ws, 0, 4, st));
+    bounded_wait_selftest_kernel<<<1, 64, 0, st>>>(reinterpret_cast<int *>(ws), complete != 0, (uint32_t)max_polls);
+    GB_CUDA(cudaGetLastError());
+    return gb_workspace_status(workspace, stream);
+}
+
 int gb_plan_set_profiling(gb_plan *P, int enable)
 {
     if (!P) return fail(GB_E_ARG, "null plan");

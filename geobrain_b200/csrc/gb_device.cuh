@@ -79,6 +79,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t by
                  : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 {
     uint32_t ok;
@@ -94,9 +99,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 
 // Returns false (and the caller reports GB_E_TIMEOUT) if the phase never
 // completes.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t max_polls = kMaxPolls)
 {
-    for (uint32_t i = 0; i < kMaxPolls; ++i) {
+    for (uint32_t i = 0; i < max_polls; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
         if (i > 64) __nanosleep(256);
     }

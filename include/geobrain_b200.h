@@ -281,6 +281,17 @@ int gb_trace_misfit(const float *pred, const float *obs, int32_t n_shots, int32_
  * bounded wait inside a kernel gave up. */
 int gb_workspace_status(const void *workspace, void *stream);
 
+/* Failure-detection self-test of the bounded waits (no counterpart in the
+ * reference).  One CTA waits on an mbarrier that completes only if
+ * `complete` is nonzero.  Otherwise the wait gives up after max_polls polls
+ * (1 .. 2^22; the step kernels use 2^22) and sets the workspace status word, as a
+ * step kernel does when its loads never land.  Returns what
+ * gb_workspace_status then reads: GB_OK, or GB_E_TIMEOUT.  No GPU fault and
+ * no hang either way; the context stays usable.  Workspace: 4 bytes past
+ * the first 256-byte boundary (as every other workspace here). */
+int gb_selftest_bounded_wait(void *workspace, size_t workspace_bytes, int32_t complete, int32_t max_polls,
+                             void *stream);
+
 /* Forward modelling without any device allocation: the same computation and
  * outputs as gb_forward (no checkpoints), with the scratch held in a static
  * device array inside this library instead of a caller workspace.
