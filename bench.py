@@ -348,6 +348,7 @@ def main():
         extras.update(batch_rates(torch, wave, synthetic, dev))
         extras.update(large_gradient_rate(torch, wave, synthetic, dev))
         extras.update(rates_3d(torch, wave, dev))
+        extras.update(reference_gpu_rates(torch, wave, synthetic, dev))
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -408,6 +409,56 @@ def plain_forward_rates(torch, wave, synthetic, dev):
         out[name] = {"gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms,
                      "fd_order": w.fd_order, "nt": w.nt, "shots": w.n_shots, "absorbing": absorbing}
     return out
+
+
+def reference_gpu_rates(torch, wave, synthetic, dev, nt=100, segments=4):
+    """The reference's own PyTorch path on the B200, for comparison: its
+    acoustic_forward_kernel (geobrain/physics/wave/kernels/acoustic_2d.py
+    :294-501, installed unmodified under baseline/_ref) on the benchmark's
+    400 x 1200 grid, 30-cell PML and 32 shots at its only order (4), nt
+    truncated to 100 steps.  Forward without autograd, and the gradient of
+    0.5 ||p - d_obs||^2 by loss.backward() through its checkpointed step loop
+    (checkpoint_segments = 4, as examples/07 uses); one unit = one forward
+    plus one adjoint step of a (shot, padded cell), as for the headline."""
+    ref_dir = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref_dir, "geobrain")):
+        return {"reference_pytorch_gpu": {"unavailable": "the reference is not installed under baseline/_ref"}}
+    sys.path.insert(0, ref_dir)
+    try:
+        from geobrain.physics.wave.kernels import acoustic_forward_kernel as ref_kernel
+    finally:
+        sys.path.remove(ref_dir)
+    w = synthetic.fwi_400x1200(nt=nt)
+    S = w.n_shots
+    damp = torch.tensor(wave.bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp.max()), False),
+                        dtype=torch.float32, device=dev)
+    kw = dict(nx=w.nx, nz=w.nz, dx=w.dx, dz=w.dx, nt=nt, dt=w.dt, nabc=w.nabc, free_surface=False,
+              src_x=torch.tensor(w.src_x, dtype=torch.long, device=dev),
+              src_z=torch.tensor(w.src_z, dtype=torch.long, device=dev), src_n=S,
+              src_v=torch.tensor(np.tile(w.wavelet[:nt], (S, 1)), device=dev),
+              rcv_x=torch.tensor(w.rcv_x, dtype=torch.long, device=dev),
+              rcv_z=torch.tensor(w.rcv_z, dtype=torch.long, device=dev), rcv_n=int(w.rcv_x.size), damp=damp,
+              rho=torch.tensor(w.rho, device=dev), device=dev, dtype=torch.float32)
+    vp = torch.tensor(w.vp, device=dev)
+    units = S * (w.nz + 2 * w.nabc) * (w.nx + 2 * w.nabc) * nt
+    with torch.no_grad():
+        d_obs = ref_kernel(vp=vp * 1.02, **kw)["p"]
+
+    def fwd():
+        with torch.no_grad():
+            ref_kernel(vp=vp, **kw)
+
+    def grad():
+        v = vp.clone().requires_grad_(True)
+        r = ref_kernel(vp=v, checkpoint_segments=segments, **kw)["p"] - d_obs
+        (0.5 * (r * r).sum()).backward()
+
+    ms_f, ms_g = _timed(torch, fwd, 2), _timed(torch, grad, 1)
+    return {"reference_pytorch_gpu": {
+        "forward_gcell_updates_per_s": units / (ms_f * 1e-3) / 1e9, "forward_ms": ms_f,
+        "gradient_gcell_updates_per_s": units / (ms_g * 1e-3) / 1e9, "gradient_ms": ms_g,
+        "nt": nt, "shots": S, "fd_order": 4, "checkpoint_segments": segments,
+        "sample": "400x1200 grid, 30-cell PML, 32 shots, nt truncated to 100 (the reference has no 8th order)"}}
 
 
 def _model_kwargs(torch, wave, w, dev, vp=None):
