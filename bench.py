@@ -348,6 +348,7 @@ def main():
         extras.update(batch_rates(torch, wave, synthetic, dev))
         extras.update(large_gradient_rate(torch, wave, synthetic, dev))
         extras.update(rates_3d(torch, wave, dev))
+        extras.update(cpml_gradient_rate(torch, wave, synthetic, dev))
         extras.update(reference_gpu_rates(torch, wave, synthetic, dev))
 
     line = {
@@ -409,6 +410,31 @@ def plain_forward_rates(torch, wave, synthetic, dev):
         out[name] = {"gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms,
                      "fd_order": w.fd_order, "nt": w.nt, "shots": w.n_shots, "absorbing": absorbing}
     return out
+
+
+def cpml_gradient_rate(torch, wave, synthetic, dev, nt=1000):
+    """The CPML option's gradient through the public API: the 400 x 1200
+    grid, 32 shots, 8th order, nt truncated to 1000 steps (its adjoint reads
+    every step's fp24 imaging field: 56 GB here), loss 0.5 ||p - d_obs||^2."""
+    w = synthetic.fwi_400x1200(nt=nt)
+    kw = _model_kwargs(torch, wave, w, dev)
+    kw.pop("vp")
+    vp0 = torch.tensor(w.vp, device=dev)
+    common = dict(dx=w.dx, dz=w.dx, nt=w.nt, dt=w.dt, nabc=w.nabc, device=dev, fd_order=w.fd_order,
+                  absorbing="cpml", imaging_dtype="fp24")
+    kw = {k: v for k, v in kw.items() if k not in common}
+    with torch.no_grad():
+        d_obs = wave.acoustic_forward_kernel(vp=vp0 * 1.02, **kw, **common)["p"]
+
+    def grad():
+        v = vp0.clone().requires_grad_(True)
+        r = wave.acoustic_forward_kernel(vp=v, **kw, **common)["p"] - d_obs
+        (0.5 * (r * r).sum()).backward()
+
+    ms = _timed(torch, grad, 1)
+    return {"cpml_gradient_400x1200_32shots": {"gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9,
+                                               "ms": ms, "nt": nt, "shots": w.n_shots, "fd_order": w.fd_order,
+                                               "imaging": "fp24, every step"}}
 
 
 def reference_gpu_rates(torch, wave, synthetic, dev, nt=100, segments=4):

@@ -9,6 +9,7 @@
 #include "gb_stream.cuh"
 #include "gb_3d.cuh"
 #include "gb_fwd.cuh"
+#include "gb_cpml_adj.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -287,7 +288,7 @@ namespace {
 struct Layout {
     size_t err, coef, fields, energy, src, rcv_ptr, rcv_ent, tile_fast, amax, cpml, psi, total;
     // gradient only
-    size_t mu, img, g1, c1, g2, c2, arcv_ptr, arcv_ent;
+    size_t mu, img, g1, c1, g2, c2, arcv_ptr, arcv_ent, cprcv;
     int n_img;
 };
 
@@ -318,7 +319,8 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
     if (with_gradient > 0) {
         const size_t K = std::max(1, std::min(checkpoint_every, p->d.nt));
         const size_t G = p->n_groups;
-        L.mu = o; o = align256(o + 2 * S * 3 * p->plane * 4);
+        // adjoint state: p, vx, vz (and, with CPML, the four memory variables)
+        L.mu = o; o = align256(o + 2 * S * (p->cpml ? kCpmlFields : 3) * p->plane * 4);
         L.img = o; o = align256(o + K * L.n_img * S * p->plane * img_esize(img_fmt));
         L.g1 = o; o = align256(o + G * p->plane * 4);
         L.c1 = o; o = align256(o + G * p->plane * 4);
@@ -328,6 +330,9 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
         }
         L.arcv_ptr = o; o = align256(o + (p->n_tiles + 1) * 4);
         L.arcv_ent = o; o = align256(o + std::max<size_t>(p->arcv_ent.size(), 1) * 16);
+        if (p->cpml) {
+            L.cprcv = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 8);
+        }
     }
     L.total = o;
     return L;
@@ -747,6 +752,94 @@ int check_store(const gb_plan *P, const gb_grad_store *store)
     if (!img_format_ok(store->imaging_format))
         return fail(GB_E_ARG, "imaging_format must be GB_IMG_F32, GB_IMG_BF16 or GB_IMG_F24");
     if (store->cached_steps < P->d.nt && !store->checkpoints) return fail(GB_E_ARG, "checkpoint storage missing");
+    return GB_OK;
+}
+
+// Gradient of a CPML plan: the adjoint sweep of gb_cpml_adj.cuh over every
+// step, from imaging fields the forward kept for all nt steps (no recompute,
+// so no memory variables need checkpointing).
+int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *damp, const float *res_p,
+                  const float *res_vx, const float *res_vz, const gb_grad_store *store, float *grad_vp,
+                  float *grad_rho, void *workspace, size_t workspace_bytes, cudaStream_t st)
+{
+    const gb_model_desc &d = P->d;
+    if (store->cached_steps < d.nt)
+        return fail(GB_E_UNSUPPORTED, "CPML gradients need every step's imaging fields in the store (cached_steps = nt)");
+    const bool rho_fields = store->with_rho != 0;
+    const int ifmt = store->imaging_format;
+    const Layout L = layout(P, rho_fields ? 2 : 1, 1, ifmt);
+    char *ws = aligned_ws(workspace);
+    if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
+        return fail(GB_E_WORKSPACE, "workspace too small");
+    Setup Su;
+    if (int rc = common_setup(P, L, ws, vp, rho, damp, st, &Su)) return rc;
+    const int S = d.n_shots;
+    const size_t lam_fl = (size_t)S * kCpmlFields * P->plane;
+    float *lam[2] = {reinterpret_cast<float *>(ws + L.mu), reinterpret_cast<float *>(ws + L.mu) + lam_fl};
+    float *G1 = reinterpret_cast<float *>(ws + L.g1), *C1 = reinterpret_cast<float *>(ws + L.c1);
+    float *G2 = rho_fields ? reinterpret_cast<float *>(ws + L.g2) : nullptr;
+    float *C2 = rho_fields ? reinterpret_cast<float *>(ws + L.c2) : nullptr;
+    GB_CUDA(cudaMemsetAsync(lam[0], 0, 2 * lam_fl * 4, st));
+    GB_CUDA(cudaMemsetAsync(G1, 0, (size_t)P->n_groups * P->plane * 4, st));
+    GB_CUDA(cudaMemsetAsync(C1, 0, (size_t)P->n_groups * P->plane * 4, st));
+    if (G2) {
+        GB_CUDA(cudaMemsetAsync(G2, 0, (size_t)P->n_groups * P->plane * 4, st));
+        GB_CUDA(cudaMemsetAsync(C2, 0, (size_t)P->n_groups * P->plane * 4, st));
+    }
+    int2 *d_rcv = reinterpret_cast<int2 *>(ws + L.cprcv);
+    std::vector<int2> hr(d.n_rcv);
+    for (int r = 0; r < d.n_rcv; ++r) hr[r] = make_int2(P->rcv_z[r], P->rcv_x[r]);
+    // pageable host vector: cudaMemcpyAsync copies it before returning
+    if (d.n_rcv) GB_CUDA(cudaMemcpyAsync(d_rcv, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice, st));
+
+    const StepGeom g = P->geom();
+    CpmlAdjArgs A{};
+    A.g = g;
+    A.a1 = Su.a1;
+    A.a2 = Su.a2;
+    A.prof = Su.cpml;
+    A.img_field_stride = (long long)S * P->plane;
+    A.img_fmt = ifmt;
+    A.G1 = G1; A.C1 = C1; A.G2 = G2; A.C2 = C2;
+    const bool fs = d.free_surface != 0;
+    A.free_surface = fs;
+    const bool inject = d.n_rcv > 0 && (res_p || res_vx || res_vz);
+    const size_t step_img = (size_t)(rho_fields ? 3 : 1) * S * P->plane;
+    const dim3 block(128, 2), grid((P->Nx + 127) / 128, (P->Nz + 1) / 2);
+    const int fold_blocks = (int)std::min<long long>(1024, ((long long)S * P->Nx + 255) / 256);
+    P->mark(2, true, st);
+    P->phase_steps[2] += d.nt;
+    for (int it = d.nt - 1; it >= 0; --it) {
+        if (inject) {
+            cpml_inject_kernel<<<std::max(1, std::min(1024, (S * d.n_rcv + 255) / 256)), 256, 0, st>>>(
+                g, lam[0], d_rcv, res_p, res_vx, res_vz, it);
+            ++P->launches;
+        }
+        if (fs) {
+            cpml_fold_kernel<<<fold_blocks, 256, 0, st>>>(g, lam[0], 2, 1, 1.f);
+            ++P->launches;
+        }
+        A.img = img_at(store->imaging, (size_t)it * step_img, img_esize(ifmt));
+        A.lin = lam[0];
+        A.lout = lam[1];
+        if (P->R == 4) cpml_adj_v_kernel<4><<<grid, block, 0, st>>>(A);
+        else cpml_adj_v_kernel<2><<<grid, block, 0, st>>>(A);
+        if (fs) {
+            cpml_fold_kernel<<<fold_blocks, 256, 0, st>>>(g, lam[1], 0, 2, -1.f);
+            ++P->launches;
+        }
+        A.lin = lam[1];
+        A.lout = lam[0];
+        if (P->R == 4) cpml_adj_p_kernel<4><<<grid, block, 0, st>>>(A);
+        else cpml_adj_p_kernel<2><<<grid, block, 0, st>>>(A);
+        P->launches += 2;
+        GB_CUDA(cudaGetLastError());
+    }
+    P->mark(2, false, st);
+    grad_finish_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, G1, C1, G2, C2, P->n_groups, P->plane, d.nz, d.nx, d.nabc,
+                                                P->pitch, grad_vp, grad_rho);
+    GB_CUDA(cudaGetLastError());
+    ++P->launches;
     return GB_OK;
 }
 
@@ -1487,7 +1580,9 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     if (!P || !vp || !rho || !damp || !wavelet || !store || !grad_vp) return fail(GB_E_ARG, "null argument");
     if (int rc = check_store(P, store)) return rc;
     if (grad_rho && !store->with_rho) return fail(GB_E_ARG, "density gradient needs a store made with with_rho");
-    if (P->cpml) return fail(GB_E_UNSUPPORTED, "the CPML option has no adjoint: gradients need the damping layers");
+    if (P->cpml)
+        return backward_cpml(P, vp, rho, damp, res_p, res_vx, res_vz, store, grad_vp, grad_rho, workspace,
+                             workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
     const gb_model_desc &d = P->d;
     const int S = d.n_shots;
     const int K = std::min<int>(store->checkpoint_every, d.nt);

@@ -140,7 +140,8 @@ class Plan:
 
     def set_absorbing(self, mode: str = "damping", vmax: float = 0.0) -> None:
         """'damping' (the reference's damping PML) or 'cpml' (memory-variable
-        CPML with a profile for vmax; forward only)."""
+        CPML with a profile for vmax; its gradient needs every step's
+        imaging fields in the store)."""
         modes = {"damping": 0, "cpml": 1}
         if mode not in modes:
             raise ValueError(f"absorbing must be one of {sorted(modes)}, got {mode!r}")
@@ -244,7 +245,7 @@ def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device, imagi
                         checkpoint_every: int = 1, ckpt_fmt: str = "fp32", memory_budget: Optional[int] = None) -> int:
     """How many of the last time steps keep their imaging fields from the
     forward (those steps skip the recompute).  imaging_cache: a byte budget,
-    0, or 'auto': the most steps for which the cache, the checkpoints of the
+    0, 'all' (every step), or 'auto': the most steps for which the cache, the checkpoints of the
     remaining steps, the workspaces, the trace gradients and a margin (2 GiB
     + 5 %) fit in the device memory available right now, counting blocks the
     caching allocator holds unused (GEOBRAIN_B200_IMAGING_CACHE_BYTES
@@ -254,6 +255,8 @@ def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device, imagi
     per = max(plan.imaging_bytes(1, with_rho, imaging_fmt), 1)
     if imaging_cache in (None, 0, False):
         return 0
+    if imaging_cache == "all":
+        return nt
     if imaging_cache != "auto":
         return int(max(0, min(nt, int(imaging_cache) // per)))
     env = os.environ.get("GEOBRAIN_B200_IMAGING_CACHE_BYTES")

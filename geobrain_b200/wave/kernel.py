@@ -11,13 +11,14 @@ reference.
 
 Additions, all keyword-only with defaults that keep the reference's
 behaviour: fd_order (4 or 8); checkpoint_every, snapshot_dtype ('fp32',
-'bf16', 'fp16'), imaging_cache ('auto', a byte budget, or 0) and
+'bf16', 'fp16'), imaging_cache ('auto', 'all', a byte budget, or 0) and
 imaging_dtype ('fp32'; 'fp24', 3 bytes, gradient error about 1e-5; 'bf16',
 2 bytes, about 3e-3: more cached steps skip the recompute) for the
 gradient's memory, and memory_budget (bytes the gradient's store and
 workspaces may take, for the 'auto' cache); absorbing ('damping', the
 reference's PML driven by damp, or 'cpml': memory-variable convolutional
-PML layers, forward only, damp unused); want_energy (skip the energy
+PML layers, damp unused; its gradient keeps every step's imaging fields,
+imaging_cache='all'); want_energy (skip the energy
 sums); autotune (on the
 first call for a geometry, time the launch configurations and keep the
 fastest; GEOBRAIN_B200_AUTOTUNE=1 turns it on by default).
@@ -97,7 +98,10 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
                                                   getattr(rho, "requires_grad", False))
     if absorbing == "cpml":
         if needs_grad_now:
-            raise NotImplementedError("the CPML option is forward-only; gradients use absorbing='damping'")
+            # the CPML adjoint reads every step's imaging fields: no recompute
+            if imaging_cache not in ("auto", "all"):
+                raise ValueError("CPML gradients keep the imaging fields of every step (imaging_cache='all')")
+            imaging_cache = "all"
         vmax = float(vp.detach().max()) if torch.is_tensor(vp) else float(torch.as_tensor(vp).max())
         plan.set_absorbing("cpml", vmax)
     else:

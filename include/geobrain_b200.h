@@ -151,8 +151,10 @@ int gb_plan_set_streaming(gb_plan *plan, int enable, int seg_chunks);
  *   - every derivative g entering an update becomes g + psi, with
  *     psi' = b psi + a g (psi_px, psi_pz for p; psi_vx, psi_vz for the
  *     velocities), and the k damping terms are dropped.
- * Forward only (gb_backward and batched runs reject CPML plans); the
- * streaming kernel is not used with it. */
+ * Gradients: gb_backward runs the CPML adjoint, which reads every step's
+ * imaging fields from the store (cached_steps = nt; otherwise
+ * GB_E_UNSUPPORTED), so the memory variables need no checkpoints.  Batched
+ * runs reject CPML plans; the streaming kernel is not used with it. */
 #define GB_ABSORB_DAMPING 0
 #define GB_ABSORB_CPML    1
 int gb_plan_set_absorbing(gb_plan *plan, int mode, float vmax);

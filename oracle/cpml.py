@@ -11,7 +11,7 @@ d = d0 (depth / nabc)^2, d0 = -3 vmax ln(1e-6) / (2 nabc dx), on both sides
 (none above a free surface), b = exp(-d dt), a = b - 1, at integer and half
 points; every derivative g of an update becomes g + psi with
 psi' = b psi + a g; no damping terms.  Float64, whole-array operations, for
-small grids.
+small grids.  forward_torch restates it in torch for the gradient oracle.
 """
 from __future__ import annotations
 
@@ -98,3 +98,83 @@ def forward(*, nz, nx, dz, nt, dt, nabc, free_surface, src_x, src_z, src_v, rcv_
     out = dict(tr)
     out.update({f"forward_wavefield_{k}": v for k, v in en.items()})
     return out
+
+
+def forward_torch(*, nz, nx, dz, nt, dt, nabc, free_surface, src_x, src_z, src_v, rcv_x, rcv_z, vp, rho, half=4,
+                  vmax):
+    """The same scheme in float64 torch, written functionally (masks and
+    shifts, no in-place updates) so that autograd through it is the exact
+    discrete adjoint: the gradient oracle of the CPML option.  vp and rho are
+    (nz, nx) float64 tensors (they may require grad); vmax is a constant.
+    Returns the (S, nt, R) traces of p, vx and vz."""
+    import torch
+    import torch.nn.functional as F
+    R = half
+    cf = fd_coefficients(R)
+    Nz, Nx = nz + 2 * nabc, nx + 2 * nabc
+    fs = nabc if free_surface else 1
+    c = F.pad(vp[None, None], (nabc,) * 4, mode="replicate")[0, 0]
+    den = F.pad(rho[None, None], (nabc,) * 4, mode="replicate")[0, 0]
+    a1 = den * c * c * dt / dz
+    a2 = dt / (den * dz)
+    tt = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float64)
+    bzi, azi, bzh, azh = (tt(v)[:, None] for v in profiles(Nz, nabc, dz, dt, vmax, not free_surface))
+    bxi, axi, bxh, axh = (tt(v)[None, :] for v in profiles(Nx, nabc, dz, dt, vmax, True))
+
+    def box(r0, r1, c0, c1):
+        m = torch.zeros(Nz, Nx, dtype=torch.float64)
+        m[r0:r1 + 1, c0:c1 + 1] = 1.0
+        return m
+    Mp = box(max(fs + 1, R), Nz - 1 - R, R, Nx - 1 - R)
+    Mvx = box(fs, Nz - 2, R - 1, Nx - 1 - R)
+    Mvz = box(max(fs, R - 1), Nz - 1 - R, 1, Nx - 2)
+
+    def shift(f, di, dj):
+        """g[..., i, j] = f[..., i + di, j + dj], zero outside."""
+        P = R + 2
+        g = F.pad(f, (P, P, P, P))
+        return g[..., P + di:P + di + Nz, P + dj:P + dj + Nx]
+
+    S = len(src_x)
+    sx, sz = np.asarray(src_x) + nabc, np.asarray(src_z) + nabc
+    rx, rz = torch.as_tensor(np.asarray(rcv_x) + nabc), torch.as_tensor(np.asarray(rcv_z) + nabc)
+    onehot = torch.zeros(S, Nz, Nx, dtype=torch.float64)
+    onehot[torch.arange(S), torch.as_tensor(sz), torch.as_tensor(sx)] = 1.0
+    w = tt(src_v)
+    zero = torch.zeros(S, Nz, Nx, dtype=torch.float64)
+    p, vx, vz, ppx, ppz, pvx, pvz = (zero,) * 7
+    tr = {"p": [], "vx": [], "vz": []}
+    for it in range(nt):
+        Dx = sum(cf[k] * (shift(vx, 0, k) - shift(vx, 0, -1 - k)) for k in range(R))
+        Dz = sum(cf[k] * (shift(vz, k, 0) - shift(vz, -1 - k, 0)) for k in range(R))
+        ppx = Mp * (bxi * ppx + axi * Dx) + (1 - Mp) * ppx
+        ppz = Mp * (bzi * ppz + azi * Dz) + (1 - Mp) * ppz
+        p = p - Mp * a1 * ((Dx + ppx) + (Dz + ppz))
+        p = p + dt * w[:, it, None, None] * onehot
+        if free_surface:
+            p = torch.cat([p[:, :fs - 1], -p[:, fs + 1:fs + 2], p[:, fs:]], dim=1)
+        Gx = sum(cf[k] * (shift(p, 0, 1 + k) - shift(p, 0, -k)) for k in range(R))
+        pvx = Mvx * (bxh * pvx + axh * Gx) + (1 - Mvx) * pvx
+        vx = vx - Mvx * a2 * (Gx + pvx)
+        Gz = sum(cf[k] * (shift(p, 1 + k, 0) - shift(p, -k, 0)) for k in range(R))
+        pvz = Mvz * (bzh * pvz + azh * Gz) + (1 - Mvz) * pvz
+        vz = vz - Mvz * a2 * (Gz + pvz)
+        if free_surface:
+            vz = torch.cat([vz[:, :fs - 1], vz[:, fs:fs + 1], vz[:, fs:]], dim=1)
+        for k, f in (("p", p), ("vx", vx), ("vz", vz)):
+            tr[k].append(f[:, rz, rx])
+    return {k: torch.stack(v, dim=1) for k, v in tr.items()}
+
+
+def gradient(*, res_p=None, res_vx=None, res_vz=None, vp, rho, **kw):
+    """dL/dvp and dL/drho of L = sum(res_p * p) + sum(res_vx * vx) +
+    sum(res_vz * vz) over the traces, by float64 autograd through
+    forward_torch (res_* are (S, nt, R) weights, any may be None)."""
+    import torch
+    v = torch.tensor(np.asarray(vp, np.float64), requires_grad=True)
+    r = torch.tensor(np.asarray(rho, np.float64), requires_grad=True)
+    tr = forward_torch(vp=v, rho=r, **kw)
+    loss = sum((torch.as_tensor(np.asarray(w, np.float64)) * tr[k]).sum()
+               for k, w in (("p", res_p), ("vx", res_vx), ("vz", res_vz)) if w is not None)
+    loss.backward()
+    return v.grad.numpy(), r.grad.numpy()

@@ -106,15 +106,94 @@ def test_cpml_reflects_less_than_the_damping_layers(cuda_device):
     assert err_cpml < 0.5 * err_damp, (err_cpml, err_damp)
 
 
+def _okw(c):
+    kw = oracle_kwargs(c)
+    kw.pop("damp")
+    return kw
+
+
+@pytest.mark.parametrize("name", ["small_nofs", "small_fs"])
+@pytest.mark.parametrize("half", [2, 4])
+def test_torch_oracle_is_the_numpy_oracle(name, half):
+    """The functional torch restatement (the gradient oracle) computes the
+    same traces as the NumPy oracle."""
+    c = load_case(name)
+    kw = _okw(c)
+    vmax = float(np.max(c["vp"]))
+    a = ocp.forward(**kw, half=half)
+    kt = dict(kw, vp=torch.tensor(c["vp"], dtype=torch.float64), rho=torch.tensor(c["rho"], dtype=torch.float64))
+    b = ocp.forward_torch(**kt, half=half, vmax=vmax)
+    for k in ("p", "vx", "vz"):
+        assert orc.rel_l2(b[k].numpy(), a[k]) < 1e-12, k
+
+
+def test_torch_oracle_gradient_matches_central_differences():
+    """Autograd through the torch oracle against central differences of the
+    NumPy oracle along two random directions (float64; vmax held fixed, as
+    the layers are built once per plan)."""
+    c = load_case("small_fs")
+    kw = _okw(c)
+    vmax = float(np.max(c["vp"]))
+    lin = {k: c[f"lin_{k}"] for k in ("p", "vx", "vz")}
+    gvp, grho = ocp.gradient(res_p=lin["p"], res_vx=lin["vx"], res_vz=lin["vz"], half=4, vmax=vmax,
+                             **dict(kw, vp=c["vp"], rho=c["rho"]))
+    rng = np.random.default_rng(3)
+
+    def loss(vp, rho):
+        out = ocp.forward(**dict(kw, vp=vp, rho=rho), half=4, vmax=vmax)
+        return sum(float((lin[k] * out[k]).sum()) for k in ("p", "vx", "vz"))
+
+    for g, name in ((gvp, "vp"), (grho, "rho")):
+        d = rng.standard_normal(c["vp"].shape)
+        base = c[name].astype(np.float64)
+        eps = 5e-5 * float(np.abs(base).mean())   # truncation error ~ eps^2: 3e-7 relative here
+        args = lambda x: (x, c["rho"].astype(np.float64)) if name == "vp" else (c["vp"].astype(np.float64), x)
+        fd = (loss(*args(base + eps * d)) - loss(*args(base - eps * d))) / (2 * eps)
+        assert abs(fd - float((g * d).sum())) <= 2e-6 * abs(fd), (name, fd, float((g * d).sum()))
+
+
 @pytest.mark.gpu
-def test_cpml_is_forward_only(cuda_device):
+@pytest.mark.parametrize("name", ["small_nofs", "small_fs"])
+@pytest.mark.parametrize("fd_order", [4, 8])
+@pytest.mark.parametrize("imaging_dtype", ["fp32", "fp24"])
+def test_cuda_cpml_gradient_matches_oracle(cuda_device, name, fd_order, imaging_dtype):
+    """dL/dvp and dL/drho of a loss linear in all three traces: the CPML
+    adjoint (through the C ABI) against float64 autograd of the torch
+    oracle, 1e-4 relative L2."""
+    from geobrain_b200.wave import acoustic_forward_kernel
+    c = load_case(name)
+    S = len(c["src_x"])
+    vp = torch.tensor(c["vp"], device=cuda_device, requires_grad=True)
+    rho = torch.tensor(c["rho"], device=cuda_device, requires_grad=True)
+    out = acoustic_forward_kernel(
+        nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+        free_surface=c["free_surface"], src_x=c["src_x"], src_z=c["src_z"], src_n=S,
+        src_v=torch.as_tensor(c["src_v"], device=cuda_device), rcv_x=c["rcv_x"], rcv_z=c["rcv_z"],
+        rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=cuda_device), vp=vp, rho=rho,
+        device=cuda_device, fd_order=fd_order, absorbing="cpml", imaging_dtype=imaging_dtype)
+    lin = {k: c[f"lin_{k}"] for k in ("p", "vx", "vz")}
+    loss = sum((torch.as_tensor(lin[k], device=cuda_device, dtype=torch.float32) * out[k]).sum()
+               for k in ("p", "vx", "vz"))
+    loss.backward()
+    # the traces of a gradient run are the CPML forward's
+    ref_tr = ocp.forward(**_okw(c), half=fd_order // 2)
+    assert orc.rel_l2(out["p"].detach().cpu().numpy(), ref_tr["p"]) < 1e-5
+    rvp, rrho = ocp.gradient(res_p=lin["p"], res_vx=lin["vx"], res_vz=lin["vz"], half=fd_order // 2,
+                             vmax=float(np.max(c["vp"])), **dict(_okw(c), vp=c["vp"], rho=c["rho"]))
+    assert orc.rel_l2(vp.grad.cpu().numpy(), rvp) < 1e-4, orc.rel_l2(vp.grad.cpu().numpy(), rvp)
+    assert orc.rel_l2(rho.grad.cpu().numpy(), rrho) < 1e-4, orc.rel_l2(rho.grad.cpu().numpy(), rrho)
+
+
+@pytest.mark.gpu
+def test_cpml_gradient_needs_the_full_imaging_cache(cuda_device):
     from geobrain_b200.wave import acoustic_forward_kernel
     c = load_case("small_nofs")
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):
         acoustic_forward_kernel(
             nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
             free_surface=False, src_x=c["src_x"], src_z=c["src_z"], src_n=3,
             src_v=torch.as_tensor(c["src_v"], device=cuda_device), rcv_x=c["rcv_x"], rcv_z=c["rcv_z"],
             rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=cuda_device),
             vp=torch.tensor(c["vp"], device=cuda_device, requires_grad=True),
-            rho=torch.as_tensor(c["rho"], device=cuda_device), device=cuda_device, absorbing="cpml")
+            rho=torch.as_tensor(c["rho"], device=cuda_device), device=cuda_device, absorbing="cpml",
+            imaging_cache=0)
