@@ -288,7 +288,7 @@ namespace {
 struct Layout {
     size_t err, coef, fields, energy, src, rcv_ptr, rcv_ent, tile_fast, amax, cpml, psi, total;
     // gradient only
-    size_t mu, img, g1, c1, g2, c2, arcv_ptr, arcv_ent, cprcv;
+    size_t mu, img, g1, c1, g2, c2, arcv_ptr, arcv_ent, cprcv, cpcoef;
     int n_img;
 };
 
@@ -332,6 +332,7 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
         L.arcv_ent = o; o = align256(o + std::max<size_t>(p->arcv_ent.size(), 1) * 16);
         if (p->cpml) {
             L.cprcv = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 8);
+            L.cpcoef = o; o = align256(o + (size_t)kCpmlCoefPlanes * p->plane * 4);
         }
     }
     L.total = o;
@@ -793,11 +794,14 @@ int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *da
     if (d.n_rcv) GB_CUDA(cudaMemcpyAsync(d_rcv, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice, st));
 
     const StepGeom g = P->geom();
-    CpmlAdjArgs A{};
+    float *cpcoef = reinterpret_cast<float *>(ws + L.cpcoef);
+    cpml_adj_coef_kernel<<<4 * 148, 256, 0, st>>>(g, Su.a1, Su.a2, Su.cpml, cpcoef);
+    ++P->launches;
+    CpmlAdjArgs4 A{};
     A.g = g;
     A.a1 = Su.a1;
     A.a2 = Su.a2;
-    A.prof = Su.cpml;
+    A.cp = cpcoef;
     A.img_field_stride = (long long)S * P->plane;
     A.img_fmt = ifmt;
     A.G1 = G1; A.C1 = C1; A.G2 = G2; A.C2 = C2;
@@ -805,7 +809,7 @@ int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *da
     A.free_surface = fs;
     const bool inject = d.n_rcv > 0 && (res_p || res_vx || res_vz);
     const size_t step_img = (size_t)(rho_fields ? 3 : 1) * S * P->plane;
-    const dim3 block(128, 2), grid((P->Nx + 127) / 128, (P->Nz + 1) / 2);
+    const dim3 block(32, 4), grid((P->Nx + 127) / 128, (P->Nz + 3) / 4);
     const int fold_blocks = (int)std::min<long long>(1024, ((long long)S * P->Nx + 255) / 256);
     P->mark(2, true, st);
     P->phase_steps[2] += d.nt;

@@ -32,9 +32,9 @@
 // forward stores.  As in the damping adjoint, cells outside the update
 // masks never depend on the model, so their adjoint is dropped; the mirror
 // rows are folded instead.  G1 and G2 hold a1 dL/da1 and -a2 dL/da2, which
-// grad_finish_kernel turns into dL/dvp and dL/drho.  These are plain
-// gather kernels (one cell per thread, all shots, neighbours through L1):
-// the CPML gradient is an opt-in path, written for clarity.
+// grad_finish_kernel turns into dL/dvp and dL/drho.  The kernels gather
+// (4 adjacent cells per thread, all shots, neighbours through L1) with the
+// masks folded into coefficient planes built once per gradient.
 #pragma once
 
 #include "gb_adj.cuh"
@@ -42,19 +42,6 @@
 namespace gb {
 
 constexpr int kCpmlFields = 7;
-
-struct CpmlAdjArgs {
-    StepGeom g;
-    const float *a1, *a2;
-    const float *prof;          // [bz, az, bzh, azh][Nz] then [bx, ax, bxh, axh][pitch]
-    const float *lin;           // [S][7][plane]
-    float *lout;
-    const float *img;           // this step's I [S][plane], then Jx, Jz at img_field_stride
-    long long img_field_stride;
-    int img_fmt;
-    float *G1, *C1, *G2, *C2;   // one [plane] each (group 0 of the gradient planes)
-    int free_surface;
-};
 
 __device__ __forceinline__ bool cp_in_p(const StepGeom &g, int z, int x)
 {
@@ -67,13 +54,6 @@ __device__ __forceinline__ bool cp_in_vx(const StepGeom &g, int z, int x)
 __device__ __forceinline__ bool cp_in_vz(const StepGeom &g, int z, int x)
 {
     return z >= g.vz_r0 && z <= g.vz_r1 && x >= g.vz_c0 && x <= g.vz_c1;
-}
-
-// one imaging value at element offset o
-__device__ __forceinline__ float cp_img(const float *base, long long o, int fmt)
-{
-    const float4 v = decode_img4(load_img_raw(base, o & ~3LL, fmt), fmt);
-    return at(v, (int)(o & 3));
 }
 
 // adjoint receiver injection: lam[field][receiver cell] += res[s][it][r]
@@ -105,141 +85,234 @@ __global__ void cpml_fold_kernel(const StepGeom g, float *lam, int field, int to
     }
 }
 
-// block (128, 2): one cell per thread, looping over the shots, so each cell
-// of the gradient planes has one owner
+// Coefficient planes of the two adjoint kernels, with the update masks
+// folded in (zero off the mask), built once per gradient:
+//   [0] WX = M_vx a2 bxh  [1] AX = M_vx axh  [2] BX = M_vx bxh
+//   [3] WZ = M_vz a2 bzh  [4] AZ = M_vz azh  [5] BZ = M_vz bzh
+//   [6] UX = M_p a1 bx    [7] PX = M_p ax    [8] QX = M_p bx
+//   [9] UZ = M_p a1 bz    [10] PZ = M_p az   [11] QZ = M_p bz
+constexpr int kCpmlCoefPlanes = 12;
+
+__global__ void cpml_adj_coef_kernel(const StepGeom g, const float *a1, const float *a2, const float *prof,
+                                     float *cp)
+{
+    const float *bz = prof, *az = prof + g.Nz, *bzh = prof + 2 * g.Nz, *azh = prof + 3 * g.Nz;
+    const float *bx = prof + 4 * g.Nz, *ax = bx + g.pitch, *bxh = bx + 2 * g.pitch, *axh = bx + 3 * g.pitch;
+    for (long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x; o < g.plane; o += (long long)gridDim.x * blockDim.x) {
+        const int z = (int)(o / g.pitch), x = (int)(o % g.pitch);
+        const bool mvx = x < g.Nx && cp_in_vx(g, z, x), mvz = x < g.Nx && cp_in_vz(g, z, x);
+        const bool mp = x < g.Nx && cp_in_p(g, z, x);
+        const float v[kCpmlCoefPlanes] = {
+            mvx ? a2[o] * bxh[x] : 0.f, mvx ? axh[x] : 0.f, mvx ? bxh[x] : 0.f,
+            mvz ? a2[o] * bzh[z] : 0.f, mvz ? azh[z] : 0.f, mvz ? bzh[z] : 0.f,
+            mp ? a1[o] * bx[x] : 0.f,   mp ? ax[x] : 0.f,   mp ? bx[x] : 0.f,
+            mp ? a1[o] * bz[z] : 0.f,   mp ? az[z] : 0.f,   mp ? bz[z] : 0.f};
+#pragma unroll
+        for (int i = 0; i < kCpmlCoefPlanes; ++i) cp[i * g.plane + o] = v[i];
+    }
+}
+
+// Ask L2 for the next shot's 7 fields of this thread's cells while the
+// current shot computes (the loads of one shot alone leave DRAM idle
+// between shots at 12-16 resident warps per SM).
+__device__ __forceinline__ void cp_prefetch_shot(const float *L, long long P, long long o)
+{
+#pragma unroll
+    for (int f = 0; f < kCpmlFields; ++f) asm volatile("prefetch.global.L2 [%0];" ::"l"(L + f * P + o));
+}
+
+struct CpmlAdjArgs4 {
+    StepGeom g;
+    const float *a1, *a2;
+    const float *cp;            // the kCpmlCoefPlanes planes
+    const float *lin;           // [S][7][plane]
+    float *lout;
+    const float *img;           // this step's I [S][plane], then Jx, Jz at img_field_stride
+    long long img_field_stride;
+    int img_fmt;
+    float *G1, *C1, *G2, *C2;   // one [plane] each (group 0 of the gradient planes)
+    int free_surface;
+};
+
+__device__ __forceinline__ float4 cp_ld4(const float *base, long long o, bool ok)
+{
+    return ok ? __ldg(reinterpret_cast<const float4 *>(base + o)) : zero4();
+}
+__device__ __forceinline__ float4 fms4(const float4 &a, const float4 &x, const float4 &b, const float4 &y)
+{
+    // a x - b y per lane
+    return make_float4(a.x * x.x - b.x * y.x, a.y * x.y - b.y * y.y, a.z * x.z - b.z * y.z, a.w * x.w - b.w * y.w);
+}
+
+// block (32, 4): 4 adjacent cells of one row per thread, looping over the
+// shots, so each cell of the gradient planes has one owner
 template <int R>
-__global__ void __launch_bounds__(256) cpml_adj_v_kernel(const CpmlAdjArgs A)
+__global__ void __launch_bounds__(128) cpml_adj_v_kernel(const CpmlAdjArgs4 A)
 {
     const StepGeom &g = A.g;
-    const int x = blockIdx.x * 128 + threadIdx.x;
-    const int z = blockIdx.y * 2 + threadIdx.y;
-    if (x >= g.Nx || z >= g.Nz) return;
-    const long long o = (long long)z * g.pitch + x;
-    const float *bzh = A.prof + 2 * g.Nz, *azh = A.prof + 3 * g.Nz;
-    const float *bxh = A.prof + 4 * g.Nz + 2 * g.pitch, *axh = A.prof + 4 * g.Nz + 3 * g.pitch;
-    // lam_p is kept on the p mask and on the mirror row (folded next)
-    const bool mp = cp_in_p(g, z, x) || (A.free_surface && z == g.fs - 1);
-    const bool mvx = cp_in_vx(g, z, x), mvz = cp_in_vz(g, z, x);
-    const float a2 = A.a2[o];
-    float g2 = 0.f, c2 = 0.f;
+    const int x0 = 4 * (blockIdx.x * 32 + threadIdx.x);
+    const int z = blockIdx.y * 4 + threadIdx.y;
+    if (x0 >= g.Nx || z >= g.Nz) return;
+    const long long P = g.plane, o = (long long)z * g.pitch + x0;
+    const float *WX = A.cp, *AX = A.cp + P, *BX = A.cp + 2 * P, *WZ = A.cp + 3 * P, *AZ = A.cp + 4 * P,
+                *BZ = A.cp + 5 * P;
+    const bool lok = x0 >= 4, rok = x0 + 4 < g.pitch;
+    // the x taps' coefficients, the same for every shot
+    const float4 wxl = cp_ld4(WX, o - 4, lok), wxc = cp_ld4(WX, o, true), wxr = cp_ld4(WX, o + 4, rok);
+    const float4 axl = cp_ld4(AX, o - 4, lok), axc = cp_ld4(AX, o, true), axr = cp_ld4(AX, o + 4, rok);
+    const float4 bxc = cp_ld4(BX, o, true), wzc = cp_ld4(WZ, o, true), bzc = cp_ld4(BZ, o, true);
+    const float4 a2 = cp_ld4(A.a2, o, true);
+    bool mp[4], mvx[4], mvz[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int x = x0 + q;
+        mp[q] = x < g.Nx && (cp_in_p(g, z, x) || (A.free_surface && z == g.fs - 1));   // mirror row: folded next
+        mvx[q] = x < g.Nx && cp_in_vx(g, z, x);
+        mvz[q] = x < g.Nx && cp_in_vz(g, z, x);
+    }
+    float g2[4] = {0.f, 0.f, 0.f, 0.f}, c2[4] = {0.f, 0.f, 0.f, 0.f};
     for (int s = 0; s < g.n_shots; ++s) {
-        const float *L = A.lin + (long long)s * kCpmlFields * g.plane;
-        float *O = A.lout + (long long)s * kCpmlFields * g.plane;
-        const float *Lvx = L + g.plane, *Lvz = L + 2 * g.plane, *Lsvx = L + 5 * g.plane, *Lsvz = L + 6 * g.plane;
-        float lp = 0.f;
-        if (mp) {
+        const float *L = A.lin + (long long)s * kCpmlFields * P;
+        float *O = A.lout + (long long)s * kCpmlFields * P;
+        const float *Lvx = L + P, *Lvz = L + 2 * P, *Lsvx = L + 5 * P, *Lsvz = L + 6 * P;
+        if (s + 1 < g.n_shots) cp_prefetch_shot(L + kCpmlFields * P, P, o);
+        // wx = AX lam_psi_vx - WX lam_vx at x0-4 .. x0+7
+        float wx[12];
+        {
+            const float4 l = fms4(axl, cp_ld4(Lsvx, o - 4, lok), wxl, cp_ld4(Lvx, o - 4, lok));
+            const float4 c = fms4(axc, cp_ld4(Lsvx, o, true), wxc, cp_ld4(Lvx, o, true));
+            const float4 r = fms4(axr, cp_ld4(Lsvx, o + 4, rok), wxr, cp_ld4(Lvx, o + 4, rok));
+            const float t[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
+#pragma unroll
+            for (int i = 0; i < 12; ++i) wx[i] = t[i];
+        }
+        // wz = AZ lam_psi_vz - WZ lam_vz on rows z-R .. z+R-1
+        float4 wz[2 * R];
+#pragma unroll
+        for (int t = 0; t < 2 * R; ++t) {
+            const int zr = z - R + t;
+            const bool ok = zr >= 0 && zr < g.Nz;
+            const long long q = o + (long long)(t - R) * g.pitch;
+            wz[t] = ok ? fms4(cp_ld4(AZ, q, true), cp_ld4(Lsvz, q, true), cp_ld4(WZ, q, true), cp_ld4(Lvz, q, true))
+                       : zero4();
+        }
+        const float4 lp = cp_ld4(L, o, true), lvx = cp_ld4(Lvx, o, true), lvz = cp_ld4(Lvz, o, true);
+        const float4 lsvx = cp_ld4(Lsvx, o, true), lsvz = cp_ld4(Lsvz, o, true);
+        float4 op, ovx, ovz;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
             float t = 0.f;
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                float wm = 0.f, wp = 0.f, zm = 0.f, zp = 0.f;
-                const int jm = x - 1 - k, jp = x + k, im = z - 1 - k, ip = z + k;
-                if (cp_in_vx(g, z, jm)) {
-                    const long long q = (long long)z * g.pitch + jm;
-                    wm = axh[jm] * Lsvx[q] - A.a2[q] * bxh[jm] * Lvx[q];
-                }
-                if (cp_in_vx(g, z, jp)) {
-                    const long long q = (long long)z * g.pitch + jp;
-                    wp = axh[jp] * Lsvx[q] - A.a2[q] * bxh[jp] * Lvx[q];
-                }
-                if (cp_in_vz(g, im, x)) {
-                    const long long q = (long long)im * g.pitch + x;
-                    zm = azh[im] * Lsvz[q] - A.a2[q] * bzh[im] * Lvz[q];
-                }
-                if (cp_in_vz(g, ip, x)) {
-                    const long long q = (long long)ip * g.pitch + x;
-                    zp = azh[ip] * Lsvz[q] - A.a2[q] * bzh[ip] * Lvz[q];
-                }
-                t += g.c[k] * ((wm - wp) + (zm - zp));
-            }
-            lp = L[o] + t;
+            for (int k = 0; k < R; ++k)
+                t += g.c[k] * ((wx[q + 3 - k] - wx[q + 4 + k]) + (at(wz[R - 1 - k], q) - at(wz[R + k], q)));
+            at(op, q) = mp[q] ? at(lp, q) + t : 0.f;
+            at(ovx, q) = mvx[q] ? at(lvx, q) : 0.f;
+            at(ovz, q) = mvz[q] ? at(lvz, q) : 0.f;
         }
-        const float lvx = mvx ? Lvx[o] : 0.f, lvz = mvz ? Lvz[o] : 0.f;
-        O[o] = lp;
-        O[g.plane + o] = lvx;
-        O[2 * g.plane + o] = lvz;
-        O[3 * g.plane + o] = L[3 * g.plane + o];
-        O[4 * g.plane + o] = L[4 * g.plane + o];
-        O[5 * g.plane + o] = mvx ? bxh[x] * Lsvx[o] - a2 * bxh[x] * lvx : 0.f;
-        O[6 * g.plane + o] = mvz ? bzh[z] * Lsvz[o] - a2 * bzh[z] * lvz : 0.f;
-        if (A.G2 && (mvx || mvz)) {
-            const long long io = (long long)s * g.plane + o;
-            const float jx = mvx ? cp_img(A.img, A.img_field_stride + io, A.img_fmt) : 0.f;
-            const float jz = mvz ? cp_img(A.img, 2 * A.img_field_stride + io, A.img_fmt) : 0.f;
-            neumaier_add(g2, c2, a2 * (lvx * jx + lvz * jz));
+        stg4(O + o, op);
+        stg4(O + P + o, ovx);
+        stg4(O + 2 * P + o, ovz);
+        stg4(O + 3 * P + o, cp_ld4(L + 3 * P, o, true));
+        stg4(O + 4 * P + o, cp_ld4(L + 4 * P, o, true));
+        stg4(O + 5 * P + o, fms4(bxc, lsvx, wxc, lvx));
+        stg4(O + 6 * P + o, fms4(bzc, lsvz, wzc, lvz));
+        if (A.G2) {
+            const long long io = (long long)s * P + o;
+            const float4 jx = decode_img4(load_img_raw(A.img, A.img_field_stride + io, A.img_fmt), A.img_fmt);
+            const float4 jz = decode_img4(load_img_raw(A.img, 2 * A.img_field_stride + io, A.img_fmt), A.img_fmt);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                neumaier_add(g2[q], c2[q], at(a2, q) * ((mvx[q] ? at(ovx, q) * at(jx, q) : 0.f) +
+                                                        (mvz[q] ? at(ovz, q) * at(jz, q) : 0.f)));
         }
     }
-    if (A.G2) neumaier_add(A.G2[o], A.C2[o], g2 + c2);
+    if (A.G2) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (x0 + q < g.Nx) neumaier_add(A.G2[o + q], A.C2[o + q], g2[q] + c2[q]);
+    }
 }
 
 template <int R>
-__global__ void __launch_bounds__(256) cpml_adj_p_kernel(const CpmlAdjArgs A)
+__global__ void __launch_bounds__(128) cpml_adj_p_kernel(const CpmlAdjArgs4 A)
 {
     const StepGeom &g = A.g;
-    const int x = blockIdx.x * 128 + threadIdx.x;
-    const int z = blockIdx.y * 2 + threadIdx.y;
-    if (x >= g.Nx || z >= g.Nz) return;
-    const long long o = (long long)z * g.pitch + x;
-    const float *bz = A.prof, *az = A.prof + g.Nz;
-    const float *bx = A.prof + 4 * g.Nz, *ax = A.prof + 4 * g.Nz + g.pitch;
-    // lam_vz is kept on the vz mask and on the mirror row: the p update read
-    // vz[fs-1], which the previous step's mirror set (folded next step)
-    const bool mp = cp_in_p(g, z, x), mvx = cp_in_vx(g, z, x);
-    const bool mvz = cp_in_vz(g, z, x) || (A.free_surface && z == g.fs - 1);
-    const float a1 = A.a1[o];
-    float g1 = 0.f, c1 = 0.f;
-    for (int s = 0; s < g.n_shots; ++s) {
-        const float *L = A.lin + (long long)s * kCpmlFields * g.plane;
-        float *O = A.lout + (long long)s * kCpmlFields * g.plane;
-        const float *Lp = L, *Lspx = L + 3 * g.plane, *Lspz = L + 4 * g.plane;
-        const float lp = mp ? Lp[o] : 0.f;
-        float lvx = 0.f, lvz = 0.f;
-        if (mvx) {
-            // Dx^T: sum_k c_k (ux[x-k] - ux[x+1+k]),  ux[j] = M_p (ax lam_psi_px - a1 bx lam_p)
-            float t = 0.f;
+    const int x0 = 4 * (blockIdx.x * 32 + threadIdx.x);
+    const int z = blockIdx.y * 4 + threadIdx.y;
+    if (x0 >= g.Nx || z >= g.Nz) return;
+    const long long P = g.plane, o = (long long)z * g.pitch + x0;
+    const float *UX = A.cp + 6 * P, *PX = A.cp + 7 * P, *QX = A.cp + 8 * P, *UZ = A.cp + 9 * P,
+                *PZ = A.cp + 10 * P, *QZ = A.cp + 11 * P;
+    const bool lok = x0 >= 4, rok = x0 + 4 < g.pitch;
+    const float4 uxl = cp_ld4(UX, o - 4, lok), uxc = cp_ld4(UX, o, true), uxr = cp_ld4(UX, o + 4, rok);
+    const float4 pxl = cp_ld4(PX, o - 4, lok), pxc = cp_ld4(PX, o, true), pxr = cp_ld4(PX, o + 4, rok);
+    const float4 qxc = cp_ld4(QX, o, true), uzc = cp_ld4(UZ, o, true), qzc = cp_ld4(QZ, o, true);
+    const float4 a1 = cp_ld4(A.a1, o, true);
+    bool mp[4], mvx[4], mvz[4];
 #pragma unroll
-            for (int k = 0; k < R; ++k) {
-                float um = 0.f, up = 0.f;
-                const int jm = x - k, jp = x + 1 + k;
-                if (cp_in_p(g, z, jm)) {
-                    const long long q = (long long)z * g.pitch + jm;
-                    um = ax[jm] * Lspx[q] - A.a1[q] * bx[jm] * Lp[q];
-                }
-                if (cp_in_p(g, z, jp)) {
-                    const long long q = (long long)z * g.pitch + jp;
-                    up = ax[jp] * Lspx[q] - A.a1[q] * bx[jp] * Lp[q];
-                }
-                t += g.c[k] * (um - up);
-            }
-            lvx = L[g.plane + o] + t;
-        }
-        if (mvz) {
-            float t = 0.f;
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-                float um = 0.f, up = 0.f;
-                const int im = z - k, ip = z + 1 + k;
-                if (cp_in_p(g, im, x)) {
-                    const long long q = (long long)im * g.pitch + x;
-                    um = az[im] * Lspz[q] - A.a1[q] * bz[im] * Lp[q];
-                }
-                if (cp_in_p(g, ip, x)) {
-                    const long long q = (long long)ip * g.pitch + x;
-                    up = az[ip] * Lspz[q] - A.a1[q] * bz[ip] * Lp[q];
-                }
-                t += g.c[k] * (um - up);
-            }
-            lvz = L[2 * g.plane + o] + t;
-        }
-        O[o] = lp;
-        O[g.plane + o] = lvx;
-        O[2 * g.plane + o] = lvz;
-        O[3 * g.plane + o] = mp ? bx[x] * Lspx[o] - a1 * bx[x] * lp : 0.f;
-        O[4 * g.plane + o] = mp ? bz[z] * Lspz[o] - a1 * bz[z] * lp : 0.f;
-        O[5 * g.plane + o] = L[5 * g.plane + o];
-        O[6 * g.plane + o] = L[6 * g.plane + o];
-        if (mp) neumaier_add(g1, c1, a1 * lp * cp_img(A.img, (long long)s * g.plane + o, A.img_fmt));
+    for (int q = 0; q < 4; ++q) {
+        const int x = x0 + q;
+        mp[q] = x < g.Nx && cp_in_p(g, z, x);
+        mvx[q] = x < g.Nx && cp_in_vx(g, z, x);
+        // the p update read vz[fs-1], which the previous step's mirror set (folded next step)
+        mvz[q] = x < g.Nx && (cp_in_vz(g, z, x) || (A.free_surface && z == g.fs - 1));
     }
-    neumaier_add(A.G1[o], A.C1[o], g1 + c1);
+    float g1[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int s = 0; s < g.n_shots; ++s) {
+        const float *L = A.lin + (long long)s * kCpmlFields * P;
+        float *O = A.lout + (long long)s * kCpmlFields * P;
+        const float *Lspx = L + 3 * P, *Lspz = L + 4 * P;
+        if (s + 1 < g.n_shots) cp_prefetch_shot(L + kCpmlFields * P, P, o);
+        // ux = PX lam_psi_px - UX lam_p at x0-4 .. x0+7
+        float ux[12];
+        {
+            const float4 l = fms4(pxl, cp_ld4(Lspx, o - 4, lok), uxl, cp_ld4(L, o - 4, lok));
+            const float4 c = fms4(pxc, cp_ld4(Lspx, o, true), uxc, cp_ld4(L, o, true));
+            const float4 r = fms4(pxr, cp_ld4(Lspx, o + 4, rok), uxr, cp_ld4(L, o + 4, rok));
+            const float t[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
+#pragma unroll
+            for (int i = 0; i < 12; ++i) ux[i] = t[i];
+        }
+        // uz = PZ lam_psi_pz - UZ lam_p on rows z-R+1 .. z+R
+        float4 uz[2 * R];
+#pragma unroll
+        for (int t = 0; t < 2 * R; ++t) {
+            const int zr = z - R + 1 + t;
+            const bool ok = zr >= 0 && zr < g.Nz;
+            const long long q = o + (long long)(t - R + 1) * g.pitch;
+            uz[t] = ok ? fms4(cp_ld4(PZ, q, true), cp_ld4(Lspz, q, true), cp_ld4(UZ, q, true), cp_ld4(L, q, true))
+                       : zero4();
+        }
+        const float4 lp = cp_ld4(L, o, true), lvx = cp_ld4(L + P, o, true), lvz = cp_ld4(L + 2 * P, o, true);
+        const float4 lspx = cp_ld4(Lspx, o, true), lspz = cp_ld4(Lspz, o, true);
+        float4 op, ovx, ovz;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float tx = 0.f, tz = 0.f;
+#pragma unroll
+            for (int k = 0; k < R; ++k) {
+                tx += g.c[k] * (ux[q + 4 - k] - ux[q + 5 + k]);
+                tz += g.c[k] * (at(uz[R - 1 - k], q) - at(uz[R + k], q));
+            }
+            at(op, q) = mp[q] ? at(lp, q) : 0.f;
+            at(ovx, q) = mvx[q] ? at(lvx, q) + tx : 0.f;
+            at(ovz, q) = mvz[q] ? at(lvz, q) + tz : 0.f;
+        }
+        stg4(O + o, op);
+        stg4(O + P + o, ovx);
+        stg4(O + 2 * P + o, ovz);
+        stg4(O + 3 * P + o, fms4(qxc, lspx, uxc, lp));
+        stg4(O + 4 * P + o, fms4(qzc, lspz, uzc, lp));
+        stg4(O + 5 * P + o, cp_ld4(L + 5 * P, o, true));
+        stg4(O + 6 * P + o, cp_ld4(L + 6 * P, o, true));
+        const float4 im = decode_img4(load_img_raw(A.img, (long long)s * P + o, A.img_fmt), A.img_fmt);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (mp[q]) neumaier_add(g1[q], c1[q], at(a1, q) * at(op, q) * at(im, q));
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        if (x0 + q < g.Nx) neumaier_add(A.G1[o + q], A.C1[o + q], g1[q] + c1[q]);
 }
 
 }  // namespace gb
