@@ -70,3 +70,24 @@ def test_static_scratch_rejects_models_beyond_its_size(cuda_device):
                                        None, None, None, None, 0, None, torch.cuda.current_stream().cuda_stream)
     assert rc == -3
     assert b"static scratch" in lib.gb_last_error()
+
+
+@pytest.mark.parametrize("name,fd_order", [("small_nofs", 8), ("small_fs", 4)])
+def test_static_scratch_with_cpml_layers(cuda_device, name, fd_order):
+    """A CPML plan (its memory variables live in the same scratch) through
+    the no-alloc entry point: the same outputs as the workspace forward, on
+    two calls in a row (the memory variables restart from zero each call)."""
+    from geobrain_b200.wave import engine
+    c = load_case(name)
+    plan, t = _inputs(c, cuda_device, fd_order)
+    try:
+        plan.set_absorbing("cpml", float(c["vp"].max()))
+        ref = engine.run_forward(plan, t["vp"], t["rho"], t["damp"], t["src_v"], want_energy=True)
+        ref_tr = [x.cpu().numpy() for x in ref[:3]]
+        ref_en = [x.cpu().numpy() for x in ref[3]]
+        for _ in range(2):
+            tr, en = _static_call(plan, t, cuda_device)
+            for a, b in zip(tr + en, ref_tr + ref_en):
+                assert orc.rel_l2(a, b) < TOL
+    finally:
+        plan.set_absorbing("damping")
