@@ -574,7 +574,7 @@ def large_gradient_rate(torch, wave, synthetic, dev, cap_bytes=60 * 10**9):
 
 def rates_3d(torch, wave, dev, nz=200, ny=200, nx=200, shots=4, nt=200, nabc=20):
     """The 3-D path (acoustic_forward_kernel_3d, 4th order): forward and
-    gradient (forward + adjoint of 0.5 ||p||^2, checkpointed recompute) on a
+    gradient (forward + adjoint of 0.5 ||p||^2; every step's imaging fields kept) on a
     200^3 model with a 20-cell PML and 4 shots, seeded random velocities."""
     rng = np.random.default_rng(0)
     vp = torch.tensor((2000 + 1000 * rng.random((nz, ny, nx))).astype(np.float32), device=dev)

@@ -68,11 +68,12 @@ SIGNATURES = {
     "gb_trace_misfit": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P, _P, _P]),
     "gb3_workspace_bytes": (_SZ, [ctypes.POINTER(Desc3)]),
     "gb3_forward": (ctypes.c_int, [ctypes.POINTER(Desc3)] + [_P] * 6 + [_P] * 4 + [_P] * 8 + [_P, _I32] +
-                    [_P, _SZ, _P]),
+                    [_P, _I32] + [_P, _SZ, _P]),
+    "gb3_imaging_bytes": (_SZ, [ctypes.POINTER(Desc3), _I32]),
     "gb3_checkpoint_bytes": (_SZ, [ctypes.POINTER(Desc3), _I32]),
     "gb3_backward_workspace_bytes": (_SZ, [ctypes.POINTER(Desc3), _I32, _I32]),
     "gb3_backward": (ctypes.c_int, [ctypes.POINTER(Desc3)] + [_P] * 6 + [_P] * 4 + [_P] * 4 + [_P, _I32] +
-                     [_P, _P, _P, _SZ, _P]),
+                     [_P, _I32] + [_P, _P, _P, _SZ, _P]),
     "gb_plan_autotune_workspace_bytes": (_SZ, [_P]),
     "gb_plan_get_config": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),

@@ -1296,7 +1296,8 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
                 const int64_t *rcv_x, const int64_t *rcv_y, const int64_t *rcv_z, const float *vp, const float *rho,
                 const float *damp, const float *wavelet, float *trace_p, float *trace_vx, float *trace_vy,
                 float *trace_vz, float *energy_p, float *energy_vx, float *energy_vy, float *energy_vz,
-                float *checkpoints, int32_t checkpoint_every, void *workspace, size_t workspace_bytes, void *stream)
+                float *checkpoints, int32_t checkpoint_every, float *imaging, int32_t imaging_rho, void *workspace,
+                size_t workspace_bytes, void *stream)
 {
     g_last_error.clear();
     Geo3 g;
@@ -1337,7 +1338,12 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
     const bool fs = desc->free_surface != 0;
     const bool want_tr = g.n_rcv > 0 && (trace_p || trace_vx || trace_vy || trace_vz);
     const size_t state_bytes = (size_t)g.n_shots * 4 * g.vol * 4;
+    const size_t field = (size_t)g.n_shots * g.vol, blk = (imaging_rho ? 4 : 1) * field;
     for (int it = 0; it < g.nt; ++it) {
+        if (imaging) {   // this step's imaging fields, for a gradient without recompute
+            A.img_i = imaging + (size_t)it * blk;
+            A.img_j = imaging_rho ? A.img_i + field : nullptr;
+        }
         if (checkpoints && it % checkpoint_every == 0)   // the state before step it
             GB_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(checkpoints) + (size_t)(it / checkpoint_every) * state_bytes,
                                     state, state_bytes, cudaMemcpyDeviceToDevice, st));
@@ -1379,10 +1385,17 @@ Layout3B layout3b(const Geo3 &g, int K, bool rho)
 
 }  // namespace
 
+size_t gb3_imaging_bytes(const gb3_model_desc *desc, int32_t with_rho)
+{
+    Geo3 g;
+    if (!geo3_of(desc, &g)) return 0;
+    return (size_t)g.nt * (with_rho ? 4 : 1) * g.n_shots * g.vol * 4;
+}
+
 size_t gb3_backward_workspace_bytes(const gb3_model_desc *desc, int32_t checkpoint_every, int32_t with_rho)
 {
     Geo3 g;
-    if (!geo3_of(desc, &g) || checkpoint_every < 1) return 0;
+    if (!geo3_of(desc, &g) || checkpoint_every < 0) return 0;
     return layout3b(g, std::min<int>(checkpoint_every, g.nt), with_rho != 0).total + 256;
 }
 
@@ -1390,16 +1403,21 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
                  const int64_t *rcv_x, const int64_t *rcv_y, const int64_t *rcv_z, const float *vp, const float *rho,
                  const float *damp, const float *wavelet, const float *res_p, const float *res_vx,
                  const float *res_vy, const float *res_vz, const float *checkpoints, int32_t checkpoint_every,
-                 float *grad_vp, float *grad_rho, void *workspace, size_t workspace_bytes, void *stream)
+                 const float *imaging, int32_t imaging_rho, float *grad_vp, float *grad_rho, void *workspace,
+                 size_t workspace_bytes, void *stream)
 {
     g_last_error.clear();
     Geo3 g;
     if (!geo3_of(desc, &g)) return fail(GB_E_ARG, "invalid 3-D model description");
-    if (!vp || !rho || !damp || !wavelet || !checkpoints || !grad_vp) return fail(GB_E_ARG, "null argument");
-    if (checkpoint_every < 1) return fail(GB_E_ARG, "checkpoint_every must be >= 1");
+    if (!vp || !rho || !damp || !wavelet || !grad_vp || (!checkpoints && !imaging))
+        return fail(GB_E_ARG, "null argument");
+    if (!imaging && checkpoint_every < 1) return fail(GB_E_ARG, "checkpoint_every must be >= 1");
     if (g.Nz > 65535) return fail(GB_E_ARG, "at most 65535 padded z planes");
-    const int K = std::min<int>(checkpoint_every, g.nt);
     const bool with_rho = grad_rho != nullptr;
+    if (imaging && with_rho && !imaging_rho)
+        return fail(GB_E_ARG, "the density gradient needs imaging fields kept with imaging_rho");
+    // with every step's imaging fields there is no recompute and no segment buffer
+    const int K = imaging ? 0 : std::min<int>(checkpoint_every, g.nt);
     const Layout3B L = layout3b(g, K, with_rho);
     char *ws = aligned_ws(workspace);
     if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
@@ -1440,16 +1458,19 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
     A.G1 = G1; A.C1 = C1; A.G2 = G2; A.C2 = C2;
     const bool fs = desc->free_surface != 0;
     const dim3 block(32, 4), grid((g.Nx + 127) / 128, (g.Ny + 3) / 4, g.Nz);
-    const int n_seg = (g.nt + K - 1) / K;
+    const size_t blk = (imaging_rho ? 4 : 1) * field;      // one step of the caller's imaging buffer
+    const int n_seg = imaging ? 1 : (g.nt + K - 1) / K;
     for (int seg = n_seg - 1; seg >= 0; --seg) {
-        const int t0 = seg * K, t1 = std::min(g.nt, t0 + K);
-        // recompute the segment from its checkpoint, keeping the imaging fields
-        GB_CUDA(cudaMemcpyAsync(state, reinterpret_cast<const char *>(checkpoints) + (size_t)seg * state_bytes,
-                                state_bytes, cudaMemcpyDeviceToDevice, st));
-        for (int it = t0; it < t1; ++it) {
-            F.img_i = img_i + (size_t)(it - t0) * field;
-            F.img_j = with_rho ? img_j + (size_t)(it - t0) * 3 * field : nullptr;
-            if (int rc = step3(g, F, it, fs, st)) return rc;
+        const int t0 = imaging ? 0 : seg * K, t1 = imaging ? g.nt : std::min(g.nt, t0 + K);
+        if (!imaging) {
+            // recompute the segment from its checkpoint, keeping the imaging fields
+            GB_CUDA(cudaMemcpyAsync(state, reinterpret_cast<const char *>(checkpoints) + (size_t)seg * state_bytes,
+                                    state_bytes, cudaMemcpyDeviceToDevice, st));
+            for (int it = t0; it < t1; ++it) {
+                F.img_i = img_i + (size_t)(it - t0) * field;
+                F.img_j = with_rho ? img_j + (size_t)(it - t0) * 3 * field : nullptr;
+                if (int rc = step3(g, F, it, fs, st)) return rc;
+            }
         }
         // adjoint steps, last to first
         for (int it = t1 - 1; it >= t0; --it) {
@@ -1457,8 +1478,13 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
                 inj3_kernel<<<(g.n_shots * g.n_rcv + 255) / 256, 256, 0, st>>>(g, lam_a, d_rcv, res_p, res_vx,
                                                                               res_vy, res_vz, it);
             if (fs) fold3_kernel<<<148, 256, 0, st>>>(g, lam_a, 3, 1, 1.f);
-            A.img_i = img_i + (size_t)(it - t0) * field;
-            A.img_j = with_rho ? img_j + (size_t)(it - t0) * 3 * field : nullptr;
+            if (imaging) {
+                A.img_i = imaging + (size_t)it * blk;
+                A.img_j = with_rho ? imaging + (size_t)it * blk + field : nullptr;
+            } else {
+                A.img_i = img_i + (size_t)(it - t0) * field;
+                A.img_j = with_rho ? img_j + (size_t)(it - t0) * 3 * field : nullptr;
+            }
             A.lam_in = lam_a;
             A.lam_out = lam_b;
             adj_v3_kernel<<<grid, block, 0, st>>>(A);

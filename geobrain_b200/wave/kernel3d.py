@@ -7,9 +7,10 @@ array) and returns the same dict: traces p / vx / vy / vz (src_n, nt, rcv_n)
 and energy maps forward_wavefield_{p,vx,vy,vz} (nz, ny, nx).  The CUDA
 library (gb3_forward) computes them.  As in the reference, every derivative
 is scaled by 1/dz.  When vp or rho requires grad, the traces are
-differentiable: the forward keeps checkpoints and the backward runs the
-hand-written adjoint (gb3_backward) in place of autograd through the
-reference's time loop.
+differentiable: the forward keeps every step's imaging fields when they fit
+in the device memory (imaging_cache='auto'; no recompute), else checkpoints,
+and the backward runs the hand-written adjoint (gb3_backward) in place of
+autograd through the reference's time loop.
 """
 from __future__ import annotations
 
@@ -46,7 +47,7 @@ class _Run3:
             raise ValueError(self.L.gb_last_error().decode())
         _lib.check(rc)
 
-    def forward(self, vp, rho, ckpt=None, K=0):
+    def forward(self, vp, rho, ckpt=None, K=0, img=None, img_rho=False):
         d, dev = self.desc, self.device
         ws = engine.workspace(int(self.L.gb3_workspace_bytes(ctypes.byref(d))), dev)
         f32 = dict(device=dev, dtype=torch.float32)
@@ -56,13 +57,14 @@ class _Run3:
             rc = self.L.gb3_forward(ctypes.byref(d), *[p.ctypes.data for p in self.pos],
                                     *[p.ctypes.data for p in self.rpos], vp.data_ptr(), rho.data_ptr(),
                                     self.damp.data_ptr(), self.w.data_ptr(), *[t.data_ptr() for t in tr],
-                                    *[e.data_ptr() for e in en], _lib.ptr(ckpt), int(K), ws.data_ptr(), ws.numel(),
-                                    engine.stream_handle(dev))
+                                    *[e.data_ptr() for e in en], _lib.ptr(ckpt), int(K), _lib.ptr(img),
+                                    int(bool(img_rho)), ws.data_ptr(), ws.numel(), engine.stream_handle(dev))
         self.check(rc)
         return tr, en
 
-    def backward(self, vp, rho, res, ckpt, K, want_rho):
+    def backward(self, vp, rho, res, ckpt, K, want_rho, img=None, img_rho=False):
         d, dev = self.desc, self.device
+        K = 0 if img is not None else K
         ws = engine.workspace(int(self.L.gb3_backward_workspace_bytes(ctypes.byref(d), int(K), int(want_rho))), dev)
         gvp = torch.empty((d.nz, d.ny, d.nx), device=dev, dtype=torch.float32)
         grho = torch.empty_like(gvp) if want_rho else None
@@ -70,25 +72,42 @@ class _Run3:
             rc = self.L.gb3_backward(ctypes.byref(d), *[p.ctypes.data for p in self.pos],
                                      *[p.ctypes.data for p in self.rpos], vp.data_ptr(), rho.data_ptr(),
                                      self.damp.data_ptr(), self.w.data_ptr(), *[_lib.ptr(r) for r in res],
-                                     ckpt.data_ptr(), int(K), gvp.data_ptr(), _lib.ptr(grho), ws.data_ptr(),
-                                     ws.numel(), engine.stream_handle(dev))
+                                     _lib.ptr(ckpt), int(K), _lib.ptr(img), int(bool(img_rho)), gvp.data_ptr(),
+                                     _lib.ptr(grho), ws.data_ptr(), ws.numel(), engine.stream_handle(dev))
         self.check(rc)
         return gvp, grho
 
 
+def _imaging_fits(run, nbytes: int) -> bool:
+    """Whether nbytes of imaging fields, the adjoint's workspace and a margin
+    (2 GiB + 5 %) fit in the device memory available now (counting blocks the
+    caching allocator holds unused)."""
+    free, _ = torch.cuda.mem_get_info(run.device)
+    avail = free + torch.cuda.memory_reserved(run.device) - torch.cuda.memory_allocated(run.device)
+    ws = int(run.L.gb3_backward_workspace_bytes(ctypes.byref(run.desc), 0, 1))
+    return nbytes + ws + (2 << 30) + avail // 20 <= avail
+
+
 class _Function3D(torch.autograd.Function):
-    """3-D traces as a differentiable function of (vp, rho): checkpoints every
-    K steps in the forward, the hand-written adjoint in the backward
-    (replaces autograd through acoustic_3d.py:446-460)."""
+    """3-D traces as a differentiable function of (vp, rho): every step's
+    imaging fields (or checkpoints every K steps) in the forward, the
+    hand-written adjoint in the backward (replaces autograd through
+    acoustic_3d.py:446-460)."""
 
     @staticmethod
-    def forward(ctx, vp, rho, run, K):
+    def forward(ctx, vp, rho, run, K, imaging_cache):
         vp32 = vp.detach().to(torch.float32).contiguous()
         rho32 = rho.detach().to(torch.float32).contiguous()
-        ckpt = torch.empty(int(run.L.gb3_checkpoint_bytes(ctypes.byref(run.desc), int(K))) // 4,
-                           device=run.device, dtype=torch.float32)
-        tr, en = run.forward(vp32, rho32, ckpt, K)
-        ctx.run, ctx.K, ctx.ckpt = run, K, ckpt
+        img_rho = bool(ctx.needs_input_grad[1])
+        nimg = int(run.L.gb3_imaging_bytes(ctypes.byref(run.desc), int(img_rho)))
+        img = ckpt = None
+        if imaging_cache == "auto" and _imaging_fits(run, nimg):
+            img = torch.empty(nimg // 4, device=run.device, dtype=torch.float32)
+        else:
+            ckpt = torch.empty(int(run.L.gb3_checkpoint_bytes(ctypes.byref(run.desc), int(K))) // 4,
+                               device=run.device, dtype=torch.float32)
+        tr, en = run.forward(vp32, rho32, ckpt, K, img, img_rho)
+        ctx.run, ctx.K, ctx.ckpt, ctx.img, ctx.img_rho = run, K, ckpt, img, img_rho
         ctx.save_for_backward(vp32, rho32)
         ctx.mark_non_differentiable(*en)
         return (*tr, *en)
@@ -98,16 +117,18 @@ class _Function3D(torch.autograd.Function):
         vp32, rho32 = ctx.saved_tensors
         need_vp, need_rho = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
         res = [None if t is None else t.to(torch.float32).contiguous() for t in (gp, gvx, gvy, gvz)]
-        gvp, grho = ctx.run.backward(vp32, rho32, res, ctx.ckpt, ctx.K, need_rho)
-        ctx.ckpt = None
-        return (gvp if need_vp else None), (grho if need_rho else None), None, None
+        # img_rho was set from needs_input_grad at the forward, so it covers need_rho
+        gvp, grho = ctx.run.backward(vp32, rho32, res, ctx.ckpt, ctx.K, need_rho, ctx.img, ctx.img_rho)
+        ctx.ckpt = ctx.img = None
+        return (gvp if need_vp else None), (grho if need_rho else None), None, None, None
 
 
 def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, dz: float, nt: int, dt: float,
                                nabc: int, free_surface: bool, src_x: Tensor, src_y: Tensor, src_z: Tensor,
                                src_n: int, src_v: Tensor, rcv_x: Tensor, rcv_y: Tensor, rcv_z: Tensor, rcv_n: int,
                                damp: Tensor, vp: Tensor, rho: Tensor, checkpoint_segments: int = 1,
-                               device: torch.device = torch.device("cpu"), dtype: torch.dtype = torch.float32):
+                               device: torch.device = torch.device("cpu"), dtype: torch.dtype = torch.float32, *,
+                               imaging_cache="auto"):
     device = torch.device(device)
     if device.type != "cuda":
         raise ValueError(f"geobrain_b200 runs on CUDA devices only (device={device})")
@@ -115,6 +136,8 @@ def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, 
         raise TypeError(f"geobrain_b200 computes in float32 (dtype={dtype})")
     if checkpoint_segments < 1:
         raise ValueError(f"checkpoint_segments must be >= 1, got {checkpoint_segments}")
+    if imaging_cache not in ("auto", 0):
+        raise ValueError(f"imaging_cache must be 'auto' or 0, got {imaging_cache!r}")
     nx, ny, nz, nt, nabc, src_n, rcv_n = (int(v) for v in (nx, ny, nz, nt, nabc, src_n, rcv_n))
     pos = [engine._i64(a) for a in (src_x, src_y, src_z)]
     rpos = [engine._i64(a) for a in (rcv_x, rcv_y, rcv_z)]
@@ -149,7 +172,7 @@ def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, 
         # segments of about sqrt(nt) steps, and never fewer than the caller's checkpoint_segments
         n_seg = max(int(checkpoint_segments), int(math.ceil(math.sqrt(nt))))
         K = max(1, -(-nt // n_seg))
-        outs = _Function3D.apply(vp_g, rho_g, run, K)
+        outs = _Function3D.apply(vp_g, rho_g, run, K, imaging_cache)
         tr, en = list(outs[:4]), list(outs[4:])
     else:
         vp_t = _as_f32(vp.detach() if torch.is_tensor(vp) else vp, device, "vp")

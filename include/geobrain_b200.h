@@ -344,26 +344,35 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
                 const float *vp, const float *rho, const float *damp, const float *wavelet,
                 float *trace_p, float *trace_vx, float *trace_vy, float *trace_vz,
                 float *energy_p, float *energy_vx, float *energy_vy, float *energy_vz,
-                float *checkpoints, int32_t checkpoint_every,
+                float *checkpoints, int32_t checkpoint_every, float *imaging, int32_t imaging_rho,
                 void *workspace, size_t workspace_bytes, void *stream);
 
 /* Gradient of the 3-D path (the reference differentiates it with autograd
- * through torch.utils.checkpoint, acoustic_3d.py:446-460).  gb3_forward keeps
- * the full state before every checkpoint_every-th step in `checkpoints`
- * (gb3_checkpoint_bytes; may be NULL when no gradient follows).  gb3_backward
- * recomputes each segment from its checkpoint, keeping the imaging fields,
- * and runs the exact discrete adjoint backwards in time with the zero-lag
- * imaging condition.  res_* = dL/d(trace_*) (n_shots, nt, n_rcv), any may
- * be NULL.  grad_vp, grad_rho: (nz, ny, nx), overwritten; grad_rho may be
- * NULL.  Workspace: gb3_backward_workspace_bytes(desc, checkpoint_every,
- * grad_rho != NULL). */
+ * through torch.utils.checkpoint, acoustic_3d.py:446-460).  The forward keeps
+ * what the adjoint needs in one of two ways:
+ *   - checkpoints: the full state before every checkpoint_every-th step
+ *     (gb3_checkpoint_bytes); gb3_backward recomputes each segment from its
+ *     checkpoint, keeping the imaging fields;
+ *   - imaging (no recompute): every step's imaging fields, I = -div v (and,
+ *     with imaging_rho, dp/dx, dp/dy, dp/dz), gb3_imaging_bytes(desc,
+ *     imaging_rho) bytes, [nt][1 or 4][n_shots][vol] fp32.
+ * Either (or both) may be NULL in gb3_forward when no gradient follows.
+ * gb3_backward takes the imaging buffer if it is not NULL (checkpoints may
+ * then be NULL; grad_rho needs imaging_rho), else the checkpoints, and runs
+ * the exact discrete adjoint backwards in time with the zero-lag imaging
+ * condition.  res_* = dL/d(trace_*) (n_shots, nt, n_rcv), any may be NULL.
+ * grad_vp, grad_rho: (nz, ny, nx), overwritten; grad_rho may be NULL.
+ * Workspace: gb3_backward_workspace_bytes(desc, checkpoint_every,
+ * grad_rho != NULL), with checkpoint_every = 0 for the imaging buffer. */
 size_t gb3_checkpoint_bytes(const gb3_model_desc *desc, int32_t checkpoint_every);
+size_t gb3_imaging_bytes(const gb3_model_desc *desc, int32_t with_rho);
 size_t gb3_backward_workspace_bytes(const gb3_model_desc *desc, int32_t checkpoint_every, int32_t with_rho);
 int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t *src_y, const int64_t *src_z,
                  const int64_t *rcv_x, const int64_t *rcv_y, const int64_t *rcv_z,
                  const float *vp, const float *rho, const float *damp, const float *wavelet,
                  const float *res_p, const float *res_vx, const float *res_vy, const float *res_vz,
-                 const float *checkpoints, int32_t checkpoint_every, float *grad_vp, float *grad_rho,
+                 const float *checkpoints, int32_t checkpoint_every, const float *imaging,
+                 int32_t imaging_rho, float *grad_vp, float *grad_rho,
                  void *workspace, size_t workspace_bytes, void *stream);
 
 /* Message of the last failure on this thread ("" if none). */

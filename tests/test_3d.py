@@ -117,11 +117,12 @@ def test_cuda_3d_rejects_what_the_reference_cannot_index(cuda_device):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("segments", [1, 4])
-def test_cuda_3d_gradient_matches_reference_autograd(cuda_device, name, segments):
+@pytest.mark.parametrize("segments,imaging_cache", [(1, 0), (4, 0), (1, "auto")])
+def test_cuda_3d_gradient_matches_reference_autograd(cuda_device, name, segments, imaging_cache):
     """dL/dvp and dL/drho of a loss linear in all four traces: the
-    hand-written 3-D adjoint (checkpointed recompute) against the reference's
-    float64 autograd gradient, 1e-4 relative L2."""
+    hand-written 3-D adjoint (checkpointed recompute, or every step's imaging
+    fields kept by the forward) against the reference's float64 autograd
+    gradient, 1e-4 relative L2."""
     from geobrain_b200.wave import acoustic_forward_kernel_3d
     c = load3(name)
     vp = torch.tensor(c["vp"], device=cuda_device, requires_grad=True)
@@ -131,12 +132,38 @@ def test_cuda_3d_gradient_matches_reference_autograd(cuda_device, name, segments
         nabc=c["nabc"], free_surface=c["free_surface"], src_x=c["src_x"], src_y=c["src_y"], src_z=c["src_z"],
         src_n=2, src_v=torch.as_tensor(c["src_v"], device=cuda_device), rcv_x=c["rcv_x"], rcv_y=c["rcv_y"],
         rcv_z=c["rcv_z"], rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=cuda_device), vp=vp,
-        rho=rho, checkpoint_segments=segments, device=cuda_device)
+        rho=rho, checkpoint_segments=segments, device=cuda_device, imaging_cache=imaging_cache)
     loss = sum((torch.as_tensor(c[f"lin_{k}"], device=cuda_device, dtype=torch.float32) * out[k]).sum()
                for k in ("p", "vx", "vy", "vz"))
     loss.backward()
     assert orc.rel_l2(vp.grad.cpu().numpy(), c["ref64_grad_vp"]) < 1e-4
     assert orc.rel_l2(rho.grad.cpu().numpy(), c["ref64_grad_rho"]) < 1e-4
+
+
+@pytest.mark.gpu
+def test_cuda_3d_imaging_cache_and_recompute_agree(cuda_device):
+    """Velocity-only and velocity + density gradients through both storage
+    modes: the cached imaging fields are the numbers the recompute writes,
+    so the two gradients are identical."""
+    from geobrain_b200.wave import acoustic_forward_kernel_3d
+    c = load3("small_3d_fs")
+    for want_rho in (False, True):
+        grads = []
+        for cache in (0, "auto"):
+            vp = torch.tensor(c["vp"], device=cuda_device, requires_grad=True)
+            rho = torch.tensor(c["rho"], device=cuda_device, requires_grad=want_rho)
+            out = acoustic_forward_kernel_3d(
+                nx=c["nx"], ny=c["ny"], nz=c["nz"], dx=c["dx"], dy=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"],
+                nabc=c["nabc"], free_surface=c["free_surface"], src_x=c["src_x"], src_y=c["src_y"],
+                src_z=c["src_z"], src_n=2, src_v=torch.as_tensor(c["src_v"], device=cuda_device), rcv_x=c["rcv_x"],
+                rcv_y=c["rcv_y"], rcv_z=c["rcv_z"], rcv_n=len(c["rcv_x"]),
+                damp=torch.as_tensor(c["damp"], device=cuda_device), vp=vp, rho=rho, device=cuda_device,
+                imaging_cache=cache)
+            (0.5 * (out["p"] ** 2).sum() + out["vz"].sum()).backward()
+            grads.append((vp.grad.cpu().numpy(), rho.grad.cpu().numpy() if want_rho else None))
+        np.testing.assert_array_equal(grads[0][0], grads[1][0])
+        if want_rho:
+            np.testing.assert_array_equal(grads[0][1], grads[1][1])
 
 
 def test_oracle_gradient_matches_reference_autograd():
