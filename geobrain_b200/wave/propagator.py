@@ -102,13 +102,16 @@ class AcousticPropagator(AbstractPropagator):
         else:
             src_x, src_z, src_n, wavelet = self.src_x, self.src_z, self.src_n, self.wavelet
         if self.model.ndim == 3:
+            if absorbing != "damping":
+                raise NotImplementedError("3-D models use the damping layers (absorbing='damping')")
             src_y = self.src_y[sl] if shot_index is not None else self.src_y
             result = acoustic_forward_kernel_3d(
                 nx=self.nx, ny=self.ny, nz=self.nz, dx=self.dx, dy=self.dy, dz=self.dz, nt=self.nt, dt=self.dt,
                 nabc=self.nabc, free_surface=self.free_surface, src_x=src_x, src_y=src_y, src_z=src_z,
                 src_n=src_n, src_v=wavelet, rcv_x=self.rcv_x, rcv_y=self.rcv_y, rcv_z=self.rcv_z,
                 rcv_n=self.rcv_n, damp=self.damp, vp=model.vp, rho=model.rho,
-                checkpoint_segments=checkpoint_segments, device=torch.device(self.device), dtype=self.dtype)
+                checkpoint_segments=checkpoint_segments, device=torch.device(self.device), dtype=self.dtype,
+                imaging_cache="auto" if imaging_cache in ("auto", "all") else 0)
             return WaveResult.from_dict(result)
         result = acoustic_forward_kernel(
             nx=self.nx, nz=self.nz, dx=self.dx, dz=self.dz, nt=self.nt, dt=self.dt, nabc=self.nabc,

@@ -197,3 +197,46 @@ def test_cpml_gradient_needs_the_full_imaging_cache(cuda_device):
             vp=torch.tensor(c["vp"], device=cuda_device, requires_grad=True),
             rho=torch.as_tensor(c["rho"], device=cuda_device), device=cuda_device, absorbing="cpml",
             imaging_cache=0)
+
+
+@pytest.mark.gpu
+def test_propagator_cpml_gradient_is_the_kernel_gradient(cuda_device):
+    """AcousticPropagator.forward(absorbing='cpml') and loss.backward(), the
+    way the FWI example drives the reference, give the kernel's CPML
+    gradient; a 3-D model refuses the option instead of ignoring it."""
+    from geobrain_b200.wave import (AcousticModel, AcousticPropagator, BoundaryConfig, GridConfig, Receiver,
+                                    Source, Survey, acoustic_forward_kernel)
+    c = load_case("small_nofs")
+    grid = GridConfig(nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"])
+    model = AcousticModel(grid, BoundaryConfig(n_layers=c["nabc"]), vp=c["vp"], rho=c["rho"], vp_grad=True,
+                          auto_update_rho=False, device=str(cuda_device))
+    src = Source(nt=c["nt"], dt=c["dt"], f0=25.0)
+    src.add_sources(x=c["src_x"], z=c["src_z"], wavelet=c["src_v"][0])
+    rcv = Receiver(nt=c["nt"], dt=c["dt"])
+    rcv.add_receivers(x=c["rcv_x"], z=c["rcv_z"], rcv_type="pr")
+    prop = AcousticPropagator(model, Survey(src, rcv), device=str(cuda_device))
+    lin = torch.as_tensor(c["lin_p"], device=cuda_device, dtype=torch.float32)
+    (lin * prop.forward(absorbing="cpml").p).sum().backward()
+    g_prop = model.vp.grad.detach().cpu().numpy()
+
+    vp = torch.tensor(c["vp"], device=cuda_device, requires_grad=True)
+    out = acoustic_forward_kernel(
+        nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+        free_surface=False, src_x=c["src_x"], src_z=c["src_z"], src_n=3,
+        src_v=torch.as_tensor(np.tile(c["src_v"][0], (3, 1)), device=cuda_device), rcv_x=c["rcv_x"],
+        rcv_z=c["rcv_z"], rcv_n=len(c["rcv_x"]), damp=prop.damp, vp=vp,
+        rho=torch.as_tensor(c["rho"], device=cuda_device), device=cuda_device, absorbing="cpml")
+    (lin * out["p"]).sum().backward()
+    assert orc.rel_l2(g_prop, vp.grad.cpu().numpy()) < 1e-6
+
+    from test_3d import load3
+    c3 = load3("small_3d_nofs")
+    grid3 = GridConfig(nx=c3["nx"], nz=c3["nz"], dx=c3["dx"], dz=c3["dx"], ny=c3["ny"], dy=c3["dx"])
+    m3 = AcousticModel(grid3, BoundaryConfig(n_layers=c3["nabc"]), vp=c3["vp"], rho=c3["rho"], auto_update_rho=False,
+                       device=str(cuda_device))
+    s3 = Source(nt=c3["nt"], dt=c3["dt"], f0=25.0)
+    s3.add_sources(x=c3["src_x"], z=c3["src_z"], y=c3["src_y"], wavelet=c3["src_v"][0])
+    r3 = Receiver(nt=c3["nt"], dt=c3["dt"])
+    r3.add_receivers(x=c3["rcv_x"], z=c3["rcv_z"], y=c3["rcv_y"], rcv_type="pr")
+    with pytest.raises(NotImplementedError):
+        AcousticPropagator(m3, Survey(s3, r3), device=str(cuda_device)).forward(absorbing="cpml")
