@@ -82,7 +82,7 @@ SIGNATURES = {
     "gb_plan_set_absorbing": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_float]),
     "gb_plan_autotune": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _SZ, _I32, _P, ctypes.POINTER(ctypes.c_float)]),
     "gb_forward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _I32, _P, _P, _P, _SZ, _P]),
-    "gb_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
+    "gb_backward": (ctypes.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
     "gb_workspace_status": (ctypes.c_int, [_P, _P]),
     "gb_selftest_bounded_wait": (ctypes.c_int, [_P, _SZ, _I32, _I32, _P]),
     "gb_plan_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),

@@ -42,6 +42,11 @@ struct AdjArgs {
     float *G1, *C1, *G2, *C2;                // [n_groups][plane] sums and compensations
     int grp0, grp_count;             // shot groups this launch covers
     int *err;
+    // dL/dwavelet [S][nt] (or null): dt * lambda_p at the source cell after
+    // stage A, i.e. the adjoint of p just after the source was added
+    // (acoustic_2d.py:228-237); sources lie on the p mask (checked on the host)
+    float *grad_wavelet;
+    const int *src_z, *src_x;                // padded source cells
 };
 
 __device__ __forceinline__ void neumaier_add(float &s, float &c, float x)
@@ -214,6 +219,14 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
             }
         }
         __syncthreads();
+        if (A.grad_wavelet && threadIdx.x == 0) {
+            // the tile that owns the source cell: mu_p / a1 there is lambda_p
+            const int sz = A.src_z[s], sx = A.src_x[s];
+            if (sz >= z0 && sz < z0 + TZ && sx >= x0 && sx < x0 + TX) {
+                const int r = sz - (z0 - R), c = sx - (x0 - 4);
+                A.grad_wavelet[(long long)s * g.nt + A.it] = g.dt * (sP[r * RW + c] / sA1[r * RW + c]);
+            }
+        }
 
         // ---------------- stage B: tile --------------------------------------
         if (vlane) {

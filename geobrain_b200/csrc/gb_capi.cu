@@ -761,7 +761,7 @@ int check_store(const gb_plan *P, const gb_grad_store *store)
 // so no memory variables need checkpointing).
 int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *damp, const float *res_p,
                   const float *res_vx, const float *res_vz, const gb_grad_store *store, float *grad_vp,
-                  float *grad_rho, void *workspace, size_t workspace_bytes, cudaStream_t st)
+                  float *grad_rho, float *grad_wavelet, void *workspace, size_t workspace_bytes, cudaStream_t st)
 {
     const gb_model_desc &d = P->d;
     if (store->cached_steps < d.nt)
@@ -830,6 +830,11 @@ int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *da
         else cpml_adj_v_kernel<2><<<grid, block, 0, st>>>(A);
         if (fs) {
             cpml_fold_kernel<<<fold_blocks, 256, 0, st>>>(g, lam[1], 0, 2, -1.f);
+            ++P->launches;
+        }
+        if (grad_wavelet) {
+            cpml_wavelet_grad_kernel<<<(S + 127) / 128, 128, 0, st>>>(g, lam[1], Su.d_src, Su.d_src + S, grad_wavelet,
+                                                                       it);
             ++P->launches;
         }
         A.lin = lam[1];
@@ -1604,15 +1609,26 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
 
 int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp, const float *wavelet,
                 const float *res_p, const float *res_vx, const float *res_vz, const gb_grad_store *store,
-                float *grad_vp, float *grad_rho, void *workspace, size_t workspace_bytes, void *stream)
+                float *grad_vp, float *grad_rho, float *grad_wavelet, void *workspace, size_t workspace_bytes,
+                void *stream)
 {
     g_last_error.clear();
     if (!P || !vp || !rho || !damp || !wavelet || !store || !grad_vp) return fail(GB_E_ARG, "null argument");
     if (int rc = check_store(P, store)) return rc;
     if (grad_rho && !store->with_rho) return fail(GB_E_ARG, "density gradient needs a store made with with_rho");
+    if (grad_wavelet) {
+        // the adjoint keeps lambda_p on the p mask only (cells off it never
+        // depend on the model); a source off it would need the dropped part
+        const StepGeom gm = P->geom();
+        for (int s = 0; s < P->d.n_shots; ++s)
+            if (P->src_z[s] < gm.p_r0 || P->src_z[s] > gm.p_r1 || P->src_x[s] < gm.p_c0 || P->src_x[s] > gm.p_c1)
+                return fail(GB_E_UNSUPPORTED, "wavelet gradients need every source inside the p update region");
+        GB_CUDA(cudaMemsetAsync(grad_wavelet, 0, (size_t)P->d.n_shots * P->d.nt * 4,
+                                reinterpret_cast<cudaStream_t>(stream)));
+    }
     if (P->cpml)
-        return backward_cpml(P, vp, rho, damp, res_p, res_vx, res_vz, store, grad_vp, grad_rho, workspace,
-                             workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
+        return backward_cpml(P, vp, rho, damp, res_p, res_vx, res_vz, store, grad_vp, grad_rho, grad_wavelet,
+                             workspace, workspace_bytes, reinterpret_cast<cudaStream_t>(stream));
     const gb_model_desc &d = P->d;
     const int S = d.n_shots;
     const int K = std::min<int>(store->checkpoint_every, d.nt);
@@ -1681,6 +1697,9 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     A.img_field_stride = (long long)S * P->plane;
     A.G1 = G1; A.C1 = C1; A.G2 = G2; A.C2 = C2;
     A.err = Su.err;
+    A.grad_wavelet = grad_wavelet;
+    A.src_z = Su.d_src;
+    A.src_x = Su.d_src + S;
 
     GroupStreams gs;
     if (int rc = group_streams(P, st, &gs)) return rc;

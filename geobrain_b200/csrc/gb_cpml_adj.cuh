@@ -72,6 +72,17 @@ __global__ void cpml_inject_kernel(const StepGeom g, float *lam, const int2 *rcv
     }
 }
 
+// dL/dwavelet[s, it] = dt * lam_p at the source cell, read between adj_v and
+// adj_p (lam_p is then the adjoint of p just after the source was added)
+__global__ void cpml_wavelet_grad_kernel(const StepGeom g, const float *lam, const int *src_z, const int *src_x,
+                                         float *grad_wavelet, int it)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.n_shots) return;
+    const long long o = (long long)src_z[s] * g.pitch + src_x[s];
+    grad_wavelet[(long long)s * g.nt + it] = g.dt * lam[(long long)s * kCpmlFields * g.plane + o];
+}
+
 // free-surface fold of field f: row fs-1 into row fs-1+to with sign, then cleared
 __global__ void cpml_fold_kernel(const StepGeom g, float *lam, int field, int to, float sign)
 {

@@ -292,25 +292,29 @@ def choose_cached_steps(plan: Plan, imaging_cache, with_rho: bool, device, imagi
 
 
 def run_backward(plan: Plan, vp, rho, damp, src_v, res_p, res_vx, res_vz, store: "_lib.GradStore",
-                 want_rho: bool):
+                 want_rho: bool, want_wavelet: bool = False):
     g = plan.geo
     dev = vp.device
     grad_vp = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32)
     grad_rho = torch.empty((g.nz, g.nx), device=dev, dtype=torch.float32) if want_rho else None
+    grad_w = torch.empty((plan.n_shots, g.nt), device=dev, dtype=torch.float32) if want_wavelet else None
     seg = max(1, min(store.checkpoint_every, g.nt - store.cached_steps))    # steps of one recompute segment
     ifmt = {v: k for k, v in _lib.IMAGING_FORMATS.items()}[store.imaging_format]
     ws = workspace(plan.gradient_workspace_bytes(bool(store.with_rho), seg, ifmt), dev)
     with torch.cuda.device(dev):
         rc = plan._lib.gb_backward(plan.h, vp.data_ptr(), rho.data_ptr(), damp.data_ptr(), src_v.data_ptr(),
                                    _lib.ptr(res_p), _lib.ptr(res_vx), _lib.ptr(res_vz), ctypes.byref(store),
-                                   grad_vp.data_ptr(), _lib.ptr(grad_rho), ws.data_ptr(), ws.numel(),
-                                   stream_handle(dev))
+                                   grad_vp.data_ptr(), _lib.ptr(grad_rho), _lib.ptr(grad_w), ws.data_ptr(),
+                                   ws.numel(), stream_handle(dev))
     _lib.check(rc)
+    if want_wavelet:
+        return grad_vp, grad_rho, grad_w
     return grad_vp, grad_rho
 
 
 class AcousticFunction(torch.autograd.Function):
-    """Traces (p, vx, vz) as a differentiable function of (vp, rho).
+    """Traces (p, vx, vz) as a differentiable function of (vp, rho) and of
+    the source wavelets src_v.
 
     forward: gb_forward keeping checkpoints every K steps (fp32, or bf16 /
     fp16 with per-snapshot scales) and the imaging fields of the last
@@ -322,6 +326,7 @@ class AcousticFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, vp, rho, plan, damp, src_v, opts):
         dev = vp.device
+        src_v = src_v.detach().contiguous()
         vp32 = vp.detach().to(torch.float32).contiguous()
         rho32 = rho.detach().to(torch.float32).contiguous()
         K, fmt, with_rho, cached = opts["checkpoint_every"], opts["fmt"], opts["with_rho"], opts["cached_steps"]
@@ -346,17 +351,19 @@ class AcousticFunction(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gp, gvx, gvz, *unused):
         vp32, rho32, damp, src_v = ctx.saved_tensors
-        need_vp, need_rho = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
-        if not (need_vp or need_rho):
+        need_vp, need_rho, need_w = ctx.needs_input_grad[0], ctx.needs_input_grad[1], ctx.needs_input_grad[4]
+        if not (need_vp or need_rho or need_w):
             return None, None, None, None, None, None
         res = [None if t is None else t.to(torch.float32).contiguous() for t in (gp, gvx, gvz)]
         if all(r is None for r in res):
             z = torch.zeros_like(vp32)
-            return (z if need_vp else None), (z.clone() if need_rho else None), None, None, None, None
-        gvp, grho = run_backward(ctx.plan, vp32, rho32, damp, src_v, *res, ctx.store,
-                                 need_rho and bool(ctx.store.with_rho))
+            return ((z if need_vp else None), (z.clone() if need_rho else None), None, None,
+                    (torch.zeros_like(src_v) if need_w else None), None)
+        out = run_backward(ctx.plan, vp32, rho32, damp, src_v, *res, ctx.store,
+                           need_rho and bool(ctx.store.with_rho), want_wavelet=need_w)
+        gvp, grho = out[0], out[1]
         ctx.store_keep = None
-        return (gvp if need_vp else None), (grho if need_rho else None), None, None, None, None
+        return (gvp if need_vp else None), (grho if need_rho else None), None, None, (out[2] if need_w else None), None
 
 
 def differentiable_forward(plan: Plan, vp, rho, damp, src_v, *, device, snapshot_every: int = 0,

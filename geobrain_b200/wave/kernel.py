@@ -94,8 +94,17 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
         if tuple(t.shape) != (int(nz), int(nx)):
             raise ValueError(f"{name} must have shape {(int(nz), int(nx))}, got {tuple(t.shape)}")
 
+    wave_grad = torch.is_grad_enabled() and w.requires_grad
+    if wave_grad:
+        # the adjoint keeps lambda_p on the pressure update region only
+        fs = int(nabc) if free_surface else 1
+        R = engine.FD_ORDERS[fd_order]
+        pz, px = sz + int(nabc), sx + int(nabc)
+        if ((pz < max(fs + 1, R)) | (pz > Nz - 1 - R) | (px < R) | (px > Nx - 1 - R)).any():
+            raise NotImplementedError("wavelet gradients need every source inside the pressure update region "
+                                      f"(no closer than {R} cells to the padded edge, below the free surface)")
     needs_grad_now = torch.is_grad_enabled() and (getattr(vp, "requires_grad", False) or
-                                                  getattr(rho, "requires_grad", False))
+                                                  getattr(rho, "requires_grad", False) or wave_grad)
     if absorbing == "cpml":
         if needs_grad_now:
             # the CPML adjoint reads every step's imaging fields: no recompute
@@ -113,8 +122,7 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
         rho_a = _as_f32(rho.detach() if torch.is_tensor(rho) else rho, device, "rho")
         plan.autotune(vp_a, rho_a, damp_t, w)
 
-    needs_grad = torch.is_grad_enabled() and (getattr(vp, "requires_grad", False) or
-                                              getattr(rho, "requires_grad", False))
+    needs_grad = needs_grad_now
     if needs_grad:
         return engine.differentiable_forward(plan, vp, rho, damp_t, w, device=device,
                                              snapshot_every=int(snapshot_every),

@@ -214,14 +214,18 @@ int gb_forward(gb_plan *plan, const float *vp, const float *rho, const float *da
  * over shots and time with compensated fp32 summation and folds the padding
  * back into the edge cells (the adjoint of pad_model).  grad_vp / grad_rho
  * are (nz, nx) float32 and are overwritten; grad_rho may be NULL (it needs a
- * store made with with_rho).  Workspace: gb_plan_gradient_workspace_bytes
+ * store made with with_rho).  grad_wavelet, (n_shots, nt) float32 or NULL,
+ * receives dL/d(wavelet), what autograd through the reference's source
+ * injection gives (acoustic_2d.py:228-237); it needs every source inside the
+ * pressure update region (padded z in [max(fs+1, R), Nz-1-R], x in
+ * [R, Nx-1-R]; GB_E_UNSUPPORTED otherwise).  Workspace: gb_plan_gradient_workspace_bytes
  * (the recompute segments only cover the uncached steps, and their imaging
  * fields are kept in the store's imaging_format). */
 int gb_backward(gb_plan *plan, const float *vp, const float *rho, const float *damp,
                 const float *wavelet,
                 const float *res_p, const float *res_vx, const float *res_vz,
                 const gb_grad_store *store,
-                float *grad_vp, float *grad_rho,
+                float *grad_vp, float *grad_rho, float *grad_wavelet,
                 void *workspace, size_t workspace_bytes, void *stream);
 
 /* Profiling (used by the benchmark): when enabled, gb_forward and

@@ -140,7 +140,7 @@ def forward_torch(*, nz, nx, dz, nt, dt, nabc, free_surface, src_x, src_z, src_v
     rx, rz = torch.as_tensor(np.asarray(rcv_x) + nabc), torch.as_tensor(np.asarray(rcv_z) + nabc)
     onehot = torch.zeros(S, Nz, Nx, dtype=torch.float64)
     onehot[torch.arange(S), torch.as_tensor(sz), torch.as_tensor(sx)] = 1.0
-    w = tt(src_v)
+    w = src_v if torch.is_tensor(src_v) else tt(src_v)
     zero = torch.zeros(S, Nz, Nx, dtype=torch.float64)
     p, vx, vz, ppx, ppz, pvx, pvz = (zero,) * 7
     tr = {"p": [], "vx": [], "vz": []}
@@ -166,15 +166,19 @@ def forward_torch(*, nz, nx, dz, nt, dt, nabc, free_surface, src_x, src_z, src_v
     return {k: torch.stack(v, dim=1) for k, v in tr.items()}
 
 
-def gradient(*, res_p=None, res_vx=None, res_vz=None, vp, rho, **kw):
-    """dL/dvp and dL/drho of L = sum(res_p * p) + sum(res_vx * vx) +
-    sum(res_vz * vz) over the traces, by float64 autograd through
-    forward_torch (res_* are (S, nt, R) weights, any may be None)."""
+def gradient(*, res_p=None, res_vx=None, res_vz=None, vp, rho, src_v, with_wavelet=False, **kw):
+    """dL/dvp and dL/drho (and, with_wavelet, dL/dsrc_v) of L = sum(res_p *
+    p) + sum(res_vx * vx) + sum(res_vz * vz) over the traces, by float64
+    autograd through forward_torch (res_* are (S, nt, R) weights, any may be
+    None)."""
     import torch
     v = torch.tensor(np.asarray(vp, np.float64), requires_grad=True)
     r = torch.tensor(np.asarray(rho, np.float64), requires_grad=True)
-    tr = forward_torch(vp=v, rho=r, **kw)
-    loss = sum((torch.as_tensor(np.asarray(w, np.float64)) * tr[k]).sum()
-               for k, w in (("p", res_p), ("vx", res_vx), ("vz", res_vz)) if w is not None)
+    w = torch.tensor(np.asarray(src_v, np.float64), requires_grad=with_wavelet)
+    tr = forward_torch(vp=v, rho=r, src_v=w, **kw)
+    loss = sum((torch.as_tensor(np.asarray(x, np.float64)) * tr[k]).sum()
+               for k, x in (("p", res_p), ("vx", res_vx), ("vz", res_vz)) if x is not None)
     loss.backward()
+    if with_wavelet:
+        return v.grad.numpy(), r.grad.numpy(), w.grad.numpy()
     return v.grad.numpy(), r.grad.numpy()

@@ -240,3 +240,23 @@ def test_propagator_cpml_gradient_is_the_kernel_gradient(cuda_device):
     r3.add_receivers(x=c3["rcv_x"], z=c3["rcv_z"], y=c3["rcv_y"], rcv_type="pr")
     with pytest.raises(NotImplementedError):
         AcousticPropagator(m3, Survey(s3, r3), device=str(cuda_device)).forward(absorbing="cpml")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small_nofs", "small_fs"])
+def test_cuda_cpml_wavelet_gradient_matches_oracle(cuda_device, name):
+    from geobrain_b200.wave import acoustic_forward_kernel
+    c = load_case(name)
+    w = torch.tensor(c["src_v"], device=cuda_device, requires_grad=True)
+    vp = torch.tensor(c["vp"], device=cuda_device, requires_grad=True)
+    out = acoustic_forward_kernel(
+        nx=c["nx"], nz=c["nz"], dx=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"],
+        free_surface=c["free_surface"], src_x=c["src_x"], src_z=c["src_z"], src_n=3, src_v=w,
+        rcv_x=c["rcv_x"], rcv_z=c["rcv_z"], rcv_n=len(c["rcv_x"]), damp=torch.as_tensor(c["damp"], device=cuda_device),
+        vp=vp, rho=torch.as_tensor(c["rho"], device=cuda_device), device=cuda_device, fd_order=8, absorbing="cpml")
+    lin = {k: c[f"lin_{k}"] for k in ("p", "vx", "vz")}
+    sum((torch.as_tensor(lin[k], device=cuda_device, dtype=torch.float32) * out[k]).sum() for k in lin).backward()
+    rvp, _, rw = ocp.gradient(res_p=lin["p"], res_vx=lin["vx"], res_vz=lin["vz"], half=4, with_wavelet=True,
+                              vmax=float(np.max(c["vp"])), **dict(_okw(c), vp=c["vp"], rho=c["rho"]))
+    assert orc.rel_l2(w.grad.cpu().numpy(), rw) < 1e-4, orc.rel_l2(w.grad.cpu().numpy(), rw)
+    assert orc.rel_l2(vp.grad.cpu().numpy(), rvp) < 1e-4
