@@ -73,7 +73,7 @@ SIGNATURES = {
     "gb3_checkpoint_bytes": (_SZ, [ctypes.POINTER(Desc3), _I32]),
     "gb3_backward_workspace_bytes": (_SZ, [ctypes.POINTER(Desc3), _I32, _I32]),
     "gb3_backward": (ctypes.c_int, [ctypes.POINTER(Desc3)] + [_P] * 6 + [_P] * 4 + [_P] * 4 + [_P, _I32] +
-                     [_P, _I32] + [_P, _P, _P, _SZ, _P]),
+                     [_P, _I32] + [_P, _P, _P, _P, _SZ, _P]),
     "gb_plan_autotune_workspace_bytes": (_SZ, [_P]),
     "gb_plan_get_config": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                           ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),

@@ -549,6 +549,17 @@ __global__ void __launch_bounds__(128, 4) adj_p3_kernel(const AdjArgs3 A)
         if (x0 + q < g.Nx) neumaier3(A.G1[o + q], A.C1[o + q], g1[q]);
 }
 
+// dL/dwavelet[s, it] = dt * lam_p at the source cell, read after the adjoint
+// of the velocity updates and the free-surface fold (lam_p is then the
+// adjoint of p just after the source was added, acoustic_3d.py:153-163)
+__global__ void wavelet_grad3_kernel(const Geo3 g, const float *lam, const int *src, float *grad_wavelet, int it)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= g.n_shots) return;
+    const long long o = (long long)src[s] * g.plane + (long long)src[g.n_shots + s] * g.pitch + src[2 * g.n_shots + s];
+    grad_wavelet[(long long)s * g.nt + it] = g.dt * lam[(long long)s * 4 * g.vol + o];
+}
+
 // Adjoint of the recording: lam[field][receiver cell] += res[field][s][it][r]
 __global__ void inj3_kernel(const Geo3 g, float *lam, const int *rcv, const float *res_p, const float *res_vx,
                             const float *res_vy, const float *res_vz, int it)

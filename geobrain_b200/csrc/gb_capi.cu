@@ -1408,8 +1408,8 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
                  const int64_t *rcv_x, const int64_t *rcv_y, const int64_t *rcv_z, const float *vp, const float *rho,
                  const float *damp, const float *wavelet, const float *res_p, const float *res_vx,
                  const float *res_vy, const float *res_vz, const float *checkpoints, int32_t checkpoint_every,
-                 const float *imaging, int32_t imaging_rho, float *grad_vp, float *grad_rho, void *workspace,
-                 size_t workspace_bytes, void *stream)
+                 const float *imaging, int32_t imaging_rho, float *grad_vp, float *grad_rho, float *grad_wavelet,
+                 void *workspace, size_t workspace_bytes, void *stream)
 {
     g_last_error.clear();
     Geo3 g;
@@ -1447,6 +1447,7 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
         GB_CUDA(cudaMemsetAsync(G2, 0, (size_t)g.vol * 4, st));
         GB_CUDA(cudaMemsetAsync(C2, 0, (size_t)g.vol * 4, st));
     }
+    if (grad_wavelet) GB_CUDA(cudaMemsetAsync(grad_wavelet, 0, (size_t)g.n_shots * g.nt * 4, st));
     coef3_kernel<<<4 * 148, 256, 0, st>>>(g, vp, rho, damp, desc->dz, coef, coef + g.vol, coef + 2 * g.vol,
                                           coef + 3 * g.vol, coef + 4 * g.vol, coef + 5 * g.vol);
     GB_CUDA(cudaGetLastError());
@@ -1494,6 +1495,8 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
             A.lam_out = lam_b;
             adj_v3_kernel<<<grid, block, 0, st>>>(A);
             if (fs) fold3_kernel<<<148, 256, 0, st>>>(g, lam_b, 0, 2, -1.f);
+            if (grad_wavelet)
+                wavelet_grad3_kernel<<<(g.n_shots + 127) / 128, 128, 0, st>>>(g, lam_b, d_src, grad_wavelet, it);
             A.lam_in = lam_b;
             A.lam_out = lam_a;
             adj_p3_kernel<<<grid, block, 0, st>>>(A);

@@ -62,20 +62,22 @@ class _Run3:
         self.check(rc)
         return tr, en
 
-    def backward(self, vp, rho, res, ckpt, K, want_rho, img=None, img_rho=False):
+    def backward(self, vp, rho, res, ckpt, K, want_rho, img=None, img_rho=False, want_wavelet=False):
         d, dev = self.desc, self.device
         K = 0 if img is not None else K
         ws = engine.workspace(int(self.L.gb3_backward_workspace_bytes(ctypes.byref(d), int(K), int(want_rho))), dev)
         gvp = torch.empty((d.nz, d.ny, d.nx), device=dev, dtype=torch.float32)
         grho = torch.empty_like(gvp) if want_rho else None
+        gw = torch.empty((d.n_shots, d.nt), device=dev, dtype=torch.float32) if want_wavelet else None
         with torch.cuda.device(dev):
             rc = self.L.gb3_backward(ctypes.byref(d), *[p.ctypes.data for p in self.pos],
                                      *[p.ctypes.data for p in self.rpos], vp.data_ptr(), rho.data_ptr(),
                                      self.damp.data_ptr(), self.w.data_ptr(), *[_lib.ptr(r) for r in res],
                                      _lib.ptr(ckpt), int(K), _lib.ptr(img), int(bool(img_rho)), gvp.data_ptr(),
-                                     _lib.ptr(grho), ws.data_ptr(), ws.numel(), engine.stream_handle(dev))
+                                     _lib.ptr(grho), _lib.ptr(gw), ws.data_ptr(), ws.numel(),
+                                     engine.stream_handle(dev))
         self.check(rc)
-        return gvp, grho
+        return gvp, grho, gw
 
 
 def _imaging_fits(run, nbytes: int) -> bool:
@@ -95,7 +97,9 @@ class _Function3D(torch.autograd.Function):
     acoustic_3d.py:446-460)."""
 
     @staticmethod
-    def forward(ctx, vp, rho, run, K, imaging_cache):
+    def forward(ctx, vp, rho, wavelet, run, K, imaging_cache):
+        # the C calls read run.w, the wavelet this graph node differentiates
+        run.w = wavelet.detach().contiguous()
         vp32 = vp.detach().to(torch.float32).contiguous()
         rho32 = rho.detach().to(torch.float32).contiguous()
         img_rho = bool(ctx.needs_input_grad[1])
@@ -115,12 +119,13 @@ class _Function3D(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gp, gvx, gvy, gvz, *unused):
         vp32, rho32 = ctx.saved_tensors
-        need_vp, need_rho = ctx.needs_input_grad[0], ctx.needs_input_grad[1]
+        need_vp, need_rho, need_w = ctx.needs_input_grad[0], ctx.needs_input_grad[1], ctx.needs_input_grad[2]
         res = [None if t is None else t.to(torch.float32).contiguous() for t in (gp, gvx, gvy, gvz)]
         # img_rho was set from needs_input_grad at the forward, so it covers need_rho
-        gvp, grho = ctx.run.backward(vp32, rho32, res, ctx.ckpt, ctx.K, need_rho, ctx.img, ctx.img_rho)
+        gvp, grho, gw = ctx.run.backward(vp32, rho32, res, ctx.ckpt, ctx.K, need_rho, ctx.img, ctx.img_rho,
+                                         want_wavelet=need_w)
         ctx.ckpt = ctx.img = None
-        return (gvp if need_vp else None), (grho if need_rho else None), None, None, None
+        return (gvp if need_vp else None), (grho if need_rho else None), gw, None, None, None
 
 
 def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, dz: float, nt: int, dt: float,
@@ -162,7 +167,7 @@ def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, 
                       float(dz))
     run = _Run3(desc, pos, rpos, damp_t, w, device)
     needs_grad = torch.is_grad_enabled() and (getattr(vp, "requires_grad", False) or
-                                              getattr(rho, "requires_grad", False))
+                                              getattr(rho, "requires_grad", False) or w.requires_grad)
     if needs_grad:
         vp_g = vp if torch.is_tensor(vp) else torch.as_tensor(vp)
         rho_g = rho if torch.is_tensor(rho) else torch.as_tensor(rho)
@@ -172,7 +177,7 @@ def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, 
         # segments of about sqrt(nt) steps, and never fewer than the caller's checkpoint_segments
         n_seg = max(int(checkpoint_segments), int(math.ceil(math.sqrt(nt))))
         K = max(1, -(-nt // n_seg))
-        outs = _Function3D.apply(vp_g, rho_g, run, K, imaging_cache)
+        outs = _Function3D.apply(vp_g, rho_g, w, run, K, imaging_cache)
         tr, en = list(outs[:4]), list(outs[4:])
     else:
         vp_t = _as_f32(vp.detach() if torch.is_tensor(vp) else vp, device, "vp")

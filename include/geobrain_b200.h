@@ -366,6 +366,9 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
  * the exact discrete adjoint backwards in time with the zero-lag imaging
  * condition.  res_* = dL/d(trace_*) (n_shots, nt, n_rcv), any may be NULL.
  * grad_vp, grad_rho: (nz, ny, nx), overwritten; grad_rho may be NULL.
+ * grad_wavelet: (n_shots, nt) or NULL, receives dL/d(wavelet) (what
+ * autograd through the reference's source line gives, acoustic_3d.py:153-163;
+ * any source position).
  * Workspace: gb3_backward_workspace_bytes(desc, checkpoint_every,
  * grad_rho != NULL), with checkpoint_every = 0 for the imaging buffer. */
 size_t gb3_checkpoint_bytes(const gb3_model_desc *desc, int32_t checkpoint_every);
@@ -376,7 +379,7 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
                  const float *vp, const float *rho, const float *damp, const float *wavelet,
                  const float *res_p, const float *res_vx, const float *res_vy, const float *res_vz,
                  const float *checkpoints, int32_t checkpoint_every, const float *imaging,
-                 int32_t imaging_rho, float *grad_vp, float *grad_rho,
+                 int32_t imaging_rho, float *grad_vp, float *grad_rho, float *grad_wavelet,
                  void *workspace, size_t workspace_bytes, void *stream);
 
 /* Message of the last failure on this thread ("" if none). */

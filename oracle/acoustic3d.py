@@ -93,8 +93,10 @@ def forward(*, nz, ny, nx, dz, nt, dt, nabc, free_surface, src_x, src_y, src_z, 
 
 
 def gradient(*, nz, ny, nx, dz, nt, dt, nabc, free_surface, src_x, src_y, src_z, src_v, rcv_x, rcv_y, rcv_z,
-             damp, vp, rho, res_p=None, res_vx=None, res_vy=None, res_vz=None):
-    """dL/dvp and dL/drho (nz, ny, nx), float64, for the adjoint sources
+             damp, vp, rho, res_p=None, res_vx=None, res_vy=None, res_vz=None, with_wavelet=False):
+    """dL/dvp and dL/drho (nz, ny, nx), float64 (and, with_wavelet,
+    dL/dsrc_v (shots, nt): dt times the adjoint of p just after the source
+    was added, acoustic_3d.py:153-163), for the adjoint sources
     res_* = dL/d(trace_*) (shots, nt, receivers): the exact discrete adjoint
     of forward() run backwards in time over the stored states (the
     transposed p / v updates, the free-surface folds, the receiver
@@ -160,6 +162,7 @@ def gradient(*, nz, ny, nx, dz, nt, dt, nabc, free_surface, src_x, src_y, src_z,
     zero = np.zeros((S, nt, len(rx)))
     res = [np.asarray(r, t) if r is not None else zero for r in (res_p, res_vx, res_vy, res_vz)]
     lp, lx, ly, lz = np.zeros_like(p), np.zeros_like(vx), np.zeros_like(vy), np.zeros_like(vz)
+    gw = np.zeros((S, nt))             # dL/dsrc_v
     g1 = np.zeros((Nz, Ny, Nx))       # dL/da1
     g2 = np.zeros((Nz, Ny, Nx))       # dL/da2
     si = np.arange(S)[:, None]
@@ -195,6 +198,7 @@ def gradient(*, nz, ny, nx, dz, nt, dt, nabc, free_surface, src_x, src_y, src_z,
         if free_surface:                                   # p[fs-1] = -p[fs+1]
             lp[:, fs + 1] -= lp[:, fs - 1]
             lp[:, fs - 1] = 0
+        gw[:, it] = dt * lp[np.arange(S), sz, sy, sx]      # adjoint of the source line
         # adjoint of the pressure update (it reads v^n)
         vxn, vyn, vzn = hist_v[it]
         R = (slice(None), slice(z0, z1), slice(y0, y1), slice(x0, x1))
@@ -228,4 +232,6 @@ def gradient(*, nz, ny, nx, dz, nt, dt, nabc, free_surface, src_x, src_y, src_z,
         ix = np.clip(np.arange(Nx) - nabc, 0, nx - 1)
         np.add.at(out, (iz[:, None, None], iy[None, :, None], ix[None, None, :]), g)
         return out
+    if with_wavelet:
+        return fold(g_c), fold(g_den), gw
     return fold(g_c), fold(g_den)

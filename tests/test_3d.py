@@ -195,3 +195,45 @@ def test_propagator_runs_3d_models(cuda_device):
     assert res.vy is not None
     for k in ("p", "vx", "vy", "vz"):
         assert orc.rel_l2(getattr(res, k).cpu().numpy(), c[f"ref32_{k}"]) < 1e-5, k
+
+
+def test_oracle_wavelet_gradient_is_exact_for_the_linear_source():
+    """The traces are linear in the wavelet, so <dL/dw, d> equals
+    (L(w + d) - L(w - d)) / 2 up to rounding, for any d."""
+    c = load3("small_3d_fs")
+    lin = {k: c[f"lin_{k}"] for k in ("p", "vx", "vy", "vz")}
+    _, _, gw = o3.gradient(**kw3(c), res_p=lin["p"], res_vx=lin["vx"], res_vy=lin["vy"], res_vz=lin["vz"],
+                           with_wavelet=True)
+    d = np.random.default_rng(4).standard_normal(c["src_v"].shape)
+
+    def loss(w):
+        out = o3.forward(**dict(kw3(c), src_v=w), dtype=np.float64)
+        return sum(float((lin[k] * out[k]).sum()) for k in lin)
+
+    w0 = c["src_v"].astype(np.float64)
+    fd = (loss(w0 + d) - loss(w0 - d)) / 2
+    assert abs(fd - float((gw * d).sum())) <= 1e-10 * abs(fd)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("imaging_cache", [0, "auto"])
+def test_cuda_3d_wavelet_gradient_matches_oracle(cuda_device, imaging_cache):
+    """dL/d(src_v) with the model gradient, a source on the outermost padded
+    plane included (the 3-D adjoint keeps lambda everywhere)."""
+    from geobrain_b200.wave import acoustic_forward_kernel_3d
+    c = dict(load3("small_3d_fs"))
+    c["src_x"] = np.array([c["src_x"][0], -c["nabc"]])
+    lin = {k: c[f"lin_{k}"] for k in ("p", "vx", "vy", "vz")}
+    w = torch.tensor(c["src_v"], device=cuda_device, requires_grad=True)
+    vp = torch.tensor(c["vp"], device=cuda_device, requires_grad=True)
+    out = acoustic_forward_kernel_3d(
+        nx=c["nx"], ny=c["ny"], nz=c["nz"], dx=c["dx"], dy=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"],
+        nabc=c["nabc"], free_surface=c["free_surface"], src_x=c["src_x"], src_y=c["src_y"], src_z=c["src_z"],
+        src_n=2, src_v=w, rcv_x=c["rcv_x"], rcv_y=c["rcv_y"], rcv_z=c["rcv_z"], rcv_n=len(c["rcv_x"]),
+        damp=torch.as_tensor(c["damp"], device=cuda_device), vp=vp,
+        rho=torch.as_tensor(c["rho"], device=cuda_device), device=cuda_device, imaging_cache=imaging_cache)
+    sum((torch.as_tensor(lin[k], device=cuda_device, dtype=torch.float32) * out[k]).sum() for k in lin).backward()
+    rvp, _, rw = o3.gradient(**kw3(c), res_p=lin["p"], res_vx=lin["vx"], res_vy=lin["vy"], res_vz=lin["vz"],
+                             with_wavelet=True)
+    assert orc.rel_l2(w.grad.cpu().numpy(), rw) < 1e-4, orc.rel_l2(w.grad.cpu().numpy(), rw)
+    assert orc.rel_l2(vp.grad.cpu().numpy(), rvp) < 1e-4
