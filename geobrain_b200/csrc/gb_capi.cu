@@ -320,7 +320,7 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
         const size_t K = std::max(1, std::min(checkpoint_every, p->d.nt));
         const size_t G = p->n_groups;
         // adjoint state: p, vx, vz (and, with CPML, the four memory variables)
-        L.mu = o; o = align256(o + 2 * S * (p->cpml ? kCpmlFields : 3) * p->plane * 4);
+        L.mu = o; o = align256(o + S * (p->cpml ? kCpmlPlanes : 2 * 3) * p->plane * 4);
         L.img = o; o = align256(o + K * L.n_img * S * p->plane * img_esize(img_fmt));
         L.g1 = o; o = align256(o + G * p->plane * 4);
         L.c1 = o; o = align256(o + G * p->plane * 4);
@@ -775,12 +775,11 @@ int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *da
     Setup Su;
     if (int rc = common_setup(P, L, ws, vp, rho, damp, st, &Su)) return rc;
     const int S = d.n_shots;
-    const size_t lam_fl = (size_t)S * kCpmlFields * P->plane;
-    float *lam[2] = {reinterpret_cast<float *>(ws + L.mu), reinterpret_cast<float *>(ws + L.mu) + lam_fl};
+    float *lam = reinterpret_cast<float *>(ws + L.mu);   // [S][kCpmlPlanes][plane]
     float *G1 = reinterpret_cast<float *>(ws + L.g1), *C1 = reinterpret_cast<float *>(ws + L.c1);
     float *G2 = rho_fields ? reinterpret_cast<float *>(ws + L.g2) : nullptr;
     float *C2 = rho_fields ? reinterpret_cast<float *>(ws + L.c2) : nullptr;
-    GB_CUDA(cudaMemsetAsync(lam[0], 0, 2 * lam_fl * 4, st));
+    GB_CUDA(cudaMemsetAsync(lam, 0, (size_t)S * kCpmlPlanes * P->plane * 4, st));
     GB_CUDA(cudaMemsetAsync(G1, 0, (size_t)P->n_groups * P->plane * 4, st));
     GB_CUDA(cudaMemsetAsync(C1, 0, (size_t)P->n_groups * P->plane * 4, st));
     if (G2) {
@@ -802,6 +801,7 @@ int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *da
     A.a1 = Su.a1;
     A.a2 = Su.a2;
     A.cp = cpcoef;
+    A.lam = lam;
     A.img_field_stride = (long long)S * P->plane;
     A.img_fmt = ifmt;
     A.G1 = G1; A.C1 = C1; A.G2 = G2; A.C2 = C2;
@@ -813,34 +813,37 @@ int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *da
     const int fold_blocks = (int)std::min<long long>(1024, ((long long)S * P->Nx + 255) / 256);
     P->mark(2, true, st);
     P->phase_steps[2] += d.nt;
+    int sv = 0, sp = 0;   // the memory-variable slots read this step
     for (int it = d.nt - 1; it >= 0; --it) {
         if (inject) {
             cpml_inject_kernel<<<std::max(1, std::min(1024, (S * d.n_rcv + 255) / 256)), 256, 0, st>>>(
-                g, lam[0], d_rcv, res_p, res_vx, res_vz, it);
+                g, lam, d_rcv, res_p, res_vx, res_vz, it);
             ++P->launches;
         }
         if (fs) {
-            cpml_fold_kernel<<<fold_blocks, 256, 0, st>>>(g, lam[0], 2, 1, 1.f);
+            cpml_fold_kernel<<<fold_blocks, 256, 0, st>>>(g, lam, kLamVZ, 1, 1.f);
             ++P->launches;
         }
         A.img = img_at(store->imaging, (size_t)it * step_img, img_esize(ifmt));
-        A.lin = lam[0];
-        A.lout = lam[1];
+        A.psi_in = kPsiV0 + 2 * sv;
+        A.psi_out = kPsiV0 + 2 * (sv ^ 1);
         if (P->R == 4) cpml_adj_v_kernel<4><<<grid, block, 0, st>>>(A);
         else cpml_adj_v_kernel<2><<<grid, block, 0, st>>>(A);
+        sv ^= 1;
         if (fs) {
-            cpml_fold_kernel<<<fold_blocks, 256, 0, st>>>(g, lam[1], 0, 2, -1.f);
+            cpml_fold_kernel<<<fold_blocks, 256, 0, st>>>(g, lam, kLamP, 2, -1.f);
             ++P->launches;
         }
         if (grad_wavelet) {
-            cpml_wavelet_grad_kernel<<<(S + 127) / 128, 128, 0, st>>>(g, lam[1], Su.d_src, Su.d_src + S, grad_wavelet,
+            cpml_wavelet_grad_kernel<<<(S + 127) / 128, 128, 0, st>>>(g, lam, Su.d_src, Su.d_src + S, grad_wavelet,
                                                                        it);
             ++P->launches;
         }
-        A.lin = lam[1];
-        A.lout = lam[0];
+        A.psi_in = kPsiP0 + 2 * sp;
+        A.psi_out = kPsiP0 + 2 * (sp ^ 1);
         if (P->R == 4) cpml_adj_p_kernel<4><<<grid, block, 0, st>>>(A);
         else cpml_adj_p_kernel<2><<<grid, block, 0, st>>>(A);
+        sp ^= 1;
         P->launches += 2;
         GB_CUDA(cudaGetLastError());
     }

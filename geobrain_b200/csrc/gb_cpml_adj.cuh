@@ -11,9 +11,10 @@
 //
 // With b = 1 + a these read p' = p - a1 (bx (Dx + psi_px) + bz (Dz + psi_pz))
 // and vx' = vx - a2 bxh (Gx + psi_vx), which give the transposes below.  The
-// adjoint state lam (unscaled) of the seven fields lives in ping-pong
-// buffers [S][7][plane] (p, vx, vz, psi_px, psi_pz, psi_vx, psi_vz).  Per
-// step, in reverse order of the forward:
+// adjoint state lam (unscaled) of the seven fields lives in one buffer
+// [S][11][plane]: lam_p, lam_vx, lam_vz updated in place, and two slots of
+// each memory variable used in turn (the kernels read those at neighbours
+// while they write them).  Per step, in reverse order of the forward:
 //
 //   inject   lam[receiver] += dL/dtrace[s, n, r]
 //   fold     lam_vz[fs] += lam_vz[fs-1], lam_vz[fs-1] = 0
@@ -41,7 +42,7 @@
 
 namespace gb {
 
-constexpr int kCpmlFields = 7;
+constexpr int kCpmlPlanes = 11;   // the adjoint state planes of one shot (below)
 
 __device__ __forceinline__ bool cp_in_p(const StepGeom &g, int z, int x)
 {
@@ -64,7 +65,7 @@ __global__ void cpml_inject_kernel(const StepGeom g, float *lam, const int2 *rcv
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const int s = (int)(i / g.n_rcv), r = (int)(i % g.n_rcv);
         const long long o = (long long)rcv[r].x * g.pitch + rcv[r].y;
-        float *L = lam + (long long)s * kCpmlFields * g.plane;
+        float *L = lam + (long long)s * kCpmlPlanes * g.plane;
         const long long t = ((long long)s * g.nt + it) * g.n_rcv + r;
         if (res_p) atomicAdd(L + o, res_p[t]);   // receivers may share a cell
         if (res_vx) atomicAdd(L + g.plane + o, res_vx[t]);
@@ -80,7 +81,7 @@ __global__ void cpml_wavelet_grad_kernel(const StepGeom g, const float *lam, con
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= g.n_shots) return;
     const long long o = (long long)src_z[s] * g.pitch + src_x[s];
-    grad_wavelet[(long long)s * g.nt + it] = g.dt * lam[(long long)s * kCpmlFields * g.plane + o];
+    grad_wavelet[(long long)s * g.nt + it] = g.dt * lam[(long long)s * kCpmlPlanes * g.plane + o];
 }
 
 // free-surface fold of field f: row fs-1 into row fs-1+to with sign, then cleared
@@ -89,7 +90,7 @@ __global__ void cpml_fold_kernel(const StepGeom g, float *lam, int field, int to
     const long long n = (long long)g.n_shots * g.Nx;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const int s = (int)(i / g.Nx), x = (int)(i % g.Nx);
-        float *F = lam + ((long long)s * kCpmlFields + field) * g.plane;
+        float *F = lam + ((long long)s * kCpmlPlanes + field) * g.plane;
         const long long m = (long long)(g.fs - 1) * g.pitch + x;
         F[m + (long long)to * g.pitch] += sign * F[m];
         F[m] = 0.f;
@@ -123,21 +124,32 @@ __global__ void cpml_adj_coef_kernel(const StepGeom g, const float *a1, const fl
     }
 }
 
-// Ask L2 for the next shot's 7 fields of this thread's cells while the
-// current shot computes (the loads of one shot alone leave DRAM idle
-// between shots at 12-16 resident warps per SM).
-__device__ __forceinline__ void cp_prefetch_shot(const float *L, long long P, long long o)
+// The adjoint state of one shot: [kCpmlPlanes][plane].  lam_p, lam_vx and
+// lam_vz have one slot each and are updated in place (neither kernel reads
+// at its neighbours a field it writes); the memory variables, which the
+// kernels read at neighbours and rewrite, have two slots each, used in turn:
+constexpr int kLamP = 0, kLamVX = 1, kLamVZ = 2;
+constexpr int kPsiP0 = 3;   // psi_px, psi_pz, slot 0 at 3, 4 and slot 1 at 5, 6
+constexpr int kPsiV0 = 7;   // psi_vx, psi_vz, slot 0 at 7, 8 and slot 1 at 9, 10
+
+// Ask L2 for the next shot's fields of this thread's cells while the current
+// shot computes (the loads of one shot alone leave DRAM idle between shots
+// at 12-16 resident warps per SM).
+__device__ __forceinline__ void cp_prefetch(const float *L, long long P, long long o, int f0, int f1)
 {
-#pragma unroll
-    for (int f = 0; f < kCpmlFields; ++f) asm volatile("prefetch.global.L2 [%0];" ::"l"(L + f * P + o));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(L + o));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(L + P + o));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(L + 2 * P + o));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(L + f0 * P + o));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(L + f1 * P + o));
 }
 
 struct CpmlAdjArgs4 {
     StepGeom g;
     const float *a1, *a2;
     const float *cp;            // the kCpmlCoefPlanes planes
-    const float *lin;           // [S][7][plane]
-    float *lout;
+    float *lam;                 // [S][kCpmlPlanes][plane]
+    int psi_in, psi_out;        // first plane of the memory-variable slot read / written
     const float *img;           // this step's I [S][plane], then Jx, Jz at img_field_stride
     long long img_field_stride;
     int img_fmt;
@@ -149,6 +161,11 @@ __device__ __forceinline__ float4 cp_ld4(const float *base, long long o, bool ok
 {
     return ok ? __ldg(reinterpret_cast<const float4 *>(base + o)) : zero4();
 }
+// plain load, for the fields a kernel also writes (in place, own cells only)
+__device__ __forceinline__ float4 cp_ldw4(const float *base, long long o)
+{
+    return *reinterpret_cast<const float4 *>(base + o);
+}
 __device__ __forceinline__ float4 fms4(const float4 &a, const float4 &x, const float4 &b, const float4 &y)
 {
     // a x - b y per lane
@@ -156,9 +173,11 @@ __device__ __forceinline__ float4 fms4(const float4 &a, const float4 &x, const f
 }
 
 // block (32, 4): 4 adjacent cells of one row per thread, looping over the
-// shots, so each cell of the gradient planes has one owner
+// shots, so each cell of the gradient planes has one owner.  Reads lam_vx,
+// lam_vz and the psi_v slot psi_in (at neighbours), writes lam_p in place
+// and the psi_v slot psi_out.
 template <int R>
-__global__ void __launch_bounds__(128) cpml_adj_v_kernel(const CpmlAdjArgs4 A)
+__global__ void __launch_bounds__(128, 4) cpml_adj_v_kernel(const CpmlAdjArgs4 A)
 {
     const StepGeom &g = A.g;
     const int x0 = 4 * (blockIdx.x * 32 + threadIdx.x);
@@ -183,10 +202,10 @@ __global__ void __launch_bounds__(128) cpml_adj_v_kernel(const CpmlAdjArgs4 A)
     }
     float g2[4] = {0.f, 0.f, 0.f, 0.f}, c2[4] = {0.f, 0.f, 0.f, 0.f};
     for (int s = 0; s < g.n_shots; ++s) {
-        const float *L = A.lin + (long long)s * kCpmlFields * P;
-        float *O = A.lout + (long long)s * kCpmlFields * P;
-        const float *Lvx = L + P, *Lvz = L + 2 * P, *Lsvx = L + 5 * P, *Lsvz = L + 6 * P;
-        if (s + 1 < g.n_shots) cp_prefetch_shot(L + kCpmlFields * P, P, o);
+        float *L = A.lam + (long long)s * kCpmlPlanes * P;
+        const float *Lvx = L + kLamVX * P, *Lvz = L + kLamVZ * P;
+        const float *Lsvx = L + A.psi_in * P, *Lsvz = L + (A.psi_in + 1) * P;
+        if (s + 1 < g.n_shots) cp_prefetch(L + kCpmlPlanes * P, P, o, A.psi_in, A.psi_in + 1);
         // wx = AX lam_psi_vx - WX lam_vx at x0-4 .. x0+7
         float wx[12];
         {
@@ -207,9 +226,9 @@ __global__ void __launch_bounds__(128) cpml_adj_v_kernel(const CpmlAdjArgs4 A)
             wz[t] = ok ? fms4(cp_ld4(AZ, q, true), cp_ld4(Lsvz, q, true), cp_ld4(WZ, q, true), cp_ld4(Lvz, q, true))
                        : zero4();
         }
-        const float4 lp = cp_ld4(L, o, true), lvx = cp_ld4(Lvx, o, true), lvz = cp_ld4(Lvz, o, true);
+        const float4 lp = cp_ldw4(L, o), lvx = cp_ld4(Lvx, o, true), lvz = cp_ld4(Lvz, o, true);
         const float4 lsvx = cp_ld4(Lsvx, o, true), lsvz = cp_ld4(Lsvz, o, true);
-        float4 op, ovx, ovz;
+        float4 op, mvxv, mvzv;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             float t = 0.f;
@@ -217,24 +236,19 @@ __global__ void __launch_bounds__(128) cpml_adj_v_kernel(const CpmlAdjArgs4 A)
             for (int k = 0; k < R; ++k)
                 t += g.c[k] * ((wx[q + 3 - k] - wx[q + 4 + k]) + (at(wz[R - 1 - k], q) - at(wz[R + k], q)));
             at(op, q) = mp[q] ? at(lp, q) + t : 0.f;
-            at(ovx, q) = mvx[q] ? at(lvx, q) : 0.f;
-            at(ovz, q) = mvz[q] ? at(lvz, q) : 0.f;
+            at(mvxv, q) = mvx[q] ? at(lvx, q) : 0.f;
+            at(mvzv, q) = mvz[q] ? at(lvz, q) : 0.f;
         }
-        stg4(O + o, op);
-        stg4(O + P + o, ovx);
-        stg4(O + 2 * P + o, ovz);
-        stg4(O + 3 * P + o, cp_ld4(L + 3 * P, o, true));
-        stg4(O + 4 * P + o, cp_ld4(L + 4 * P, o, true));
-        stg4(O + 5 * P + o, fms4(bxc, lsvx, wxc, lvx));
-        stg4(O + 6 * P + o, fms4(bzc, lsvz, wzc, lvz));
+        stg4(L + o, op);
+        stg4(L + A.psi_out * P + o, fms4(bxc, lsvx, wxc, lvx));
+        stg4(L + (A.psi_out + 1) * P + o, fms4(bzc, lsvz, wzc, lvz));
         if (A.G2) {
             const long long io = (long long)s * P + o;
             const float4 jx = decode_img4(load_img_raw(A.img, A.img_field_stride + io, A.img_fmt), A.img_fmt);
             const float4 jz = decode_img4(load_img_raw(A.img, 2 * A.img_field_stride + io, A.img_fmt), A.img_fmt);
 #pragma unroll
             for (int q = 0; q < 4; ++q)
-                neumaier_add(g2[q], c2[q], at(a2, q) * ((mvx[q] ? at(ovx, q) * at(jx, q) : 0.f) +
-                                                        (mvz[q] ? at(ovz, q) * at(jz, q) : 0.f)));
+                neumaier_add(g2[q], c2[q], at(a2, q) * (at(mvxv, q) * at(jx, q) + at(mvzv, q) * at(jz, q)));
         }
     }
     if (A.G2) {
@@ -244,8 +258,10 @@ __global__ void __launch_bounds__(128) cpml_adj_v_kernel(const CpmlAdjArgs4 A)
     }
 }
 
+// Reads lam_p and the psi_p slot psi_in (at neighbours), writes lam_vx and
+// lam_vz in place and the psi_p slot psi_out.
 template <int R>
-__global__ void __launch_bounds__(128) cpml_adj_p_kernel(const CpmlAdjArgs4 A)
+__global__ void __launch_bounds__(128, 4) cpml_adj_p_kernel(const CpmlAdjArgs4 A)
 {
     const StepGeom &g = A.g;
     const int x0 = 4 * (blockIdx.x * 32 + threadIdx.x);
@@ -270,10 +286,9 @@ __global__ void __launch_bounds__(128) cpml_adj_p_kernel(const CpmlAdjArgs4 A)
     }
     float g1[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
     for (int s = 0; s < g.n_shots; ++s) {
-        const float *L = A.lin + (long long)s * kCpmlFields * P;
-        float *O = A.lout + (long long)s * kCpmlFields * P;
-        const float *Lspx = L + 3 * P, *Lspz = L + 4 * P;
-        if (s + 1 < g.n_shots) cp_prefetch_shot(L + kCpmlFields * P, P, o);
+        float *L = A.lam + (long long)s * kCpmlPlanes * P;
+        const float *Lspx = L + A.psi_in * P, *Lspz = L + (A.psi_in + 1) * P;
+        if (s + 1 < g.n_shots) cp_prefetch(L + kCpmlPlanes * P, P, o, A.psi_in, A.psi_in + 1);
         // ux = PX lam_psi_px - UX lam_p at x0-4 .. x0+7
         float ux[12];
         {
@@ -294,9 +309,9 @@ __global__ void __launch_bounds__(128) cpml_adj_p_kernel(const CpmlAdjArgs4 A)
             uz[t] = ok ? fms4(cp_ld4(PZ, q, true), cp_ld4(Lspz, q, true), cp_ld4(UZ, q, true), cp_ld4(L, q, true))
                        : zero4();
         }
-        const float4 lp = cp_ld4(L, o, true), lvx = cp_ld4(L + P, o, true), lvz = cp_ld4(L + 2 * P, o, true);
+        const float4 lp = cp_ld4(L, o, true), lvx = cp_ldw4(L + kLamVX * P, o), lvz = cp_ldw4(L + kLamVZ * P, o);
         const float4 lspx = cp_ld4(Lspx, o, true), lspz = cp_ld4(Lspz, o, true);
-        float4 op, ovx, ovz;
+        float4 ovx, ovz;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             float tx = 0.f, tz = 0.f;
@@ -305,21 +320,17 @@ __global__ void __launch_bounds__(128) cpml_adj_p_kernel(const CpmlAdjArgs4 A)
                 tx += g.c[k] * (ux[q + 4 - k] - ux[q + 5 + k]);
                 tz += g.c[k] * (at(uz[R - 1 - k], q) - at(uz[R + k], q));
             }
-            at(op, q) = mp[q] ? at(lp, q) : 0.f;
             at(ovx, q) = mvx[q] ? at(lvx, q) + tx : 0.f;
             at(ovz, q) = mvz[q] ? at(lvz, q) + tz : 0.f;
         }
-        stg4(O + o, op);
-        stg4(O + P + o, ovx);
-        stg4(O + 2 * P + o, ovz);
-        stg4(O + 3 * P + o, fms4(qxc, lspx, uxc, lp));
-        stg4(O + 4 * P + o, fms4(qzc, lspz, uzc, lp));
-        stg4(O + 5 * P + o, cp_ld4(L + 5 * P, o, true));
-        stg4(O + 6 * P + o, cp_ld4(L + 6 * P, o, true));
+        stg4(L + kLamVX * P + o, ovx);
+        stg4(L + kLamVZ * P + o, ovz);
+        stg4(L + A.psi_out * P + o, fms4(qxc, lspx, uxc, lp));
+        stg4(L + (A.psi_out + 1) * P + o, fms4(qzc, lspz, uzc, lp));
         const float4 im = decode_img4(load_img_raw(A.img, (long long)s * P + o, A.img_fmt), A.img_fmt);
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-            if (mp[q]) neumaier_add(g1[q], c1[q], at(a1, q) * at(op, q) * at(im, q));
+            if (mp[q]) neumaier_add(g1[q], c1[q], at(a1, q) * at(lp, q) * at(im, q));
     }
 #pragma unroll
     for (int q = 0; q < 4; ++q)
