@@ -63,6 +63,11 @@ class _Prepared:
                 w = w.unsqueeze(0).expand(src_n, -1)
             w = w.contiguous()
             damp = _as_f32(m["damp"], device, "damp")
+            try:
+                engine.check_model_inputs(_as_f32(m["vp"], device, "vp"), _as_f32(m["rho"], device, "rho"), w,
+                                          float(m["dt"]), float(m["dx"]), fd_order)
+            except ValueError as e:
+                raise ValueError(f"model {i}: {e}") from None
             self.plans.append(plan)
             self.inputs.append((m["vp"], m["rho"], damp, w))
         for plan in self.plans:

@@ -24,6 +24,38 @@ _PLAN_CACHE: "OrderedDict[tuple, Plan]" = OrderedDict()
 _PLAN_CACHE_SIZE = 32
 
 
+# staggered Taylor coefficients c_k of each order (acoustic_2d.py:211-285 at order 4)
+FD_COEFFICIENTS = {4: (9 / 8, 1 / 24), 8: (1225 / 1024, 245 / 3072, 49 / 5120, 5 / 7168)}
+
+
+def courant_number(vmax: float, dt: float, dx: float, fd_order: int, ndim: int = 2) -> float:
+    """Courant number of the staggered leapfrog, vmax dt / dx * sum|c_k| *
+    sqrt(ndim); the scheme is stable below 1."""
+    return float(vmax) * float(dt) / float(dx) * sum(FD_COEFFICIENTS[fd_order]) * math.sqrt(ndim)
+
+
+def check_model_inputs(vp: torch.Tensor, rho: torch.Tensor, src_v: torch.Tensor, dt: float, dx: float,
+                       fd_order: int, ndim: int = 2) -> float:
+    """Host-side checks before a launch (the reference has none: an unstable
+    or non-finite run there ends in Inf / NaN traces): vp, rho and the
+    wavelets finite, vp and rho positive, and the Courant number below 1.
+    One device-to-host read.  Returns vmax."""
+    vp, rho, src_v = vp.detach(), rho.detach(), src_v.detach()
+    flags = torch.stack([torch.isfinite(vp).all(), torch.isfinite(rho).all(), torch.isfinite(src_v).all(),
+                         (vp > 0).all(), (rho > 0).all()]).to(torch.float32)
+    vals = torch.cat([flags, vp.max().reshape(1).to(torch.float32)]).tolist()
+    for ok, what in zip(vals[:5], ("vp has non-finite values", "rho has non-finite values",
+                                   "src_v has non-finite values", "vp must be positive", "rho must be positive")):
+        if not ok:
+            raise ValueError(what)
+    vmax = vals[5]
+    cn = courant_number(vmax, dt, dx, fd_order, ndim)
+    if cn >= 1.0:
+        raise ValueError(f"unstable time step: Courant number {cn:.3f} >= 1 (vmax {vmax:g}, dt {dt:g}, dx {dx:g}, "
+                         f"order {fd_order}, {ndim}-D); reduce dt")
+    return vmax
+
+
 def _i64(a) -> np.ndarray:
     if torch.is_tensor(a):
         a = a.detach().cpu().numpy()

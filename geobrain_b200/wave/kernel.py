@@ -93,6 +93,7 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
     for name, t in (("vp", vp), ("rho", rho)):
         if tuple(t.shape) != (int(nz), int(nx)):
             raise ValueError(f"{name} must have shape {(int(nz), int(nx))}, got {tuple(t.shape)}")
+    vmax = engine.check_model_inputs(_as_f32(vp, device, "vp"), _as_f32(rho, device, "rho"), w, dt, dx, fd_order)
 
     wave_grad = torch.is_grad_enabled() and w.requires_grad
     if wave_grad:
@@ -111,7 +112,6 @@ def acoustic_forward_kernel(nx: int, nz: int, dx: float, dz: float, nt: int, dt:
             if imaging_cache not in ("auto", "all"):
                 raise ValueError("CPML gradients keep the imaging fields of every step (imaging_cache='all')")
             imaging_cache = "all"
-        vmax = float(vp.detach().max()) if torch.is_tensor(vp) else float(torch.as_tensor(vp).max())
         plan.set_absorbing("cpml", vmax)
     else:
         plan.set_absorbing(absorbing)

@@ -163,6 +163,8 @@ def acoustic_forward_kernel_3d(nx: int, ny: int, nz: int, dx: float, dy: float, 
     for name, t in (("vp", vp), ("rho", rho)):
         if tuple(t.shape) != (nz, ny, nx):
             raise ValueError(f"{name} must have shape {(nz, ny, nx)}, got {tuple(t.shape)}")
+    # every derivative is scaled by 1/dz, as in the reference
+    engine.check_model_inputs(_as_f32(vp, device, "vp"), _as_f32(rho, device, "rho"), w, dt, dz, 4, ndim=3)
     desc = _lib.Desc3(nz, ny, nx, nabc, nt, src_n, rcv_n, int(bool(free_surface)), float(dt), float(dx), float(dy),
                       float(dz))
     run = _Run3(desc, pos, rpos, damp_t, w, device)

@@ -113,3 +113,15 @@ def test_shared_receiver_cells_and_border_positions(cuda_device, free_surface):
         np.testing.assert_array_equal(out["p"][:, :, 0], out["p"][:, :, 1])
         check_forward(c, out, fd_order)
         check_gradient(c, out, lin, fd_order)
+
+
+def test_unstable_or_non_finite_runs_are_refused(cuda_device):
+    """The reference would return Inf / NaN traces; the boundary refuses the
+    run before any launch instead, naming the Courant number or the input."""
+    c = case()
+    with pytest.raises(ValueError, match="Courant"):
+        run(dict(c, dt=3e-3), cuda_device, 8)
+    bad = dict(c, vp=c["vp"].copy())
+    bad["vp"][3, 4] = np.inf
+    with pytest.raises(ValueError, match="non-finite"):
+        run(bad, cuda_device, 4)

@@ -145,3 +145,32 @@ def test_uneven_batch_covers_sizes():
     assert len(ms) == 24
     assert all(4 <= m.n_shots <= 16 for m in ms)
     assert all(m.vp.min() >= 1500 and m.vp.max() <= 4500 for m in ms)
+
+
+def test_courant_number_and_input_checks():
+    """The host checks the boundary runs before a launch: the Courant number
+    of the staggered scheme (stable below 1), finite and positive models and
+    finite wavelets."""
+    import torch
+    from geobrain_b200.wave import engine
+    # 4th order, 2-D: vmax dt / dx * (9/8 + 1/24) * sqrt(2)
+    assert abs(engine.courant_number(3000.0, 1e-3, 10.0, 4) - 0.3 * (7 / 6) * 2 ** 0.5) < 1e-12
+    assert engine.courant_number(3000.0, 1e-3, 10.0, 8) > engine.courant_number(3000.0, 1e-3, 10.0, 4)
+    assert abs(engine.courant_number(1.0, 1.0, 1.0, 4, ndim=3) / engine.courant_number(1.0, 1.0, 1.0, 4) -
+               (3 / 2) ** 0.5) < 1e-12
+    vp = torch.full((8, 9), 3000.0)
+    rho = torch.full((8, 9), 2000.0)
+    w = torch.zeros(2, 5)
+    assert engine.check_model_inputs(vp, rho, w, 1e-3, 10.0, 8) == 3000.0
+    with pytest.raises(ValueError, match="Courant"):
+        engine.check_model_inputs(vp, rho, w, 3e-3, 10.0, 8)
+    with pytest.raises(ValueError, match="Courant"):
+        engine.check_model_inputs(vp, rho, w, 2e-3, 10.0, 4, ndim=3)
+    bad = vp.clone()
+    bad[3, 4] = float("nan")
+    with pytest.raises(ValueError, match="vp has non-finite"):
+        engine.check_model_inputs(bad, rho, w, 1e-3, 10.0, 8)
+    with pytest.raises(ValueError, match="rho must be positive"):
+        engine.check_model_inputs(vp, -rho, w, 1e-3, 10.0, 8)
+    with pytest.raises(ValueError, match="src_v has non-finite"):
+        engine.check_model_inputs(vp, rho, w + float("inf"), 1e-3, 10.0, 8)
