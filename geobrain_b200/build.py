@@ -14,7 +14,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SRC = os.path.join(HERE, "csrc", "gb_capi.cu")
+# the translation units of the library (headers are included from them)
+SRC = [os.path.join(HERE, "csrc", f) for f in ("gb_capi.cu", "gb_capi3d.cu")]
 OUT = os.path.join(HERE, "_so", "libgeobrain_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -44,7 +45,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-o", OUT + ".tmp", SRC]
+           "-o", OUT + ".tmp", *SRC]
     if verbose:
         cmd.append("-Xptxas=-v")
     subprocess.run(cmd, check=True)
