@@ -80,9 +80,6 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
     const int s0 = group * g.shots_per_cta;
     const int ns = min(g.n_shots - s0, g.shots_per_cta);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const bool fast = A.tile_fast[tile] != 0;
-    const int rcv0 = A.rcv_ptr[tile], rcv1 = A.rcv_ptr[tile + 1];
-    const bool has_rcv = rcv1 > rcv0 && (A.res_p || A.res_vx || A.res_vz);
 
     if (threadIdx.x == 0) {
         mbar_init(&bars[0], 1);
@@ -90,6 +87,11 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
         mbar_init(&bars[2], 1);
         fence_mbar_init();
     }
+    grid_dependency_wait();
+    grid_launch_dependents();
+    const bool fast = A.tile_fast[tile] != 0;
+    const int rcv0 = A.rcv_ptr[tile], rcv1 = A.rcv_ptr[tile + 1];
+    const bool has_rcv = rcv1 > rcv0 && (A.res_p || A.res_vx || A.res_vz);
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bars[2], SM::COEF_BYTES);

@@ -84,6 +84,14 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Programmatic dependent launch.  A step kernel launched with programmatic
+// stream serialisation may start while the previous kernel of its stream is
+// still running: it sets up shared memory, then waits here before it reads
+// or writes anything a previous kernel touches (a no-op for a kernel
+// launched without the attribute), then lets the next one launch.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 {
     uint32_t ok;

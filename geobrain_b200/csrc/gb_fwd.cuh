@@ -122,9 +122,6 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
 
     const int z0 = (tile / g.tiles_x) * TZ;
     const int x0 = (tile % g.tiles_x) * TX;
-    // a CUDA graph replays the same launches for every chunk of steps; the
-    // chunk's first step comes from device memory
-    const int it = A.step_base ? *reinterpret_cast<const volatile int *>(A.step_base) + A.it : A.it;
     const int s0 = group * g.shots_per_cta;
     const int ns = min(g.n_shots - s0, g.shots_per_cta);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -135,6 +132,11 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
         mbar_init(&bars[2], 1);
         fence_mbar_init();
     }
+    grid_dependency_wait();
+    grid_launch_dependents();
+    // a CUDA graph replays the same launches for every chunk of steps; the
+    // chunk's first step comes from device memory
+    const int it = A.step_base ? *reinterpret_cast<const volatile int *>(A.step_base) + A.it : A.it;
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bars[2], SM::COEF_BYTES);

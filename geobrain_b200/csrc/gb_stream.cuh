@@ -162,7 +162,6 @@ fwd_stream_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant_
     if (zs >= g.Nz) return;                                    // uniform per CTA
     const int n_chunks = min(SA.seg_chunks, (g.Nz - zs + SCH - 1) / SCH);
     const int ze = zs + n_chunks * SCH;                          // rows this CTA owns: [zs, min(ze, Nz))
-    const int it = A.step_base ? *reinterpret_cast<const volatile int *>(A.step_base) + A.it : A.it;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int gx0 = x0 - 4 + 4 * lane;
     const bool vlane = lane >= 1 && lane <= 30;
@@ -177,6 +176,9 @@ fwd_stream_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant_
         mbar_init(&bars[2], 1);
         fence_mbar_init();
     }
+    grid_dependency_wait();
+    grid_launch_dependents();
+    const int it = A.step_base ? *reinterpret_cast<const volatile int *>(A.step_base) + A.it : A.it;
     __syncthreads();
     if (threadIdx.x == 0) {
         stream_stage_load(&mP, &mVX, &mVZ, &mA1, &mA2, sP, sVX, sVZ, sA1, sA2, bars, -1, zs, x0, s, R, true);
