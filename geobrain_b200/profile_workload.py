@@ -3,6 +3,7 @@
     python -m geobrain_b200.profile_workload --phase forward  --nt 6
     python -m geobrain_b200.profile_workload --phase gradient --nt 6 [--imaging-dtype fp24]
     python -m geobrain_b200.profile_workload --model 3d --phase forward --nt 6
+    python -m geobrain_b200.profile_workload --phase gradient --nt 6 --imaging-dtype fp24 --absorbing cpml
 
 Builds the 400 x 1200 / 32-shot / 8th-order model of the benchmark, runs
 ``nt`` time steps of the forward (or forward + adjoint) once, synchronises
@@ -11,7 +12,9 @@ and exits 0.  Everything stays on the device; nothing is timed.  With
 format (as the benchmark does); without it, one fp32 checkpoint and a
 recompute of all steps.  --model 3d runs the 3-D path instead: a 200^3
 model with a 20-cell PML and 4 shots, 4th order (acoustic_forward_kernel_3d;
-the gradient is that of 0.5 ||p||^2 with one checkpoint).
+the gradient is that of 0.5 ||p||^2 with one checkpoint).  --absorbing cpml
+uses the CPML layers (its gradient needs --imaging-dtype: the adjoint reads
+every step's imaging fields).
 """
 from __future__ import annotations
 
@@ -34,6 +37,7 @@ def main() -> None:
     ap.add_argument("--energy", action="store_true")
     ap.add_argument("--imaging-dtype", choices=["fp32", "fp24", "bf16"], default=None)
     ap.add_argument("--model", choices=["2d", "3d"], default="2d")
+    ap.add_argument("--absorbing", choices=["damping", "cpml"], default="damping")
     args = ap.parse_args()
     dev = torch.device("cuda:0")
     if args.model == "3d":
@@ -46,6 +50,7 @@ def main() -> None:
                         device=dev)
     geo = engine.Geometry(w.nz, w.nx, w.nabc, w.nt, float(w.dt), float(w.dx), w.fd_order // 2, False)
     plan = engine.get_plan(geo, w.src_x, w.src_z, w.rcv_x, w.rcv_z)
+    plan.set_absorbing(args.absorbing, float(w.vp.max()) if args.absorbing == "cpml" else 0.0)
     if args.tile_rows or args.shots_per_cta:
         plan.set_tiling(args.tile_rows, args.shots_per_cta)
     vp = torch.tensor(w.vp, device=dev)
