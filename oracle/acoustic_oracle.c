@@ -35,8 +35,13 @@
  *
  * The gradient routine is the exact discrete adjoint of that step (the
  * reverse-mode graph torch.autograd builds through acoustic_step_forward and
- * pad_model), written out by hand in the unscaled form; it keeps the whole
- * forward history in memory, so it is meant for small grids.
+ * pad_model), written out by hand in the unscaled form.  It keeps the state
+ * before every K-th step (K = ceil(sqrt(nt))) and recomputes each segment's
+ * states before running its adjoint steps, so its memory is about
+ * 2 sqrt(nt) states per shot in flight.  With fewer shots than threads the
+ * row loops run in parallel instead of the shots (the adjoint's scatter
+ * loops in two passes over alternate blocks of rows, so that no two threads
+ * add into the same cell); only the order of some additions changes.
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -80,6 +85,16 @@ int orc_fd_coefficients(int R, double *c)
     return 0;
 }
 
+int orc_max_threads(void);
+
+/* Split the rows of each step over the threads instead of the shots: when
+ * there are fewer shots than threads and the grid is large enough for the
+ * per-loop thread start-up to pay (small grids keep one thread per shot). */
+static int orc_split_rows(int n_shots, size_t cells)
+{
+    return n_shots < orc_max_threads() && cells >= ((size_t)1 << 17);
+}
+
 static inline int imax(int a, int b) { return a > b ? a : b; }
 static inline int iclamp(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
@@ -101,5 +116,16 @@ int orc_max_threads(void)
     return omp_get_max_threads();
 #else
     return 1;
+#endif
+}
+
+/* Thread count of the following calls (tests compare the row-split and the
+ * shot-split schedules); n < 1 restores the default. */
+void orc_set_threads(int n)
+{
+#ifdef _OPENMP
+    omp_set_num_threads(n >= 1 ? n : omp_get_num_procs());
+#else
+    (void)n;
 #endif
 }

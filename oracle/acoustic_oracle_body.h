@@ -35,11 +35,13 @@ static void SFX(orc_coefs)(const orc_desc *d, const REAL *vp, const REAL *rho,
     }
 }
 
-/* One leapfrog step for one shot (acoustic_2d.py:211-269), in place. */
+/* One leapfrog step for one shot (acoustic_2d.py:211-269), in place.  With
+ * par_rows the row loops run on all threads: every update reads only other
+ * fields (or the already updated pressure), so rows are independent. */
 static void SFX(orc_step)(const orc_desc *d, const REAL *cf, const REAL *a1,
                           const REAL *a2, const REAL *k1, const REAL *k2,
                           const REAL *k3, REAL *p, REAL *vx, REAL *vz,
-                          int spz, int spx, REAL src_amp, REAL *idiv)
+                          int spz, int spx, REAL src_amp, REAL *idiv, int par_rows)
 {
     const int pml = d->nabc, R = d->half;
     const int Nz = d->nz + 2 * pml, Nx = d->nx + 2 * pml;
@@ -49,6 +51,7 @@ static void SFX(orc_step)(const orc_desc *d, const REAL *cf, const REAL *a1,
     const int vz_r0 = imax(fs, R - 1), vz_r1 = Nz - 1 - R, vz_c0 = 1, vz_c1 = Nx - 2;
 
     /* pressure (:211-226) */
+#pragma omp parallel for schedule(static) if(par_rows)
     for (int i = p_r0; i <= p_r1; ++i)
         for (int j = p_c0; j <= p_c1; ++j) {
             size_t o = (size_t)i * Nx + j;
@@ -66,6 +69,7 @@ static void SFX(orc_step)(const orc_desc *d, const REAL *cf, const REAL *a1,
         for (int j = 0; j < Nx; ++j)
             p[(size_t)(fs - 1) * Nx + j] = -p[(size_t)(fs + 1) * Nx + j];
     /* vx (:244-253) */
+#pragma omp parallel for schedule(static) if(par_rows)
     for (int i = vx_r0; i <= vx_r1; ++i)
         for (int j = vx_c0; j <= vx_c1; ++j) {
             size_t o = (size_t)i * Nx + j;
@@ -74,6 +78,7 @@ static void SFX(orc_step)(const orc_desc *d, const REAL *cf, const REAL *a1,
             vx[o] = ((REAL)1 - k2[o]) * vx[o] - a2[o] * D;
         }
     /* vz (:256-265) */
+#pragma omp parallel for schedule(static) if(par_rows)
     for (int i = vz_r0; i <= vz_r1; ++i)
         for (int j = vz_c0; j <= vz_c1; ++j) {
             size_t o = (size_t)i * Nx + j;
@@ -131,13 +136,14 @@ int SFX(orc_forward)(const orc_desc *d, const REAL *vp, const REAL *rho, const R
     memset(en_vx, 0, sizeof(REAL) * nz * nx);
     memset(en_vz, 0, sizeof(REAL) * nz * nx);
     const REAL dt = (REAL)d->dt;
+    const int par_rows = orc_split_rows(S, NN);
     int snap_i = 0;
     for (int it = 0; it < nt; ++it) {
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if(!par_rows)
         for (int s = 0; s < S; ++s) {
             REAL *p = F + (size_t)s * 3 * NN, *vx = p + NN, *vz = vx + NN;
             SFX(orc_step)(d, cf, a1, a2, k1, k2, k3, p, vx, vz,
-                          (int)sz[s] + pml, (int)sx[s] + pml, dt * wav[(size_t)s * nt + it], NULL);
+                          (int)sz[s] + pml, (int)sx[s] + pml, dt * wav[(size_t)s * nt + it], NULL, par_rows);
             for (int r = 0; r < NR; ++r) {
                 size_t o = (size_t)(rz[r] + pml) * Nx + (rx[r] + pml);
                 size_t t = ((size_t)s * nt + it) * NR + r;
@@ -175,8 +181,8 @@ int SFX(orc_forward)(const orc_desc *d, const REAL *vp, const REAL *rho, const R
 
 /* Gradient of L with respect to vp and rho (and the wavelet) given the
  * adjoint sources dL/d(trace) res_* (n_shots, nt, n_rcv): the discrete
- * adjoint of every forward stage above, run backwards in time over the stored
- * forward history, then the adjoint of pad_model (edge cells collect the
+ * adjoint of every forward stage above, run backwards in time over the
+ * forward states (recomputed a segment at a time from stored ones), then the adjoint of pad_model (edge cells collect the
  * gradient of the padding they were replicated into).  g_vp, g_rho are
  * (nz, nx); g_wav (n_shots, nt) may be NULL. */
 int SFX(orc_gradient)(const orc_desc *d, const REAL *vp, const REAL *rho, const REAL *damp,
@@ -203,105 +209,140 @@ int SFX(orc_gradient)(const orc_desc *d, const REAL *vp, const REAL *rho, const 
     const REAL dt = (REAL)d->dt, dz = (REAL)d->dz;
 
     REAL *coef = (REAL *)calloc(NN * 7, sizeof(REAL));
-    REAL *hist = (REAL *)malloc(sizeof(REAL) * NN * 3 * (size_t)S * (size_t)nt);
     REAL *work = (REAL *)calloc(NN * 7 * (size_t)S, sizeof(REAL));
-    if (!coef || !hist || !work) { free(coef); free(hist); free(work); return -3; }
+    if (!coef || !work) { free(coef); free(work); return -3; }
     REAL *a1 = coef, *a2 = a1 + NN, *k1 = a2 + NN, *k2 = k1 + NN, *k3 = k2 + NN;
     REAL *cpad = k3 + NN, *dpad = cpad + NN;
     SFX(orc_coefs)(d, vp, rho, damp, a1, a2, k1, k2, k3, cpad, dpad);
+    /* segment length of the stored states, and how the threads split */
+    int Kc = 1;
+    while ((long long)Kc * Kc < nt) ++Kc;
+    const int n_ck = (nt + Kc - 1) / Kc;
+    const int par_rows = orc_split_rows(S, NN);
+    /* blocks of rows for the scatter loops: a row's updates reach at most R
+     * rows either side, so blocks of at least 2R rows, two apart, never touch
+     * the same cell */
+    const int B = 16 > 2 * R ? 16 : 2 * R;
 
     int err = 0;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if(!par_rows)
     for (int s = 0; s < S; ++s) {
         REAL *p = work + (size_t)s * 7 * NN, *vx = p + NN, *vz = vx + NN;
         REAL *lp = vz + NN, *lvx = lp + NN, *lvz = lvx + NN, *idv = lvz + NN;
         REAL *ga1 = (REAL *)calloc(NN * 2, sizeof(REAL));
-        if (!ga1) { err = -3; continue; }
+        REAL *ck = (REAL *)malloc(sizeof(REAL) * 3 * NN * (size_t)n_ck);
+        REAL *seg = (REAL *)malloc(sizeof(REAL) * 3 * NN * (size_t)Kc);
+        REAL *tvx = (REAL *)malloc(sizeof(REAL) * 2 * NN);
+        if (!ga1 || !ck || !seg || !tvx) {
+            err = -3;
+            free(ga1); free(ck); free(seg); free(tvx);
+            continue;
+        }
         REAL *ga2 = ga1 + NN;
         const int spz = (int)sz[s] + pml, spx = (int)sx[s] + pml;
-        /* forward, keeping the state before every step */
+        /* forward, keeping the state before every Kc-th step */
         for (int it = 0; it < nt; ++it) {
-            memcpy(hist + ((size_t)it * S + s) * 3 * NN, p, sizeof(REAL) * 3 * NN);
+            if (it % Kc == 0) memcpy(ck + (size_t)(it / Kc) * 3 * NN, p, sizeof(REAL) * 3 * NN);
             SFX(orc_step)(d, cf, a1, a2, k1, k2, k3, p, vx, vz, spz, spx,
-                          dt * wav[(size_t)s * nt + it], NULL);
+                          dt * wav[(size_t)s * nt + it], NULL, par_rows);
         }
         memset(lp, 0, sizeof(REAL) * 3 * NN);
-        for (int it = nt - 1; it >= 0; --it) {
-            /* rebuild the state before step it, and p3 (p after update,
-             * source and free surface) and -Dv(v^it) from it */
-            const REAL *h = hist + ((size_t)it * S + s) * 3 * NN;
-            memcpy(p, h, sizeof(REAL) * 3 * NN);
-            {
-                REAL *tvx = (REAL *)malloc(sizeof(REAL) * 2 * NN);
+        for (int c = n_ck - 1; c >= 0; --c) {
+            const int t0 = c * Kc, t1 = t0 + Kc < nt ? t0 + Kc : nt;
+            /* recompute the segment's states from its stored state */
+            memcpy(p, ck + (size_t)c * 3 * NN, sizeof(REAL) * 3 * NN);
+            for (int it = t0; it < t1; ++it) {
+                memcpy(seg + (size_t)(it - t0) * 3 * NN, p, sizeof(REAL) * 3 * NN);
+                SFX(orc_step)(d, cf, a1, a2, k1, k2, k3, p, vx, vz, spz, spx,
+                              dt * wav[(size_t)s * nt + it], NULL, par_rows);
+            }
+            for (int it = t1 - 1; it >= t0; --it) {
+                /* rebuild the state before step it, and p3 (p after update,
+                 * source and free surface) and -Dv(v^it) from it */
+                memcpy(p, seg + (size_t)(it - t0) * 3 * NN, sizeof(REAL) * 3 * NN);
                 memcpy(tvx, vx, sizeof(REAL) * 2 * NN);
                 SFX(orc_step)(d, cf, a1, a2, k1, k2, k3, p, tvx, tvx + NN, spz, spx,
-                              dt * wav[(size_t)s * nt + it], idv);
-                free(tvx);
+                              dt * wav[(size_t)s * nt + it], idv, par_rows);
+                /* p now holds p3; vx, vz hold the pre-step velocities */
+                /* receivers (:272-274): gather -> scatter-add of the residuals */
+                for (int r = 0; r < NR; ++r) {
+                    size_t o = (size_t)(rz[r] + pml) * Nx + (rx[r] + pml);
+                    size_t t = ((size_t)s * nt + it) * NR + r;
+                    lp[o] += res_p[t];
+                    lvx[o] += res_vx[t];
+                    lvz[o] += res_vz[t];
+                }
+                /* vz free surface (:268-269) */
+                if (d->free_surface)
+                    for (int j = 0; j < Nx; ++j) {
+                        lvz[(size_t)fs * Nx + j] += lvz[(size_t)(fs - 1) * Nx + j];
+                        lvz[(size_t)(fs - 1) * Nx + j] = 0;
+                    }
+                /* vz update (:256-265); it adds into lp up to R rows away */
+                for (int color = 0; color < 2; ++color) {
+                    const int nblk = (vz_r1 - vz_r0 + B) / B;
+#pragma omp parallel for schedule(static) if(par_rows)
+                    for (int b = color; b < nblk; b += 2) {
+                        const int i0 = vz_r0 + b * B, i1 = i0 + B - 1 < vz_r1 ? i0 + B - 1 : vz_r1;
+                        for (int i = i0; i <= i1; ++i)
+                            for (int j = vz_c0; j <= vz_c1; ++j) {
+                                size_t o = (size_t)i * Nx + j;
+                                REAL q = lvz[o], D = 0;
+                                for (int k = 0; k < R; ++k) {
+                                    D += cf[k] * (p[o + (size_t)(1 + k) * Nx] - p[o - (size_t)k * Nx]);
+                                    lp[o + (size_t)(1 + k) * Nx] -= a2[o] * cf[k] * q;
+                                    lp[o - (size_t)k * Nx] += a2[o] * cf[k] * q;
+                                }
+                                ga2[o] -= q * D;
+                                lvz[o] = ((REAL)1 - k3[o]) * q;
+                            }
+                    }
+                }
+                /* vx update (:244-253); its additions stay in the row */
+#pragma omp parallel for schedule(static) if(par_rows)
+                for (int i = vx_r0; i <= vx_r1; ++i)
+                    for (int j = vx_c0; j <= vx_c1; ++j) {
+                        size_t o = (size_t)i * Nx + j;
+                        REAL q = lvx[o], D = 0;
+                        for (int k = 0; k < R; ++k) {
+                            D += cf[k] * (p[o + 1 + k] - p[o - k]);
+                            lp[o + 1 + k] -= a2[o] * cf[k] * q;
+                            lp[o - k] += a2[o] * cf[k] * q;
+                        }
+                        ga2[o] -= q * D;
+                        lvx[o] = ((REAL)1 - k2[o]) * q;
+                    }
+                /* p free surface (:240-241) */
+                if (d->free_surface)
+                    for (int j = 0; j < Nx; ++j) {
+                        lp[(size_t)(fs + 1) * Nx + j] -= lp[(size_t)(fs - 1) * Nx + j];
+                        lp[(size_t)(fs - 1) * Nx + j] = 0;
+                    }
+                /* source (:228-237) */
+                if (g_wav) g_wav[(size_t)s * nt + it] = dt * lp[(size_t)spz * Nx + spx];
+                /* p update (:211-226); it adds into lvz up to R rows away */
+                for (int color = 0; color < 2; ++color) {
+                    const int nblk = (p_r1 - p_r0 + B) / B;
+#pragma omp parallel for schedule(static) if(par_rows)
+                    for (int b = color; b < nblk; b += 2) {
+                        const int i0 = p_r0 + b * B, i1 = i0 + B - 1 < p_r1 ? i0 + B - 1 : p_r1;
+                        for (int i = i0; i <= i1; ++i)
+                            for (int j = p_c0; j <= p_c1; ++j) {
+                                size_t o = (size_t)i * Nx + j;
+                                REAL q = lp[o];
+                                REAL w = a1[o] * q;
+                                ga1[o] += q * idv[o];
+                                for (int k = 0; k < R; ++k) {
+                                    lvx[o + k] -= cf[k] * w;
+                                    lvx[o - 1 - k] += cf[k] * w;
+                                    lvz[o + (size_t)k * Nx] -= cf[k] * w;
+                                    lvz[o - (size_t)(1 + k) * Nx] += cf[k] * w;
+                                }
+                                lp[o] = ((REAL)1 - k1[o]) * q;
+                            }
+                    }
+                }
             }
-            /* p now holds p3; vx, vz hold the pre-step velocities */
-            /* receivers (:272-274): gather -> scatter-add of the residuals */
-            for (int r = 0; r < NR; ++r) {
-                size_t o = (size_t)(rz[r] + pml) * Nx + (rx[r] + pml);
-                size_t t = ((size_t)s * nt + it) * NR + r;
-                lp[o] += res_p[t];
-                lvx[o] += res_vx[t];
-                lvz[o] += res_vz[t];
-            }
-            /* vz free surface (:268-269) */
-            if (d->free_surface)
-                for (int j = 0; j < Nx; ++j) {
-                    lvz[(size_t)fs * Nx + j] += lvz[(size_t)(fs - 1) * Nx + j];
-                    lvz[(size_t)(fs - 1) * Nx + j] = 0;
-                }
-            /* vz update (:256-265) */
-            for (int i = vz_r0; i <= vz_r1; ++i)
-                for (int j = vz_c0; j <= vz_c1; ++j) {
-                    size_t o = (size_t)i * Nx + j;
-                    REAL q = lvz[o], D = 0;
-                    for (int k = 0; k < R; ++k) {
-                        D += cf[k] * (p[o + (size_t)(1 + k) * Nx] - p[o - (size_t)k * Nx]);
-                        lp[o + (size_t)(1 + k) * Nx] -= a2[o] * cf[k] * q;
-                        lp[o - (size_t)k * Nx] += a2[o] * cf[k] * q;
-                    }
-                    ga2[o] -= q * D;
-                    lvz[o] = ((REAL)1 - k3[o]) * q;
-                }
-            /* vx update (:244-253) */
-            for (int i = vx_r0; i <= vx_r1; ++i)
-                for (int j = vx_c0; j <= vx_c1; ++j) {
-                    size_t o = (size_t)i * Nx + j;
-                    REAL q = lvx[o], D = 0;
-                    for (int k = 0; k < R; ++k) {
-                        D += cf[k] * (p[o + 1 + k] - p[o - k]);
-                        lp[o + 1 + k] -= a2[o] * cf[k] * q;
-                        lp[o - k] += a2[o] * cf[k] * q;
-                    }
-                    ga2[o] -= q * D;
-                    lvx[o] = ((REAL)1 - k2[o]) * q;
-                }
-            /* p free surface (:240-241) */
-            if (d->free_surface)
-                for (int j = 0; j < Nx; ++j) {
-                    lp[(size_t)(fs + 1) * Nx + j] -= lp[(size_t)(fs - 1) * Nx + j];
-                    lp[(size_t)(fs - 1) * Nx + j] = 0;
-                }
-            /* source (:228-237) */
-            if (g_wav) g_wav[(size_t)s * nt + it] = dt * lp[(size_t)spz * Nx + spx];
-            /* p update (:211-226) */
-            for (int i = p_r0; i <= p_r1; ++i)
-                for (int j = p_c0; j <= p_c1; ++j) {
-                    size_t o = (size_t)i * Nx + j;
-                    REAL q = lp[o];
-                    REAL w = a1[o] * q;
-                    ga1[o] += q * idv[o];
-                    for (int k = 0; k < R; ++k) {
-                        lvx[o + k] -= cf[k] * w;
-                        lvx[o - 1 - k] += cf[k] * w;
-                        lvz[o + (size_t)k * Nx] -= cf[k] * w;
-                        lvz[o - (size_t)(1 + k) * Nx] += cf[k] * w;
-                    }
-                    lp[o] = ((REAL)1 - k1[o]) * q;
-                }
         }
         /* alpha1 = den c^2 dt/dz, alpha2 = dt/(den dz) -> c, den */
         for (size_t o = 0; o < NN; ++o) {
@@ -314,9 +355,9 @@ int SFX(orc_gradient)(const orc_desc *d, const REAL *vp, const REAL *rho, const 
         /* park the per-shot padded gradients in the (now unused) idv/lp slots */
         memcpy(lp, ga1, sizeof(REAL) * NN);
         memcpy(lvx, ga2, sizeof(REAL) * NN);
-        free(ga1);
+        free(ga1); free(ck); free(seg); free(tvx);
     }
-    if (err) { free(coef); free(hist); free(work); return err; }
+    if (err) { free(coef); free(work); return err; }
     /* sum over shots, then fold the padding into the edge cells (pad_model
      * adjoint) */
     memset(g_vp, 0, sizeof(REAL) * nz * nx);
@@ -332,6 +373,6 @@ int SFX(orc_gradient)(const orc_desc *d, const REAL *vp, const REAL *rho, const 
             }
         }
     }
-    free(coef); free(hist); free(work);
+    free(coef); free(work);
     return 0;
 }

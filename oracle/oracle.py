@@ -51,6 +51,11 @@ def max_threads() -> int:
     return int(lib().orc_max_threads())
 
 
+def set_threads(n: int) -> None:
+    """OpenMP threads of the following oracle calls (n < 1: the default)."""
+    lib().orc_set_threads(ctypes.c_int(int(n)))
+
+
 def fd_coefficients(half: int) -> np.ndarray:
     """Staggered Taylor coefficients of half-width ``half`` (elastic_2d.py:25-68)."""
     out = np.zeros(8, dtype=np.float64)

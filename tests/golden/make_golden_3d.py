@@ -87,4 +87,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GEOBRAIN_REF", ""))
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GEOBRAIN_REF")
+    if not root:
+        sys.exit("usage: %s <path to the GeoBrain source tree> (or set GEOBRAIN_REF)" % os.path.basename(__file__))
+    main(root)

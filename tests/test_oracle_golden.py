@@ -85,3 +85,32 @@ def test_eighth_order_gradient_central_difference():
     fd = (lp - lm) / (2 * h)
     an = float(np.sum(gvp * dv))
     assert abs(fd - an) <= 1e-6 * abs(an)
+
+
+def test_row_split_schedule_matches_shot_split():
+    """Large grids with fewer shots than threads run the oracle's row loops
+    in parallel (the adjoint's scatter loops over alternate row blocks);
+    the result must not depend on the thread count.  One thread takes the
+    shot loop, the default count splits the rows of this 2-shot grid."""
+    nz, nx, nabc, nt = 320, 400, 12, 40
+    rng = np.random.default_rng(7)
+    vp = (2000 + 800 * rng.random((nz, nx))).astype(np.float64)
+    rho = (1800 + 400 * rng.random((nz, nx))).astype(np.float64)
+    from geobrain_b200.wave.boundary import bc_pml
+    damp = bc_pml(nx, nz, 10.0, 10.0, nabc, float(vp.max()), free_surface=False)
+    kw = dict(nz=nz, nx=nx, dz=10.0, nt=nt, dt=1e-3, nabc=nabc, free_surface=True, src_x=np.array([50, 300]),
+              src_z=np.array([3, 5]), src_v=rng.standard_normal((2, nt)), rcv_x=np.arange(0, nx, 3),
+              rcv_z=np.full(len(range(0, nx, 3)), 2), damp=damp, vp=vp, rho=rho, half=4)
+    res = [rng.standard_normal((2, nt, len(kw["rcv_x"]))) for _ in range(3)]
+    try:
+        orc.set_threads(1)
+        f1 = orc.forward(**kw)
+        g1 = orc.gradient(**kw, res_p=res[0], res_vx=res[1], res_vz=res[2])
+    finally:
+        orc.set_threads(0)
+    fn = orc.forward(**kw)
+    gn = orc.gradient(**kw, res_p=res[0], res_vx=res[1], res_vz=res[2])
+    for k in ("p", "vx", "vz", "forward_wavefield_p"):
+        assert orc.rel_l2(fn[k], f1[k]) <= 1e-14, k
+    for a, b in zip(gn, g1):
+        assert orc.rel_l2(a, b) <= 1e-14
