@@ -149,6 +149,87 @@ def cpu_gradient_rate(w, n_shots: int, nt: int, reps: int = 1):
                                                     f"(forward + adjoint, fp32 C oracle, OpenMP)"
 
 
+def _one_shot_kwargs(torch, wave, w, dev, shots, nt):
+    """Keyword arguments of acoustic_forward_kernel for a subset of a
+    workload's shots and its first nt steps (the full grid and receivers)."""
+    shots = np.asarray(shots)
+    damp = wave.bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp.max()), free_surface=False)
+    S = shots.size
+    return dict(nx=w.nx, nz=w.nz, dx=w.dx, dz=w.dx, nt=nt, dt=w.dt, nabc=w.nabc, free_surface=False,
+                src_x=w.src_x[shots], src_z=w.src_z[shots], src_n=S,
+                src_v=torch.tensor(np.tile(w.wavelet[:nt], (S, 1)), device=dev), rcv_x=w.rcv_x, rcv_z=w.rcv_z,
+                rcv_n=w.rcv_x.size, damp=torch.tensor(damp, dtype=torch.float32, device=dev),
+                rho=torch.tensor(w.rho, device=dev), device=dev, fd_order=w.fd_order, want_energy=False), damp
+
+
+def _oracle_kwargs(kw, w, damp, nt):
+    return dict(nz=w.nz, nx=w.nx, dz=w.dx, nt=nt, dt=w.dt, nabc=w.nabc, free_surface=False, src_x=kw["src_x"],
+                src_z=kw["src_z"], src_v=kw["src_v"].cpu().numpy(), rcv_x=w.rcv_x, rcv_z=w.rcv_z, damp=damp,
+                vp=w.vp, rho=w.rho, half=w.fd_order // 2)
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def oracle_check_fwi(torch, wave, w, dev, imaging_dtype, shots=(5, 26), nt=150):
+    """Traces and gradient of the benchmark configuration against the float64
+    C oracle, untimed: the full 460 x 1260 padded grid, 2 of the 32 shots,
+    the first 150 steps, 8th order, imaging fields cached in the benchmark's
+    format (all 150 steps fit) and fp32 checkpoints, as timed.  The adjoint
+    source is a seeded random residual (loss = sum(res * p))."""
+    from oracle import oracle as orc
+    kw, damp = _one_shot_kwargs(torch, wave, w, dev, list(shots), nt)
+    res = np.random.default_rng(11).standard_normal((len(shots), nt, w.rcv_x.size)).astype(np.float32)
+    vp = torch.tensor(w.vp, device=dev, requires_grad=True)
+    out = wave.acoustic_forward_kernel(vp=vp, imaging_dtype=imaging_dtype, **kw)
+    (out["p"] * torch.tensor(res, device=dev)).sum().backward()
+    okw = _oracle_kwargs(kw, w, damp, nt)
+    t0 = time.perf_counter()
+    ref = orc.forward(**okw, dtype=np.float64)
+    gref, _, _ = orc.gradient(**okw, res_p=res.astype(np.float64), dtype=np.float64)
+    return {"trace_rel_l2_vs_fp64_oracle": _rel(out["p"].detach().cpu().numpy(), ref["p"]),
+            "rel_l2_vs_fp64_oracle": _rel(vp.grad.cpu().numpy(), gref),
+            "oracle_case": f"{w.nz}x{w.nx} grid, shots {list(shots)}, {nt} steps, order {w.fd_order}, "
+                           f"{imaging_dtype} imaging cache, fp32 checkpoints; adjoint source seeded N(0,1)",
+            "oracle_seconds": time.perf_counter() - t0, "oracle_threads": orc.max_threads()}
+
+
+def large_gradient_check(torch, wave, synthetic, dev, K, formats, shot=7):
+    """Gradient error of the memory-capped 1000 x 3000 configuration, untimed:
+    the full 1080 x 3080 padded grid, one shot, 2K + 8 steps with the real
+    run's segment length K and no imaging cache, so the adjoint restarts
+    twice from stored snapshots (fp24 imaging fields, as in the timed run).
+    Each snapshot format is compared with the fp32-snapshot run of the same
+    problem and with the float64 C oracle.  Adjoint source: a seeded random
+    residual."""
+    from oracle import oracle as orc
+    nt = 2 * K + 8
+    w = synthetic.large_1000x3000(nt=nt)
+    kw, damp = _one_shot_kwargs(torch, wave, w, dev, [shot], nt)
+    res = np.random.default_rng(12).standard_normal((1, nt, w.rcv_x.size)).astype(np.float32)
+    res_d = torch.tensor(res, device=dev)
+
+    def grad(fmt):
+        vp = torch.tensor(w.vp, device=dev, requires_grad=True)
+        out = wave.acoustic_forward_kernel(vp=vp, checkpoint_every=K, snapshot_dtype=fmt, imaging_cache=0,
+                                           imaging_dtype="fp24", **kw)
+        (out["p"] * res_d).sum().backward()
+        return vp.grad.cpu().numpy()
+
+    g = {fmt: grad(fmt) for fmt in ("fp32",) + tuple(formats)}
+    t0 = time.perf_counter()
+    gref, _, _ = orc.gradient(**_oracle_kwargs(kw, w, damp, nt), res_p=res.astype(np.float64), dtype=np.float64)
+    out = {"case": f"{w.nz}x{w.nx} grid, shot {shot}, {nt} steps, checkpoint_every {K} (2 restarts), "
+                   f"fp24 imaging, no cache; adjoint source seeded N(0,1)",
+           "oracle_seconds": time.perf_counter() - t0, "oracle_threads": orc.max_threads(),
+           "fp32_snapshots_rel_l2_vs_fp64_oracle": _rel(g["fp32"], gref)}
+    for fmt in formats:
+        out[fmt] = {"rel_l2_vs_fp32_snapshots": _rel(g[fmt], g["fp32"]), "rel_l2_vs_fp64_oracle": _rel(g[fmt], gref)}
+    return out
+
+
 def run_reference_arm(args):
     """--impl reference: the reference algorithm's CPU restatement on the host
     cores, same metric and config, bounded sample per step."""
@@ -341,6 +422,8 @@ def main():
                                                   torch.linalg.vector_norm(g_ref)),
                   "reference_path": "fp32 checkpoints, fp32 recompute of every step, no imaging cache"}
     del g_fast, g_ref
+    if rank == 0 and world == 1:
+        grad_check.update(oracle_check_fwi(torch, wave, w, dev, args.imaging_dtype))
 
     extras = {}
     if not args.no_extras and world == 1:
@@ -383,7 +466,10 @@ def main():
 def plain_forward_rates(torch, wave, synthetic, dev):
     """Plain forward kernel rates beside the gradient: the 400 x 1200 grid
     with one shot and with 32 shots (damping layers, and the CPML option),
-    and the 100 x 200 4th-order workload."""
+    and the 100 x 200 4th-order workload.  Roofline fraction at the damping
+    scheme's algorithmic bytes, 24 + 8 / shots per unit (the CPML option
+    moves more in its layers)."""
+    peak, _ = measured_peaks()
     out = {}
     for name, w, absorbing in (("fwd_400x1200_1shot", synthetic.fwi_400x1200(nt=3000, n_shots=1), "damping"),
                                ("fwd_400x1200_32shots", synthetic.fwi_400x1200(nt=1000), "damping"),
@@ -407,8 +493,12 @@ def plain_forward_rates(torch, wave, synthetic, dev):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / reps
-        out[name] = {"gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms,
-                     "fd_order": w.fd_order, "nt": w.nt, "shots": w.n_shots, "absorbing": absorbing}
+        rate = w.cell_updates() / (ms * 1e-3) / 1e9
+        # p, vx, vz read and written once per step; a1, a2 read once per shot group
+        b_unit = 24 + 8 / w.n_shots
+        out[name] = {"gcell_updates_per_s": rate, "ms": ms, "fd_order": w.fd_order, "nt": w.nt,
+                     "shots": w.n_shots, "absorbing": absorbing, "bytes_per_unit": b_unit,
+                     "achieved_gbs": rate * b_unit, "frac": rate * b_unit / peak}
     return out
 
 
@@ -480,11 +570,26 @@ def reference_gpu_rates(torch, wave, synthetic, dev, nt=100, segments=4):
         (0.5 * (r * r).sum()).backward()
 
     ms_f, ms_g = _timed(torch, fwd, 2), _timed(torch, grad, 1)
+
+    # this library on the identical inputs and order, through the same call
+    def fwd_b200():
+        with torch.no_grad():
+            wave.acoustic_forward_kernel(vp=vp, **kw)
+
+    def grad_b200():
+        v = vp.clone().requires_grad_(True)
+        r = wave.acoustic_forward_kernel(vp=v, checkpoint_segments=segments, **kw)["p"] - d_obs
+        (0.5 * (r * r).sum()).backward()
+
+    ms_fb, ms_gb = _timed(torch, fwd_b200, 2), _timed(torch, grad_b200, 2)
     return {"reference_pytorch_gpu": {
         "forward_gcell_updates_per_s": units / (ms_f * 1e-3) / 1e9, "forward_ms": ms_f,
         "gradient_gcell_updates_per_s": units / (ms_g * 1e-3) / 1e9, "gradient_ms": ms_g,
         "nt": nt, "shots": S, "fd_order": 4, "checkpoint_segments": segments,
-        "sample": "400x1200 grid, 30-cell PML, 32 shots, nt truncated to 100 (the reference has no 8th order)"}}
+        "sample": "400x1200 grid, 30-cell PML, 32 shots, nt truncated to 100 (the reference has no 8th order)",
+        "b200_same_inputs": {"forward_gcell_updates_per_s": units / (ms_fb * 1e-3) / 1e9, "forward_ms": ms_fb,
+                             "gradient_gcell_updates_per_s": units / (ms_gb * 1e-3) / 1e9, "gradient_ms": ms_gb,
+                             "fd_order": 4, "note": "acoustic_forward_kernel of this library, same arguments"}}}
 
 
 def _model_kwargs(torch, wave, w, dev, vp=None):
@@ -515,6 +620,8 @@ def batch_rates(torch, wave, synthetic, dev):
     (128 x 256 .. 512 x 1024, 1000 .. 3000 steps, 4 .. 16 shots), forward
     and gradient (fwd + adjoint of 0.5 ||p||^2, fp24 imaging cache within
     the free memory, checkpoints for the rest)."""
+    from geobrain_b200.wave import engine
+    peak, _ = measured_peaks()
     out = {}
     for name, ws in (("ensemble_256x512_50particles", synthetic.ensemble_256x512()),
                      ("uneven_batch_24models", synthetic.uneven_batch())):
@@ -534,17 +641,39 @@ def batch_rates(torch, wave, synthetic, dev):
 
         ms_f = _timed(torch, fwd)
         ms_g = _timed(torch, grad)
+        # the batch records its phases on the plan of its first model
+        w0 = ws[0]
+        plan0 = engine.get_plan(engine.Geometry(w0.nz, w0.nx, w0.nabc, w0.nt, float(w0.dt), float(w0.dx), 4, False),
+                                w0.src_x, w0.src_z, w0.rcv_x, w0.rcv_z)
+        plan0.set_profiling(True)
+        grad()
+        prof = plan0.profile()
+        plan0.set_profiling(False)
+        b_grad = sum(w.cell_updates() * (56 + 16 / w.n_shots) for w in ws)
+        b_fwd = sum(w.cell_updates() * (24 + 8 / w.n_shots) for w in ws)
         out[name] = {"forward_gcell_updates_per_s": units / (ms_f * 1e-3) / 1e9, "forward_ms": ms_f,
+                     "forward_frac": b_fwd / (ms_f * 1e-3) / 1e9 / peak,
                      "gradient_gcell_updates_per_s": units / (ms_g * 1e-3) / 1e9, "gradient_ms": ms_g,
+                     "gradient_frac": b_grad / (ms_g * 1e-3) / 1e9 / peak,
+                     "gradient_phase_ms": {k: prof[k] for k in ("forward_ms", "recompute_ms", "adjoint_ms")},
+                     "gradient_phase_steps": {k: prof[k] for k in ("forward_steps", "recompute_steps",
+                                                                   "adjoint_steps")},
+                     "gradient_launches": prof["launches"],
                      "models": len(ws), "cell_updates": units, "launch": "batched (one launch per step)"}
     return out
 
 
-def large_gradient_rate(torch, wave, synthetic, dev, cap_bytes=60 * 10**9):
+# snapshot format of the memory-capped run: 16 bits with one scale per
+# snapshot field (fp16 keeps 11 significant bits; bf16's 8 miss the 1e-3 bar)
+LARGE_SNAPSHOTS = "fp16"
+
+
+def large_gradient_rate(torch, wave, synthetic, dev, cap_bytes=60 * 10**9, snapshot_dtype=LARGE_SNAPSHOTS):
     """1000 x 3000 (1080 x 3080 padded), 16 shots, 8000 steps, 8th order:
-    gradient within a 60 GB device-memory cap, with bf16 checkpoints (one
-    scale per snapshot), fp24 imaging fields, and as many cached steps as the
-    cap leaves room for."""
+    gradient within a 60 GB device-memory cap, with 16-bit checkpoints (one
+    scale per snapshot field), fp24 imaging fields, and as many cached steps
+    as the cap leaves room for; then, untimed, the gradient error of that
+    storage on a truncated problem with the same segment length."""
     w = synthetic.large_1000x3000()
     kw = _model_kwargs(torch, wave, w, dev)
     kw.pop("vp")
@@ -557,7 +686,8 @@ def large_gradient_rate(torch, wave, synthetic, dev, cap_bytes=60 * 10**9):
     def grad():
         vp = vp0.detach().requires_grad_(True)
         out = wave.acoustic_forward_kernel(vp=vp, **kw, device=dev, fd_order=8, want_energy=False,
-                                           snapshot_dtype="bf16", imaging_dtype="fp24", memory_budget=cap_bytes)
+                                           snapshot_dtype=snapshot_dtype, imaging_dtype="fp24",
+                                           memory_budget=cap_bytes)
         (0.5 * (out["p"] * out["p"]).sum()).backward()
         return vp.grad
 
@@ -565,11 +695,17 @@ def large_gradient_rate(torch, wave, synthetic, dev, cap_bytes=60 * 10**9):
     peak = torch.cuda.max_memory_allocated(dev) - base
     geo = engine.Geometry(w.nz, w.nx, w.nabc, w.nt, float(w.dt), float(w.dx), 4, False)
     plan = engine.get_plan(geo, w.src_x, w.src_z, w.rcv_x, w.rcv_z)
-    K = engine.choose_checkpoint_every(plan, 1, 0, "bf16", False, "fp24")
+    K = engine.choose_checkpoint_every(plan, 1, 0, snapshot_dtype, False, "fp24")
+    del kw, vp0
+    torch.cuda.empty_cache()
+    check = large_gradient_check(torch, wave, synthetic, dev, K, (snapshot_dtype,) + tuple(
+        f for f in ("fp24", "bf16", "fp16") if f != snapshot_dtype))
     return {"large_1000x3000_16shots_gradient": {
         "gcell_updates_per_s": w.cell_updates() / (ms * 1e-3) / 1e9, "ms": ms, "nt": w.nt, "shots": w.n_shots,
         "memory_cap_bytes": cap_bytes, "peak_bytes_above_inputs": int(peak), "checkpoint_every": K,
-        "checkpoints": "bf16, one scale per (checkpoint, shot, field)", "imaging": "fp24"}}
+        "checkpoints": f"{snapshot_dtype}, one scale per (checkpoint, shot, field)" if snapshot_dtype in
+        ("fp16", "bf16") else snapshot_dtype, "imaging": "fp24",
+        "gradient_check": check}}
 
 
 def rates_3d(torch, wave, dev, nz=200, ny=200, nx=200, shots=4, nt=200, nabc=20):

@@ -19,7 +19,7 @@ GB_E_WORKSPACE = -3
 GB_E_TIMEOUT = -4
 GB_E_UNSUPPORTED = -5
 
-CKPT_FORMATS = {"fp32": 0, "bf16": 1, "fp16": 2}
+CKPT_FORMATS = {"fp32": 0, "bf16": 1, "fp16": 2, "fp24": 3}
 IMAGING_FORMATS = {"fp32": 0, "bf16": 1, "fp24": 3}
 
 

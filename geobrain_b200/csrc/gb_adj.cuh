@@ -370,8 +370,9 @@ constexpr size_t adj_smem_bytes()
 //   G1 = sum(mu_p1 * I), G2 = sum(mu_v1 * J) over groups (compensated),
 //   dL/dc = 2 G1 / c, dL/dden = (G1 + G2) / den,
 // then the adjoint of pad_model: each model cell collects every padded cell
-// it was replicated into (acoustic_2d.py:55-64).
-__global__ void grad_finish_kernel(const float *__restrict__ vp, const float *__restrict__ rho,
+// it was replicated into (acoustic_2d.py:55-64).  Internal linkage: the
+// translation units that instantiate the step kernels include this header too.
+static __global__ void grad_finish_kernel(const float *__restrict__ vp, const float *__restrict__ rho,
                                    const float *__restrict__ G1, const float *__restrict__ C1,
                                    const float *__restrict__ G2, const float *__restrict__ C2, int n_groups,
                                    long long plane, int nz, int nx, int pml, int pitch, float *grad_vp,

@@ -118,6 +118,24 @@ __global__ void unpack16_kernel(const H *__restrict__ in, const float *__restric
         o[i] = from_h(p[i]) * scale;
 }
 
+// Checkpoint snapshots in 24 bits: the upper 24 bits of each fp32 (sign,
+// exponent, 15-bit mantissa) rounded to nearest even, 4 values to 3 words,
+// the same packing as the fp24 imaging fields.  The exponent is kept, so no
+// scale is needed; the relative error of each value is at most 2^-16.
+__global__ void pack24_kernel(const float *__restrict__ x, long long n4, float *__restrict__ out)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4;
+         i += (long long)gridDim.x * blockDim.x)
+        store_img4(out, 4 * i, kImgF24, ldg4(x + 4 * i));
+}
+
+__global__ void unpack24_kernel(const float *__restrict__ in, long long n4, float *__restrict__ x)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n4;
+         i += (long long)gridDim.x * blockDim.x)
+        stg4(x + 4 * i, decode_img4(load_img_raw(in, 4 * i, kImgF24), kImgF24));
+}
+
 // Self-test of the bounded waits.  One CTA waits on an mbarrier of arrival
 // count 2.  The second arrival is made only when `complete` is set, so
 // otherwise the phase never completes: the wait gives up after max_polls

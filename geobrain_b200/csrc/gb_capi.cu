@@ -1,6 +1,8 @@
 // C ABI of the B200 acoustic propagator (declared in include/geobrain_b200.h):
 // plans, workspace layout, TMA descriptors and the host-side time loops.
 #include "gb_host.h"
+#include "gb_kernels.h"
+#include "gb_symcache.h"
 
 #include "gb_adj.cuh"
 #include "gb_aux.cuh"
@@ -24,6 +26,7 @@ using namespace gb;
 using gb::host::align256;
 using gb::host::aligned_ws;
 using gb::host::fail;
+using namespace gb::host;
 
 namespace {
 thread_local std::string g_last_error;   // gb_last_error(): the message of this thread's last failure
@@ -337,91 +340,26 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
     return L;
 }
 
-template <int R, int TZ, bool FS, bool EN, int IMG>
-void *fwd_fn()
-{
-    return reinterpret_cast<void *>(&fwd_step_kernel<R, TZ, FS, EN, IMG>);
-}
-
-template <int R, int TZ, bool FS>
-void *fwd_pick_fs(bool en, int img)
-{
-    if (img == 1) return en ? fwd_fn<R, TZ, FS, true, 1>() : fwd_fn<R, TZ, FS, false, 1>();
-    if (img == 2) return en ? fwd_fn<R, TZ, FS, true, 2>() : fwd_fn<R, TZ, FS, false, 2>();
-    return en ? fwd_fn<R, TZ, FS, true, 0>() : fwd_fn<R, TZ, FS, false, 0>();
-}
-
-template <int R, int TZ>
-void *fwd_pick3(bool fs, bool en, int img)
-{
-    return fs ? fwd_pick_fs<R, TZ, true>(en, img) : fwd_pick_fs<R, TZ, false>(en, img);
-}
-
-struct StepKernel {
-    void *fn;
-    size_t smem;
-    bool stream = false;    // fwd_stream_kernel: launched over (strip, segment, shot)
-};
-
-template <int R>
-void *fwd_stream_pick(bool en, int img)
-{
-    if (img == 1) return en ? (void *)&fwd_stream_kernel<R, true, 1> : (void *)&fwd_stream_kernel<R, false, 1>;
-    if (img == 2) return en ? (void *)&fwd_stream_kernel<R, true, 2> : (void *)&fwd_stream_kernel<R, false, 2>;
-    return en ? (void *)&fwd_stream_kernel<R, true, 0> : (void *)&fwd_stream_kernel<R, false, 0>;
-}
-
 // The plan's forward step kernel: the streaming one when the plan asks for it
 // (no free surface, 16-row tiles), else the tile kernel.
-StepKernel fwd_kernel(int R, int tz, bool fs, bool en, int im);
-StepKernel fwd_kernel_for(const gb_plan *P, bool en, int im)
-{
-    if (P->stream_usable()) {
-        StepKernel k{P->R == 2 ? fwd_stream_pick<2>(en, im) : fwd_stream_pick<4>(en, im), kStreamSmemBytes, true};
-        return k;
-    }
-    return fwd_kernel(P->R, P->tz, P->d.free_surface != 0, en, im);
-}
-
 StepKernel fwd_kernel(int R, int tz, bool fs, bool en, int im)
 {
-    StepKernel k{nullptr, 0};
-    if (R == 2 && tz == 32) { k.fn = fwd_pick3<2, 32>(fs, en, im); k.smem = fwd_smem_bytes<2, 32>(); }
-    if (R == 2 && tz == 16) { k.fn = fwd_pick3<2, 16>(fs, en, im); k.smem = fwd_smem_bytes<2, 16>(); }
-    if (R == 4 && tz == 32) { k.fn = fwd_pick3<4, 32>(fs, en, im); k.smem = fwd_smem_bytes<4, 32>(); }
-    if (R == 4 && tz == 16) { k.fn = fwd_pick3<4, 16>(fs, en, im); k.smem = fwd_smem_bytes<4, 16>(); }
-    return k;
+    if (R == 2) return fwd_tile_kernel_r2(tz, fs, en, im);
+    if (R == 4) return fwd_tile_kernel_r4(tz, fs, en, im);
+    return StepKernel{};
 }
 
-template <int R, int TZ, int IMGF>
-void *adj_pick_f(bool fs, bool rho)
+StepKernel fwd_kernel_for(const gb_plan *P, bool en, int im)
 {
-    if (fs) return rho ? reinterpret_cast<void *>(&adj_step_kernel<R, TZ, true, true, IMGF>)
-                       : reinterpret_cast<void *>(&adj_step_kernel<R, TZ, true, false, IMGF>);
-    return rho ? reinterpret_cast<void *>(&adj_step_kernel<R, TZ, false, true, IMGF>)
-               : reinterpret_cast<void *>(&adj_step_kernel<R, TZ, false, false, IMGF>);
-}
-
-// The default 16-row tiles get one kernel per imaging format (the loads are
-// issued early, ahead of the stage wait, and a format switch there costs);
-// the 32-row tiles read the format at run time.
-template <int R, int TZ>
-void *adj_pick(bool fs, bool rho, int img_fmt)
-{
-    if (TZ != 16) return adj_pick_f<R, TZ, -1>(fs, rho);
-    if (img_fmt == GB_IMG_BF16) return adj_pick_f<R, TZ, kImgBF16>(fs, rho);
-    if (img_fmt == GB_IMG_F24) return adj_pick_f<R, TZ, kImgF24>(fs, rho);
-    return adj_pick_f<R, TZ, kImgF32>(fs, rho);
+    if (P->stream_usable()) return fwd_stream_kernel_for(P->R, en, im);
+    return fwd_kernel(P->R, P->tz, P->d.free_surface != 0, en, im);
 }
 
 StepKernel adj_kernel(int R, int tz, bool fs, bool rho, int img_fmt)
 {
-    StepKernel k{nullptr, 0};
-    if (R == 2 && tz == 32) { k.fn = adj_pick<2, 32>(fs, rho, img_fmt); k.smem = adj_smem_bytes<2, 32>(); }
-    if (R == 2 && tz == 16) { k.fn = adj_pick<2, 16>(fs, rho, img_fmt); k.smem = adj_smem_bytes<2, 16>(); }
-    if (R == 4 && tz == 32) { k.fn = adj_pick<4, 32>(fs, rho, img_fmt); k.smem = adj_smem_bytes<4, 32>(); }
-    if (R == 4 && tz == 16) { k.fn = adj_pick<4, 16>(fs, rho, img_fmt); k.smem = adj_smem_bytes<4, 16>(); }
-    return k;
+    if (R == 2) return adj_tile_kernel_r2(tz, fs, rho, img_fmt);
+    if (R == 4) return adj_tile_kernel_r4(tz, fs, rho, img_fmt);
+    return StepKernel{};
 }
 
 int prepare_kernel(const StepKernel &k)
@@ -643,7 +581,9 @@ size_t ck16_bytes(const gb_plan *p) { return align256((size_t)p->d.n_shots * 3 *
 size_t ck_scale_bytes(const gb_plan *p) { return align256((size_t)p->d.n_shots * 3 * 4); }
 size_t ck_bytes(const gb_plan *p, int fmt)
 {
-    return fmt == GB_CKPT_F32 ? (size_t)p->d.n_shots * 3 * p->plane * 4 : ck16_bytes(p) + ck_scale_bytes(p);
+    if (fmt == GB_CKPT_F32) return (size_t)p->d.n_shots * 3 * p->plane * 4;
+    if (fmt == GB_CKPT_F24) return align256((size_t)p->d.n_shots * 3 * p->plane * 3);
+    return ck16_bytes(p) + ck_scale_bytes(p);
 }
 
 // Save shots [s0, s0 + ns) of `state` into checkpoint k.
@@ -656,6 +596,14 @@ int save_checkpoint(gb_plan *P, const float *state, void *ckpts, int k, int fmt,
     if (fmt == GB_CKPT_F32) {
         GB_CUDA(cudaMemcpyAsync(base + (size_t)s0 * 3 * pl * 4, src, (size_t)ns * 3 * pl * 4, cudaMemcpyDeviceToDevice,
                                 st));
+        return GB_OK;
+    }
+    if (fmt == GB_CKPT_F24) {
+        // plane is a multiple of 32, so every shot's block starts on a 4-value group
+        pack24_kernel<<<4 * 148, 256, 0, st>>>(src, (long long)ns * 3 * pl / 4,
+                                               reinterpret_cast<float *>(base + (size_t)s0 * 3 * pl * 3));
+        GB_CUDA(cudaGetLastError());
+        ++P->launches;
         return GB_OK;
     }
     float *scales = reinterpret_cast<float *>(base + ck16_bytes(P)) + 3 * s0;
@@ -682,6 +630,13 @@ int restore_checkpoint(gb_plan *P, float *state, const void *ckpts, int k, int f
     if (fmt == GB_CKPT_F32) {
         GB_CUDA(cudaMemcpyAsync(dst, base + (size_t)s0 * 3 * pl * 4, (size_t)ns * 3 * pl * 4, cudaMemcpyDeviceToDevice,
                                 st));
+        return GB_OK;
+    }
+    if (fmt == GB_CKPT_F24) {
+        unpack24_kernel<<<4 * 148, 256, 0, st>>>(reinterpret_cast<const float *>(base + (size_t)s0 * 3 * pl * 3),
+                                                 (long long)ns * 3 * pl / 4, dst);
+        GB_CUDA(cudaGetLastError());
+        ++P->launches;
         return GB_OK;
     }
     const float *scales = reinterpret_cast<const float *>(base + ck16_bytes(P)) + 3 * s0;
@@ -762,7 +717,7 @@ int check_store(const gb_plan *P, const gb_grad_store *store)
 {
     if (!store) return GB_OK;
     if (store->checkpoint_every < 1) return fail(GB_E_ARG, "checkpoint_every must be >= 1");
-    if (store->format < GB_CKPT_F32 || store->format > GB_CKPT_F16) return fail(GB_E_ARG, "unknown checkpoint format");
+    if (store->format < GB_CKPT_F32 || store->format > GB_CKPT_F24) return fail(GB_E_ARG, "unknown checkpoint format");
     if (store->cached_steps < 0 || store->cached_steps > P->d.nt) return fail(GB_E_ARG, "cached_steps out of range");
     if (store->cached_steps > 0 && !store->imaging) return fail(GB_E_ARG, "cached_steps > 0 needs an imaging buffer");
     if (!img_format_ok(store->imaging_format))
@@ -1050,7 +1005,7 @@ size_t gb_plan_gradient_workspace_bytes(const gb_plan *p, int with_rho, int segm
 
 size_t gb_plan_checkpoint_bytes(const gb_plan *p, int checkpoint_every, int ckpt_format)
 {
-    if (!p || checkpoint_every < 1) return 0;
+    if (!p || checkpoint_every < 1 || ckpt_format < GB_CKPT_F32 || ckpt_format > GB_CKPT_F24) return 0;
     const size_t n_ck = (p->d.nt + checkpoint_every - 1) / checkpoint_every;
     return n_ck * ck_bytes(p, ckpt_format);
 }
@@ -1551,48 +1506,6 @@ int gb_plan_profile(gb_plan *P, double *ms_forward, double *ms_recompute, double
 // ---------------------------------------------------------------------------
 namespace {
 
-template <int R, bool FS, bool EN, int IMG>
-void *fwd_batch_fn()
-{
-    return reinterpret_cast<void *>(&fwd_batch_kernel<R, 16, FS, EN, IMG>);
-}
-
-template <int R, bool FS>
-void *fwd_batch_pick(bool en, int img)
-{
-    if (img == 1) return en ? fwd_batch_fn<R, FS, true, 1>() : fwd_batch_fn<R, FS, false, 1>();
-    if (img == 2) return en ? fwd_batch_fn<R, FS, true, 2>() : fwd_batch_fn<R, FS, false, 2>();
-    return en ? fwd_batch_fn<R, FS, true, 0>() : fwd_batch_fn<R, FS, false, 0>();
-}
-
-StepKernel fwd_batch_kernel_for(int R, bool fs, bool en, int img)
-{
-    StepKernel k{nullptr, 0};
-    if (R == 2) {
-        k.fn = fs ? fwd_batch_pick<2, true>(en, img) : fwd_batch_pick<2, false>(en, img);
-        k.smem = fwd_smem_bytes<2, 16>();
-    } else if (R == 4) {
-        k.fn = fs ? fwd_batch_pick<4, true>(en, img) : fwd_batch_pick<4, false>(en, img);
-        k.smem = fwd_smem_bytes<4, 16>();
-    }
-    return k;
-}
-
-StepKernel adj_batch_kernel_for(int R, bool fs, bool rho)
-{
-    StepKernel k{nullptr, 0};
-    if (R == 2) {
-        k.fn = fs ? (rho ? (void *)&adj_batch_kernel<2, 16, true, true> : (void *)&adj_batch_kernel<2, 16, true, false>)
-                  : (rho ? (void *)&adj_batch_kernel<2, 16, false, true> : (void *)&adj_batch_kernel<2, 16, false, false>);
-        k.smem = adj_smem_bytes<2, 16>();
-    } else if (R == 4) {
-        k.fn = fs ? (rho ? (void *)&adj_batch_kernel<4, 16, true, true> : (void *)&adj_batch_kernel<4, 16, true, false>)
-                  : (rho ? (void *)&adj_batch_kernel<4, 16, false, true> : (void *)&adj_batch_kernel<4, 16, false, false>);
-        k.smem = adj_smem_bytes<4, 16>();
-    }
-    return k;
-}
-
 struct BatchLayout {
     size_t models, maps, items, total;
     long long n_items;
@@ -1949,9 +1862,43 @@ namespace {
 constexpr size_t kStaticScratchBytes = size_t(64) << 20;   // 64 MiB per device
 __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_static_scratch_mutex;
-void *g_static_scratch_addr[kMaxDevices] = {};
+// the array's device address per (device, context); see gb_symcache.h
+gb::host::SymbolAddressCache<16> g_static_scratch_addr;
+
+// The unique ID of the calling thread's current context (cuCtxGetCurrent and
+// cuCtxGetId through the runtime's driver entry points, so that the library
+// needs no link dependency on libcuda).  A thread with no current context
+// gets the device's primary context made current first (cudaSetDevice); a
+// context the host made current is used as it is.
+using PFN_ctx_current = CUresult (*)(CUcontext *);
+using PFN_ctx_id = CUresult (*)(CUcontext, unsigned long long *);
+PFN_ctx_current g_ctx_current = nullptr;
+PFN_ctx_id g_ctx_id = nullptr;
+std::once_flag g_ctx_once;
+
+int current_context_id(int dev, unsigned long long *id)
+{
+    std::call_once(g_ctx_once, [] {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess) {
+            g_ctx_current = reinterpret_cast<PFN_ctx_current>(a);
+            g_ctx_id = reinterpret_cast<PFN_ctx_id>(b);
+        }
+    });
+    if (!g_ctx_current || !g_ctx_id) return fail(GB_E_CUDA, "cuCtxGetCurrent / cuCtxGetId unavailable");
+    CUcontext ctx = nullptr;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS) return fail(GB_E_CUDA, "cuCtxGetCurrent failed");
+    if (!ctx) {
+        GB_CUDA(cudaSetDevice(dev));
+        if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return fail(GB_E_CUDA, "no current CUDA context");
+    }
+    if (g_ctx_id(ctx, id) != CUDA_SUCCESS) return fail(GB_E_CUDA, "cuCtxGetId failed");
+    return GB_OK;
+}
 
 }  // namespace
 
@@ -1964,28 +1911,29 @@ extern "C" int gb_forward_static_scratch(gb_plan *P, const float *vp, const floa
 {
     g_last_error.clear();
     if (!P) return fail(GB_E_ARG, "null plan");
-    const size_t need = gb_plan_workspace_bytes(P, 0, 0);
+    // the array is 256-byte aligned, so gb_forward needs no alignment slack in it
+    const size_t need = layout(P).total;
     if (need > kStaticScratchBytes)
         return fail(GB_E_WORKSPACE, "this model needs " + std::to_string(need) +
                                         " bytes of scratch; the static scratch holds " +
                                         std::to_string(kStaticScratchBytes) + " bytes (use gb_forward with a workspace)");
     int dev = -1;
     GB_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return fail(GB_E_ARG, "device ordinal out of range");
+    unsigned long long ctx_id = 0;
+    if (int rc = current_context_id(dev, &ctx_id)) return rc;
+    // first call on this device and context: look the array's device address
+    // up, with the device current (the host-side symbol is not a device address)
     void *scratch = nullptr;
-    {
-        // first call on this device: look the array's device address up once,
-        // with this device current (the host-side symbol is not a device address)
-        std::lock_guard<std::mutex> lock(g_static_scratch_mutex);
-        if (!g_static_scratch_addr[dev]) {
-            void *addr = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&addr, g_static_scratch);
-            if (e != cudaSuccess)
-                return fail(GB_E_CUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
-            g_static_scratch_addr[dev] = addr;
-        }
-        scratch = g_static_scratch_addr[dev];
-    }
+    if (int rc = g_static_scratch_addr.get(dev, ctx_id,
+                                           [](void **addr) {
+                                               cudaError_t e = cudaGetSymbolAddress(addr, g_static_scratch);
+                                               if (e == cudaSuccess) return 0;
+                                               return fail(GB_E_CUDA,
+                                                           std::string("cudaGetSymbolAddress(static scratch): ") +
+                                                               cudaGetErrorString(e));
+                                           },
+                                           &scratch))
+        return rc;
     // gb_forward clears every part of the scratch that must start at zero
     // (both wavefield time levels, the energy sums, the status word).  It
     // runs with one launch per step: instantiating a CUDA graph would make

@@ -348,8 +348,8 @@ class AcousticFunction(torch.autograd.Function):
     """Traces (p, vx, vz) as a differentiable function of (vp, rho) and of
     the source wavelets src_v.
 
-    forward: gb_forward keeping checkpoints every K steps (fp32, or bf16 /
-    fp16 with per-snapshot scales) and the imaging fields of the last
+    forward: gb_forward keeping checkpoints every K steps (fp32, fp24, or
+    bf16 / fp16 with per-snapshot scales) and the imaging fields of the last
     time steps that fit the cache budget; backward: gb_backward (adjoint with
     the imaging condition, fp32 recompute of the uncached segments), in place
     of autograd through ~40 ops per step

@@ -10,8 +10,9 @@ adjoint (engine.AcousticFunction); the energy maps are detached, as in the
 reference.
 
 Additions, all keyword-only with defaults that keep the reference's
-behaviour: fd_order (4 or 8); checkpoint_every, snapshot_dtype ('fp32',
-'bf16', 'fp16'), imaging_cache ('auto', 'all', a byte budget, or 0) and
+behaviour: fd_order (4 or 8); checkpoint_every, snapshot_dtype ('fp32';
+'fp24', 3 bytes, gradient error about 1e-5; 'fp16' and 'bf16', 2 bytes with
+one scale per snapshot field, about 6e-4 and 5e-3), imaging_cache ('auto', 'all', a byte budget, or 0) and
 imaging_dtype ('fp32'; 'fp24', 3 bytes, gradient error about 1e-5; 'bf16',
 2 bytes, about 3e-3: more cached steps skip the recompute) for the
 gradient's memory, and memory_budget (bytes the gradient's store and

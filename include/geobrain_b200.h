@@ -51,6 +51,8 @@ typedef struct gb_model_desc {
 #define GB_CKPT_F32   0
 #define GB_CKPT_BF16  1   /* bf16 with one fp32 scale per (checkpoint, shot, field) */
 #define GB_CKPT_F16   2   /* fp16 with one fp32 scale per (checkpoint, shot, field) */
+#define GB_CKPT_F24   3   /* upper 24 bits of the fp32 (15-bit mantissa, fp32 exponent,
+                             no scale), 3 bytes per value */
 
 /* Storage formats of the imaging cache.  Both short formats keep the fp32
  * exponent (no scale) and round to nearest even:
@@ -181,7 +183,8 @@ size_t gb_plan_workspace_bytes(const gb_plan *plan, int with_gradient, int check
 size_t gb_plan_gradient_workspace_bytes(const gb_plan *plan, int with_rho, int segment_steps,
                                         int imaging_format);
 
-/* Bytes of checkpoint storage for a given segment length and format. */
+/* Bytes of checkpoint storage for a given segment length and format (0 for
+ * an unknown format). */
 size_t gb_plan_checkpoint_bytes(const gb_plan *plan, int checkpoint_every, int ckpt_format);
 
 /* Bytes of the imaging cache for the last cached_steps time steps
@@ -306,11 +309,14 @@ int gb_selftest_bounded_wait(void *workspace, size_t workspace_bytes, int32_t co
  * no allocation hook).  Limits and behaviour:
  *   - the array is gb_static_scratch_bytes() (64 MiB) on every GPU that
  *     loads the library, held until the process exits; a model whose
- *     gb_plan_workspace_bytes(plan, 0, 0) exceeds it is rejected with
- *     GB_E_WORKSPACE;
- *   - the first call on each device looks the array's device address up
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture;
+ *     scratch (gb_plan_workspace_bytes(plan, 0, 0) less its 256 bytes of
+ *     alignment slack, which the aligned array does not need) exceeds it is
+ *     rejected with GB_E_WORKSPACE;
+ *   - the first call on each device and CUDA context looks the array's
+ *     device address up (cudaGetSymbolAddress) with that device current, so
+ *     a new context (after cudaDeviceReset, or one the host created) gets
+ *     its own module's address; make that first call before any stream
+ *     capture;
  *   - every call shares the one array per device: calls whose work overlaps
  *     on the GPU (other streams, other threads) race and corrupt each other;
  *   - it calls no cudaMalloc / cudaFree; inputs and outputs are the caller's;

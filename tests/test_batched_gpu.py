@@ -97,3 +97,35 @@ def test_ensemble_log_likelihood_matches_per_particle_loop(cuda_device):
         li.backward()
         assert abs(float(ll[i]) - float(li.detach())) <= 1e-5 * abs(float(li.detach()))
         assert orc.rel_l2(grad[i].reshape(c["nz"], c["nx"]).cpu().numpy(), t.grad.cpu().numpy()) < 1e-5
+
+
+def test_ensemble_256x512_batched_matches_fp64_oracle(cuda_device):
+    """Three particles of the 256 x 512 ensemble workload (8th order, 20-cell
+    PML), two shots each, 300 steps, through the batched engine with the
+    fp24 imaging cache the benchmark uses: traces of every particle against
+    the float64 oracle to 1e-5 and each particle's dL/dvp to 1e-4."""
+    from geobrain_b200 import synthetic, wave
+    ws = synthetic.ensemble_256x512(n_particles=3, nt=300)
+    shots = [1, 6]
+    rng = np.random.default_rng(3)
+    models, cases, lins = [], [], []
+    for w in ws:
+        damp = wave.bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp.max()), False).astype(np.float32)
+        c = dict(nx=w.nx, nz=w.nz, dx=w.dx, nt=w.nt, dt=w.dt, nabc=w.nabc, free_surface=False,
+                 src_x=w.src_x[shots], src_z=w.src_z[shots], src_v=np.tile(w.wavelet, (2, 1)).astype(np.float32),
+                 rcv_x=w.rcv_x, rcv_z=w.rcv_z, damp=damp, vp=w.vp, rho=w.rho)
+        cases.append(c)
+        models.append(model_dict(c, cuda_device, requires_grad=True))
+        lins.append(rng.standard_normal((2, w.nt, w.rcv_x.size)).astype(np.float32))
+    outs = wave.acoustic_forward_batched(models, fd_order=8, want_energy=False, imaging_dtype="fp24")
+    loss = sum((torch.as_tensor(l, device=cuda_device) * o["p"]).sum() for l, o in zip(lins, outs))
+    loss.backward()
+    torch.cuda.synchronize()
+    for c, m, o, l in zip(cases, models, outs, lins):
+        kw = dict(nz=c["nz"], nx=c["nx"], dz=c["dx"], nt=c["nt"], dt=c["dt"], nabc=c["nabc"], free_surface=False,
+                  src_x=c["src_x"], src_z=c["src_z"], src_v=c["src_v"], rcv_x=c["rcv_x"], rcv_z=c["rcv_z"],
+                  damp=c["damp"], vp=c["vp"], rho=c["rho"], half=4)
+        ref = orc.forward(**kw, dtype=np.float64)
+        assert orc.rel_l2(o["p"].detach().cpu().numpy(), ref["p"]) < 1e-5
+        rvp, _, _ = orc.gradient(**kw, res_p=l.astype(np.float64), dtype=np.float64)
+        assert orc.rel_l2(m["vp"].grad.cpu().numpy(), rvp) < 1e-4

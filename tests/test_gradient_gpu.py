@@ -88,14 +88,17 @@ def test_group_streams_do_not_change_results(cuda_device):
     assert a[2] == b[2]
 
 
-@pytest.mark.parametrize("fmt,tol", [("fp16", 1e-3), ("bf16", 1e-2)])
-def test_16bit_checkpoints_within_budget(cuda_device, fmt, tol):
-    """Snapshots stored in 16 bits with a per-snapshot scale; the recompute
-    from them runs in fp32, so the only error is each segment restarting from
-    a rounded state (12 restarts here, the harshest case).  fp16 keeps 11
-    significant bits (about 6e-4 here), bf16 8 bits (about 8x more)."""
+@pytest.mark.parametrize("fmt,every,tol", [("fp24", 10, GTOL), ("fp24", 20, GTOL), ("fp16", 20, 1e-3),
+                                           ("bf16", 20, 1e-2)])
+def test_short_checkpoints_within_budget(cuda_device, fmt, every, tol):
+    """Snapshots stored in 24 bits (fp32 exponent, 15-bit mantissa) or in 16
+    bits with a per-snapshot scale; the recompute from them runs in fp32, so
+    the only error is each segment restarting from a rounded state (12 or 24
+    restarts here, the harshest cases).  fp24 keeps 16 significant bits and
+    stays at the fp32 bar; fp16 keeps 11 (about 6e-4 here), bf16 8 (about 8x
+    more than fp16)."""
     c = load_case("small_nofs")
-    g, _, _ = cuda_grad(c, cuda_device, fd_order=8, want_rho=False, checkpoint_every=20, imaging_cache=0,
+    g, _, _ = cuda_grad(c, cuda_device, fd_order=8, want_rho=False, checkpoint_every=every, imaging_cache=0,
                         snapshot_dtype=fmt)
     rvp, _, _ = orc.gradient(**oracle_kwargs(c), res_p=c["lin_p"], res_vx=c["lin_vx"], res_vz=c["lin_vz"],
                              half=4, dtype=np.float64)
