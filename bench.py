@@ -13,6 +13,7 @@ all-fp32 path (fp32 checkpoints, fp32 recompute, no cache) is measured once
 outside the timed region and reported.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+    python bench.py --slice forward|gradient --nt N [...]   (a short slice for ncu)
 
 Prints ONE JSON line on rank 0.  Under torchrun (N > 1) every rank models
 its own 32 shots of the same survey (weak scaling) and the per-rank
@@ -47,7 +48,86 @@ def parse():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--imaging-dtype", default="fp24", choices=["fp32", "fp24", "bf16"],
                     help="storage of the cached imaging fields")
+    # a short slice of a workload for profilers (ncu): runs once, times nothing
+    ap.add_argument("--slice", choices=["forward", "gradient"], default=None,
+                    help="run nt steps of the forward (or forward + adjoint) once and exit (for ncu)")
+    ap.add_argument("--shots", type=int, default=32, help="--slice: shots of the 400 x 1200 model")
+    ap.add_argument("--model", choices=["2d", "3d", "100x200"], default="2d", help="--slice: which workload")
+    ap.add_argument("--tile-rows", type=int, default=0, help="--slice: tile kernel rows (16 or 32)")
+    ap.add_argument("--shots-per-cta", type=int, default=0, help="--slice: shots per CTA of the tile kernel")
+    ap.add_argument("--energy", action="store_true", help="--slice: forward with the energy sums")
+    ap.add_argument("--absorbing", choices=["damping", "cpml"], default="damping", help="--slice: absorbing layers")
+    ap.add_argument("--resident", choices=["auto", "on", "off"], default="auto",
+                    help="--slice: resident forward (plain forward only)")
     return ap.parse_args()
+
+
+def run_slice(args):
+    """A short slice of a benchmark workload, for profilers: nt steps of the
+    400 x 1200 / 8th-order model (--shots of its 32 shots; --model 100x200 for
+    the 4th-order plain forward workload, --model 3d for a 200^3 model with 4
+    shots), forward or forward + adjoint, once; synchronises and exits 0.
+    Everything stays on the device; nothing is timed.  The gradient keeps
+    every step's imaging fields in --imaging-dtype (fp24 by default, as the
+    benchmark does); --absorbing cpml uses the CPML layers."""
+    import torch
+    from geobrain_b200 import synthetic, wave
+    from geobrain_b200.wave import engine
+    dev = torch.device("cuda:0")
+    if args.model == "3d":
+        _slice_3d(torch, wave, args, dev)
+        torch.cuda.synchronize()
+        print("slice: ok")
+        return
+    if args.model == "100x200":
+        w = synthetic.plain_forward_100x200()
+        w.nt = args.nt
+        w.wavelet = w.wavelet[:args.nt]
+    else:
+        w = synthetic.fwi_400x1200(nt=args.nt, n_shots=args.shots)
+    damp = torch.tensor(wave.bc_pml(w.nx, w.nz, w.dx, w.dx, w.nabc, float(w.vp.max()), False), dtype=torch.float32,
+                        device=dev)
+    geo = engine.Geometry(w.nz, w.nx, w.nabc, w.nt, float(w.dt), float(w.dx), w.fd_order // 2, False)
+    plan = engine.get_plan(geo, w.src_x, w.src_z, w.rcv_x, w.rcv_z)
+    plan.set_absorbing(args.absorbing, float(w.vp.max()) if args.absorbing == "cpml" else 0.0)
+    if args.tile_rows or args.shots_per_cta:
+        plan.set_tiling(args.tile_rows, args.shots_per_cta)
+    plan.set_resident({"auto": "auto", "on": True, "off": False}[args.resident])
+    vp = torch.tensor(w.vp, device=dev)
+    rho = torch.tensor(w.rho, device=dev)
+    src_v = torch.tensor(np.tile(w.wavelet, (w.n_shots, 1)), device=dev)
+    if args.slice == "forward":
+        engine.run_forward(plan, vp, rho, damp, src_v, want_energy=args.energy)
+    else:
+        img = torch.empty(plan.imaging_bytes(w.nt, False, args.imaging_dtype), dtype=torch.uint8, device=dev)
+        store = engine.make_store(None, w.nt, "fp32", img, w.nt, False, args.imaging_dtype)
+        p, _, _, _, _ = engine.run_forward(plan, vp, rho, damp, src_v, want_energy=args.energy, store=store)
+        engine.run_backward(plan, vp, rho, damp, src_v, p, None, None, store, False)
+    torch.cuda.synchronize()
+    print("slice: ok")
+
+
+def _slice_3d(torch, wave, args, dev, nz=200, ny=200, nx=200, shots=4, nabc=20):
+    rng = np.random.default_rng(0)
+    nt = args.nt
+    vp = torch.tensor((2000 + 1000 * rng.random((nz, ny, nx))).astype(np.float32), device=dev)
+    rho = torch.full((nz, ny, nx), 2000.0, device=dev)
+    damp = torch.tensor(wave.bc_pml_3d(nx, ny, nz, 10.0, 10.0, 10.0, nabc, 3000.0, free_surface=False)
+                        .astype(np.float32), device=dev)
+    w, _ = wave.RickerWavelet()(f0=15.0, dt=1e-3)
+    w = torch.tensor(np.pad(w.numpy(), (0, nt))[:nt], device=dev)
+    kw = dict(nx=nx, ny=ny, nz=nz, dx=10.0, dy=10.0, dz=10.0, nt=nt, dt=1e-3, nabc=nabc, free_surface=False,
+              src_x=np.linspace(10, nx - 10, shots).astype(np.int64), src_y=np.full(shots, ny // 2),
+              src_z=np.ones(shots, np.int64), src_n=shots, src_v=w, rcv_x=np.arange(0, nx, 2),
+              rcv_y=np.full(nx // 2, ny // 2), rcv_z=np.ones(nx // 2, np.int64), rcv_n=nx // 2, damp=damp,
+              rho=rho, device=dev)
+    if args.slice == "forward":
+        with torch.no_grad():
+            wave.acoustic_forward_kernel_3d(vp=vp, **kw)
+    else:
+        v = vp.detach().requires_grad_(True)
+        out = wave.acoustic_forward_kernel_3d(vp=v, **kw)
+        (0.5 * (out["p"] * out["p"]).sum()).backward()
 
 
 def measured_peaks():
@@ -264,6 +344,9 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 def main():
     args = parse()
+    if args.slice:
+        run_slice(args)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
         return
@@ -496,9 +579,15 @@ def plain_forward_rates(torch, wave, synthetic, dev):
         rate = w.cell_updates() / (ms * 1e-3) / 1e9
         # p, vx, vz read and written once per step; a1, a2 read once per shot group
         b_unit = 24 + 8 / w.n_shots
+        from geobrain_b200.wave import engine
+        plan = engine.get_plan(engine.Geometry(w.nz, w.nx, w.nabc, w.nt, float(w.dt), float(w.dx), w.fd_order // 2,
+                                               False), w.src_x, w.src_z, w.rcv_x, w.rcv_z)
+        res = plan.resident()
         out[name] = {"gcell_updates_per_s": rate, "ms": ms, "fd_order": w.fd_order, "nt": w.nt,
                      "shots": w.n_shots, "absorbing": absorbing, "bytes_per_unit": b_unit,
-                     "achieved_gbs": rate * b_unit, "frac": rate * b_unit / peak}
+                     "achieved_gbs": rate * b_unit, "frac": rate * b_unit / peak,
+                     "kernel": (f"resident ({res['tile_rows']}-row tiles, one cooperative launch)"
+                                if res["tile_rows"] else "tile kernel, one launch per step")}
     return out
 
 
@@ -614,18 +703,46 @@ def _timed(torch, fn, reps=1):
     return e0.elapsed_time(e1) / reps
 
 
+def _plans_of(engine, ws):
+    """The distinct plans (8th order, no free surface) of a list of workloads."""
+    out = {}
+    for w in ws:
+        p = engine.get_plan(engine.Geometry(w.nz, w.nx, w.nabc, w.nt, float(w.dt), float(w.dx), 4, False),
+                            w.src_x, w.src_z, w.rcv_x, w.rcv_z)
+        out[id(p)] = p
+    return list(out.values())
+
+
+def _profiled(plans, fn):
+    """Run fn with phase profiling on every plan; the summed phase split."""
+    for p in plans:
+        p.set_profiling(True)
+    fn()
+    tot = {}
+    for p in plans:
+        for k, v in p.profile().items():
+            tot[k] = tot.get(k, 0) + v
+        p.set_profiling(False)
+    return tot
+
+
 def batch_rates(torch, wave, synthetic, dev):
-    """Batched engine (one launch per time step for all models): the 50
-    particles of 256 x 512 (8 shots, 2000 steps) and the 24 uneven models
-    (128 x 256 .. 512 x 1024, 1000 .. 3000 steps, 4 .. 16 shots), forward
-    and gradient (fwd + adjoint of 0.5 ||p||^2, fp24 imaging cache within
-    the free memory, checkpoints for the rest)."""
+    """Batched engine (one launch per time step for all models of a batch):
+    the 50 particles of 256 x 512 (8 shots, 2000 steps) and the 24 uneven
+    models (128 x 256 .. 512 x 1024, 1000 .. 3000 steps, 4 .. 16 shots).
+    Forward; gradient (forward + adjoint of 0.5 ||p||^2, fp24 imaging fields)
+    by acoustic_gradient_batched, which applies the misfit between the
+    forward and the adjoint and runs memory-sized sub-batches that keep
+    every step's imaging fields; and, for comparison, the same gradient by
+    autograd through acoustic_forward_batched, whose stores must all live
+    until the backward, so the steps that do not fit are recomputed."""
     from geobrain_b200.wave import engine
     peak, _ = measured_peaks()
     out = {}
     for name, ws in (("ensemble_256x512_50particles", synthetic.ensemble_256x512()),
                      ("uneven_batch_24models", synthetic.uneven_batch())):
         units = sum(w.cell_updates() for w in ws)
+        plans = _plans_of(engine, ws)
 
         def fwd():
             with torch.no_grad():
@@ -633,6 +750,11 @@ def batch_rates(torch, wave, synthetic, dev):
                                               want_energy=False, device=dev)
 
         def grad():
+            ms = [_model_kwargs(torch, wave, w, dev) for w in ws]
+            return wave.acoustic_gradient_batched(ms, lambda i, p: (0.5 * (p * p).sum(), p), fd_order=8,
+                                                  device=dev, imaging_dtype="fp24")
+
+        def grad_autograd():
             ms = [_model_kwargs(torch, wave, w, dev, torch.tensor(w.vp, device=dev, requires_grad=True)) for w in ws]
             outs = wave.acoustic_forward_batched(ms, fd_order=8, want_energy=False, device=dev, imaging_dtype="fp24")
             loss = sum(0.5 * (o["p"] * o["p"]).sum() for o in outs)
@@ -641,24 +763,22 @@ def batch_rates(torch, wave, synthetic, dev):
 
         ms_f = _timed(torch, fwd)
         ms_g = _timed(torch, grad)
-        # the batch records its phases on the plan of its first model
-        w0 = ws[0]
-        plan0 = engine.get_plan(engine.Geometry(w0.nz, w0.nx, w0.nabc, w0.nt, float(w0.dt), float(w0.dx), 4, False),
-                                w0.src_x, w0.src_z, w0.rcv_x, w0.rcv_z)
-        plan0.set_profiling(True)
-        grad()
-        prof = plan0.profile()
-        plan0.set_profiling(False)
+        prof = _profiled(plans, grad)
+        ms_a = _timed(torch, grad_autograd)
+        prof_a = _profiled(plans, grad_autograd)
         b_grad = sum(w.cell_updates() * (56 + 16 / w.n_shots) for w in ws)
         b_fwd = sum(w.cell_updates() * (24 + 8 / w.n_shots) for w in ws)
+        split = lambda p: {"phase_ms": {k: p[k] for k in ("forward_ms", "recompute_ms", "adjoint_ms")},
+                           "phase_steps": {k: p[k] for k in ("forward_steps", "recompute_steps", "adjoint_steps")},
+                           "launches": p["launches"]}
         out[name] = {"forward_gcell_updates_per_s": units / (ms_f * 1e-3) / 1e9, "forward_ms": ms_f,
                      "forward_frac": b_fwd / (ms_f * 1e-3) / 1e9 / peak,
                      "gradient_gcell_updates_per_s": units / (ms_g * 1e-3) / 1e9, "gradient_ms": ms_g,
                      "gradient_frac": b_grad / (ms_g * 1e-3) / 1e9 / peak,
-                     "gradient_phase_ms": {k: prof[k] for k in ("forward_ms", "recompute_ms", "adjoint_ms")},
-                     "gradient_phase_steps": {k: prof[k] for k in ("forward_steps", "recompute_steps",
-                                                                   "adjoint_steps")},
-                     "gradient_launches": prof["launches"],
+                     "gradient": dict(split(prof), api="acoustic_gradient_batched (fused misfit, sub-batches, "
+                                                          "no recompute)"),
+                     "autograd_gradient_gcell_updates_per_s": units / (ms_a * 1e-3) / 1e9, "autograd_gradient_ms": ms_a,
+                     "autograd_gradient": dict(split(prof_a), api="acoustic_forward_batched + loss.backward()"),
                      "models": len(ws), "cell_updates": units, "launch": "batched (one launch per step)"}
     return out
 

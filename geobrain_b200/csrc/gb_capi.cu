@@ -11,6 +11,7 @@
 #include "gb_stream.cuh"
 #include "gb_fwd.cuh"
 #include "gb_cpml_adj.cuh"
+#include "gb_resident.cuh"
 
 #include <cudaTypedefs.h>
 
@@ -244,8 +245,72 @@ struct gb_plan {
             arcv_ptr[t + 1] = arcv_ptr[t] + (int)per[t].size();
             arcv_ent.insert(arcv_ent.end(), per[t].begin(), per[t].end());
         }
+        res_choose();
     }
     int spc_eff = 1;
+
+    // Resident forward (gb_resident.cuh): -1 automatic, 0 off, 1 on; the tile
+    // rows asked for (0 = automatic) and in use (0 = the tile kernel runs)
+    int res_mode = -1, res_tz_req = 0, res_tz = 0;
+    int res_tiles_x = 0, res_tiles_z = 0, res_n = 0, res_shots = 0;   // tiling; shots per cooperative launch
+    std::vector<int> res_ptr;                                          // CSR over resident tiles
+    std::vector<int4> res_ent;
+
+    // Can a resident tiling of tz rows run: enough SMs for one shot's tiles,
+    // and, with a free surface, rows fs-1 .. fs+1 inside one tile (the
+    // mirror rows are set where their source rows live).
+    bool res_fits(int tz, int sms) const
+    {
+        const int tx = (Nx + TX - 1) / TX, tzn = (Nz + tz - 1) / tz;
+        if ((long long)tx * tzn > sms) return false;
+        if (d.free_surface && (fs - 1) / tz != (fs + 1) / tz) return false;
+        return true;
+    }
+    // Choose the resident tiling.  Automatic mode runs it when all shots fit
+    // in one cooperative launch (few shots or a small grid: the cases where
+    // the per-step tile kernel is launch- and latency-bound), with the
+    // smallest tile height that fits; more shots keep the tile kernel.
+    void res_choose()
+    {
+        res_tz = 0;
+        if (res_mode == 0 || cpml) return;
+        const int sms = sm_count();
+        int best = 0;
+        for (int tz : kResidentRows) {
+            if (res_tz_req && tz != res_tz_req) continue;
+            if (!res_fits(tz, sms)) continue;
+            const long long n = (long long)((Nx + TX - 1) / TX) * ((Nz + tz - 1) / tz);
+            if (res_mode < 0 && n * d.n_shots > sms) continue;
+            best = tz;
+            break;
+        }
+        if (!best) return;
+        res_tz = best;
+        res_tiles_x = (Nx + TX - 1) / TX;
+        res_tiles_z = (Nz + best - 1) / best;
+        res_n = res_tiles_x * res_tiles_z;
+        res_shots = std::max(1, std::min(d.n_shots, sms / res_n));
+        res_ptr.assign(res_n + 1, 0);
+        for (int r = 0; r < d.n_rcv; ++r) res_ptr[(rcv_z[r] / best) * res_tiles_x + rcv_x[r] / TX + 1]++;
+        for (int t = 0; t < res_n; ++t) res_ptr[t + 1] += res_ptr[t];
+        res_ent.assign(d.n_rcv, int4{0, 0, 0, 0});
+        std::vector<int> fill(res_ptr.begin(), res_ptr.end() - 1);
+        for (int r = 0; r < d.n_rcv; ++r) {
+            const int t = (rcv_z[r] / best) * res_tiles_x + rcv_x[r] / TX;
+            res_ent[fill[t]++] = int4{rcv_z[r] - (rcv_z[r] / best) * best, rcv_x[r] - (rcv_x[r] / TX) * TX, r, 0};
+        }
+    }
+    // SMs of the current device (148 on a B200; also the answer without one)
+    static int sm_count()
+    {
+        int dev = 0, n = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n < 1) {
+            cudaGetLastError();
+            return 148;
+        }
+        return n;
+    }
 
     // Enough CTAs to fill the GPU several times over, as few groups as that
     // allows (each group re-reads the coefficient tiles and adds its own
@@ -288,6 +353,7 @@ namespace {
 // Workspace layout (offsets in bytes from the 256-aligned base).
 struct Layout {
     size_t err, coef, fields, energy, src, rcv_ptr, rcv_ent, tile_fast, amax, cpml, psi, total;
+    size_t res_ptr, res_ent, res_x, res_fl;   // resident forward: receiver CSR, exchange strips, flags
     // gradient only
     size_t mu, img, g1, c1, g2, c2, arcv_ptr, arcv_ent, cprcv, cpcoef;
     int n_img;
@@ -315,6 +381,13 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
     if (p->cpml) {
         L.cpml = o; o = align256(o + (4 * (size_t)p->Nz + 4 * (size_t)p->pitch) * 4);
         L.psi = o; o = align256(o + 2 * S * 4 * p->plane * 4);   // two levels of the memory variables
+    }
+    if (p->res_tz > 0 && with_gradient == 0) {
+        const ResidentKernel k = resident_kernel(p->R, p->res_tz);
+        L.res_ptr = o; o = align256(o + (p->res_n + 1) * 4);
+        L.res_ent = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 16);
+        L.res_x = o; o = align256(o + S * p->res_n * kResParts * k.part_floats * 4);
+        L.res_fl = o; o = align256(o + S * p->res_n * kResFlagStride * 4);
     }
     L.n_img = with_gradient >= 2 ? 3 : 1;
     if (with_gradient > 0) {
@@ -726,6 +799,67 @@ int check_store(const gb_plan *P, const gb_grad_store *store)
     return GB_OK;
 }
 
+// Plain forward by the resident kernel: cooperative launches of res_n tiles x
+// res_shots shots, each running a chunk of steps with the state in shared
+// memory (chunks end where a snapshot of shot 0 is due).  The state starts
+// and ends in buf (level 0 of the workspace's fields).
+int forward_resident(gb_plan *P, const Layout &L, char *ws, const Setup &Su, float *buf, float *energy,
+                     bool want_energy, const float *wavelet, float *trace_p, float *trace_vx, float *trace_vz,
+                     int32_t snapshot_every, float *snapshots, cudaStream_t st)
+{
+    const gb_model_desc &d = P->d;
+    const int S = d.n_shots;
+    const ResidentKernel K = resident_kernel(P->R, P->res_tz);
+    if (!K.fn) return fail(GB_E_UNSUPPORTED, "no resident kernel for this tile height");
+    GB_CUDA(cudaFuncSetAttribute(K.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem));
+    int *d_ptr = reinterpret_cast<int *>(ws + L.res_ptr);
+    int4 *d_ent = reinterpret_cast<int4 *>(ws + L.res_ent);
+    unsigned int *flags = reinterpret_cast<unsigned int *>(ws + L.res_fl);
+    GB_CUDA(cudaMemcpyAsync(d_ptr, P->res_ptr.data(), (P->res_n + 1) * 4, cudaMemcpyHostToDevice, st));
+    if (d.n_rcv) GB_CUDA(cudaMemcpyAsync(d_ent, P->res_ent.data(), d.n_rcv * 16, cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemsetAsync(flags, 0, (size_t)S * P->res_n * kResFlagStride * 4, st));
+    ResArgs A{};
+    A.g = P->geom();
+    A.tiles_x = P->res_tiles_x;
+    A.tiles_z = P->res_tiles_z;
+    A.n_tiles = P->res_n;
+    A.energy = want_energy ? 1 : 0;
+    A.free_surface = d.free_surface ? 1 : 0;
+    A.a1 = Su.a1; A.k1 = Su.k1; A.a2 = Su.a2; A.k2 = Su.k2; A.k3 = Su.k3;
+    A.state = buf;
+    A.src_z = Su.d_src; A.src_x = Su.d_src + S;
+    A.wavelet = wavelet;
+    A.rcv_ptr = d_ptr; A.rcv_ent = d_ent;
+    A.tr_p = trace_p; A.tr_vx = trace_vx; A.tr_vz = trace_vz;
+    A.energy_map = want_energy ? energy : nullptr;
+    A.xbuf = reinterpret_cast<float *>(ws + L.res_x);
+    A.flags = flags;
+    A.err = Su.err;
+    int snap_i = 0;
+    for (int s0 = 0; s0 < S; s0 += P->res_shots) {
+        const int ns = std::min(P->res_shots, S - s0);
+        A.shot0 = s0;
+        const bool snaps = s0 == 0 && snapshot_every > 0 && snapshots;
+        for (int it0 = 0; it0 < d.nt;) {
+            const int it1 = snaps ? std::min(d.nt, (it0 / snapshot_every + 1) * snapshot_every) : d.nt;
+            A.it0 = it0;
+            A.it1 = it1;
+            void *args[] = {(void *)&A};
+            GB_CUDA(cudaLaunchCooperativeKernel(K.fn, dim3((unsigned)(P->res_n * ns)), dim3(K.threads), args, K.smem,
+                                                st));
+            ++P->launches;
+            if (snaps) {
+                GB_CUDA(cudaMemcpy2DAsync(snapshots + (size_t)snap_i * d.nz * d.nx, (size_t)d.nx * 4,
+                                          buf + (size_t)d.nabc * P->pitch + d.nabc, (size_t)P->pitch * 4,
+                                          (size_t)d.nx * 4, d.nz, cudaMemcpyDeviceToDevice, st));
+                ++snap_i;
+            }
+            it0 = it1;
+        }
+    }
+    return GB_OK;
+}
+
 // Gradient of a CPML plan: the adjoint sweep of gb_cpml_adj.cuh over every
 // step, from imaging fields the forward kept for all nt steps (no recompute,
 // so no memory variables need checkpointing).
@@ -910,6 +1044,34 @@ int gb_plan_set_tiling(gb_plan *p, int tile_rows, int shots_per_cta)
     return GB_OK;
 }
 
+int gb_plan_set_resident(gb_plan *p, int mode, int tile_rows)
+{
+    if (!p) return fail(GB_E_ARG, "null plan");
+    if (mode < -1 || mode > 1) return fail(GB_E_ARG, "mode must be -1 (automatic), 0 (off) or 1 (on)");
+    bool known = tile_rows == 0;
+    for (int tz : kResidentRows) known |= tz == tile_rows;
+    if (!known) return fail(GB_E_ARG, "tile_rows must be 0, 8, 16, 24, 32, 40 or 48");
+    p->res_mode = mode;
+    p->res_tz_req = tile_rows;
+    p->res_choose();
+    if (mode == 1 && p->res_tz == 0) {
+        p->res_mode = -1;
+        p->res_tz_req = 0;
+        p->res_choose();
+        return fail(GB_E_UNSUPPORTED, p->cpml ? "the resident forward does not run CPML plans"
+                                              : "no resident tiling of that height fits this grid on this device");
+    }
+    return GB_OK;
+}
+
+int gb_plan_get_resident(const gb_plan *p, int *tile_rows, int *shots_per_launch)
+{
+    if (!p) return fail(GB_E_ARG, "null plan");
+    if (tile_rows) *tile_rows = p->res_tz;
+    if (shots_per_launch) *shots_per_launch = p->res_tz ? p->res_shots : 0;
+    return GB_OK;
+}
+
 int gb_plan_set_group_streams(gb_plan *p, int enable)
 {
     if (!p) return fail(GB_E_ARG, "null plan");
@@ -938,6 +1100,7 @@ int gb_plan_set_absorbing(gb_plan *p, int mode, float vmax)
     if ((mode == GB_ABSORB_CPML) == p->cpml && (!p->cpml || vmax == p->cpml_vmax)) return GB_OK;   // unchanged
     p->release_graph();
     p->cpml = mode == GB_ABSORB_CPML;
+    p->res_choose();   // the resident forward runs the damping layers only
     p->cpml_vmax = vmax;
     p->cpml_prof.clear();
     if (!p->cpml) return GB_OK;
@@ -1047,6 +1210,22 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
     GB_CUDA(cudaMemsetAsync(buf[1], 0, (size_t)S * 3 * P->plane * 4, st));
     if (want_energy) GB_CUDA(cudaMemsetAsync(energy, 0, 3 * P->plane * 4, st));
 
+    if (P->res_tz > 0 && !store && !P->cpml) {
+        P->phase_steps[0] += d.nt;
+        if (int rc = forward_resident(P, L, ws, Su, buf[0], energy, want_energy, wavelet, trace_p, trace_vx,
+                                      trace_vz, snapshot_every, snapshots, st))
+            return rc;
+        float *eo[3] = {energy_p, energy_vx, energy_vz};
+        for (int f = 0; f < 3; ++f)
+            if (eo[f]) {
+                extract_interior_kernel<<<148, 256, 0, st>>>(energy + f * P->plane, d.nz, d.nx, d.nabc, P->pitch,
+                                                             eo[f]);
+                GB_CUDA(cudaGetLastError());
+                ++P->launches;
+            }
+        P->mark(0, false, st);
+        return GB_OK;
+    }
     const StepKernel K0 = fwd_kernel_for(P, want_energy, 0);
     const StepKernel KI = fwd_kernel_for(P, want_energy, n_img == 3 ? 2 : 1);
     if (int rc = prepare_kernel(K0)) return rc;
@@ -1174,14 +1353,23 @@ int gb_trace_misfit(const float *pred, const float *obs, int32_t n_shots, int32_
 size_t gb_plan_autotune_workspace_bytes(gb_plan *p)
 {
     if (!p) return 0;
-    const int tz = p->tz;
+    const int tz = p->tz, rm = p->res_mode, rt = p->res_tz_req;
     size_t m = 0;
     for (int t : {16, 32}) {
         p->tz = t;
+        p->res_mode = 0;
         p->retile();
         m = std::max(m, gb_plan_workspace_bytes(p, 0, 0));
     }
+    p->res_mode = 1;
+    for (int t : kResidentRows) {
+        p->res_tz_req = t;
+        p->res_choose();
+        m = std::max(m, gb_plan_workspace_bytes(p, 0, 0));
+    }
     p->tz = tz;
+    p->res_mode = rm;
+    p->res_tz_req = rt;
     p->retile();
     return m;
 }
@@ -1198,8 +1386,10 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         bool streams;
         int graph;
         bool stream;
+        int res;    // resident forward tile rows, 0 = the tile kernel
     };
-    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps, P->stream};
+    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps, P->stream, P->res_tz};
+    const int saved_res_mode = P->res_mode, saved_res_req = P->res_tz_req;
     const bool prof = P->prof;
     const int nt = P->d.nt;
     const long long launches = P->launches;
@@ -1215,10 +1405,13 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
                 for (int streams = 1; streams >= 0; --streams)
                     for (int graph : {0, C}) {
                         if (graph > n) continue;
-                        cands.push_back({tz, spc, streams != 0, graph, stream != 0});
+                        cands.push_back({tz, spc, streams != 0, graph, stream != 0, 0});
                     }
             }
         }
+    if (!P->cpml)
+        for (int tz : kResidentRows)
+            if (P->res_fits(tz, gb_plan::sm_count())) cands.push_back({saved.tz, saved.spc, true, 0, false, tz});
     cudaEvent_t e0, e1;
     GB_CUDA(cudaEventCreate(&e0));
     GB_CUDA(cudaEventCreate(&e1));
@@ -1234,9 +1427,13 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         P->group_streams = k.streams;
         P->graph_steps = k.graph;
         P->stream = k.stream;
+        P->res_mode = k.res ? 1 : 0;
+        P->res_tz_req = k.res;
+        P->res_choose();
         P->release_graph();
+        if (k.res && P->res_tz != k.res) continue;
         if (gb_plan_workspace_bytes(P, 0, 0) > workspace_bytes) continue;
-        if (k.streams && P->n_groups == 1) continue;      // same as without
+        if (!k.res && k.streams && P->n_groups == 1) continue;      // same as without
         float ms = -1.f;
         for (int rep = 0; rep < 3 && rc == GB_OK; ++rep) {
             if (cudaEventRecord(e0, st) != cudaSuccess) rc = fail(GB_E_CUDA, "event record failed");
@@ -1266,6 +1463,14 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
     P->group_streams = win.streams;
     P->graph_steps = win.graph;
     P->stream = win.stream;
+    if (best < 0) {
+        P->res_mode = saved_res_mode;
+        P->res_tz_req = saved_res_req;
+    } else {
+        P->res_mode = win.res ? 1 : 0;
+        P->res_tz_req = win.res;
+    }
+    P->res_choose();
     P->release_graph();                // captured with the shortened step count
     if (rc != GB_OK) return rc;
     if (best < 0) return fail(GB_E_WORKSPACE, "no candidate fits the workspace");

@@ -30,3 +30,20 @@ StepKernel adj_batch_kernel_for(int R, bool fs, bool rho);
 
 }  // namespace host
 }  // namespace gb
+
+namespace gb {
+namespace host {
+
+// resident_fwd_kernel<R, NW, LV> (gb_resident.cuh) for tile rows tz = NW x LV
+// in kResidentRows; fn is null for other tile heights.  gb_pick_resident.cu.
+constexpr int kResidentRows[] = {8, 16, 24, 32, 40, 48};
+struct ResidentKernel {
+    void *fn = nullptr;
+    size_t smem = 0;
+    int threads = 0;
+    size_t part_floats = 0;     // floats per exchange strip
+};
+ResidentKernel resident_kernel(int R, int tz);
+
+}  // namespace host
+}  // namespace gb

@@ -18,7 +18,7 @@ kernels.pad_model; the compute runs in hand-written sm_100a CUDA kernels.
 """
 from . import kernel as kernels
 from . import misfit, sharding
-from .batched import AcousticBatch, acoustic_forward_batched
+from .batched import AcousticBatch, acoustic_forward_batched, acoustic_gradient_batched
 from .boundary import bc_pml, bc_pml_3d, create_boundary
 from .config import BoundaryConfig, GridConfig, SolverConfig, TimeConfig, WaveletConfig
 from .kernel import acoustic_forward_kernel, pad_model
@@ -35,6 +35,6 @@ __all__ = [
     "WaveletGenerator", "RickerWavelet", "GaussianWavelet", "create_wavelet",
     "bc_pml", "create_boundary", "Source", "Receiver", "Survey", "AcousticPropagator",
     "numpy2tensor", "kernels", "acoustic_forward_kernel", "pad_model",
-    "AcousticBatch", "acoustic_forward_batched", "sharding", "misfit",
+    "AcousticBatch", "acoustic_forward_batched", "acoustic_gradient_batched", "sharding", "misfit",
     "acoustic_forward_kernel_3d", "pad_model_3d", "bc_pml_3d",
 ]

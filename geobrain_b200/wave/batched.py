@@ -16,7 +16,7 @@ per particle.
 from __future__ import annotations
 
 import ctypes
-from typing import List, Sequence
+from typing import List, Optional, Sequence
 
 import numpy as np
 import torch
@@ -262,6 +262,152 @@ def acoustic_forward_batched(models: Sequence[dict], *, fd_order: int = 8, devic
         en = [e0, e1, e2] if want_energy else None
         outs.append(engine.pack_output(plan, p, vx, vz, en, None))
     return outs
+
+
+def _group_plan_array(plans):
+    return (ctypes.c_void_p * len(plans))(*[p.h.value for p in plans])
+
+
+def full_cache_bytes(plan, with_rho: bool, imaging_dtype: str) -> int:
+    """Device bytes one model of a fused batched gradient holds at its peak:
+    the imaging fields of every step, the forward and gradient workspaces
+    (a one-step segment buffer: nothing is recomputed), the three traces and
+    the residual."""
+    S, nt, NR = plan.n_shots, plan.geo.nt, plan.n_rcv
+    return (plan.imaging_bytes(nt, with_rho, imaging_dtype) + plan.workspace_bytes(False, 0) +
+            plan.gradient_workspace_bytes(with_rho, 1, imaging_dtype) + 4 * S * nt * NR * 4)
+
+
+def plan_sub_batches(sizes: Sequence[int], avail: int) -> List[List[int]]:
+    """Split models (in order) into consecutive sub-batches whose summed
+    sizes fit in `avail` bytes; a model larger than `avail` gets a sub-batch
+    of its own (it then keeps checkpoints for the steps that do not fit)."""
+    groups, cur, tot = [], [], 0
+    for i, b in enumerate(sizes):
+        if cur and tot + b > avail:
+            groups.append(cur)
+            cur, tot = [], 0
+        cur.append(i)
+        tot += b
+    if cur:
+        groups.append(cur)
+    return groups
+
+
+def acoustic_gradient_batched(models: Sequence[dict], residual, *, fd_order: int = 8, device=None,
+                              imaging_dtype: str = "fp24", snapshot_dtype: str = "fp32",
+                              memory_budget: Optional[int] = None, with_rho: bool = False):
+    """Losses and gradients of many models at once, with the misfit applied
+    between the forward and the adjoint (no autograd graph is kept).
+
+    `residual(i, p)` takes model i's pressure traces (n_shots, nt, n_rcv) and
+    returns (loss_i, dloss_i/dp) (a 0-d tensor and a tensor like p).  The
+    models run in consecutive sub-batches, each as large as the device
+    memory allows with the imaging fields of EVERY step kept: a sub-batch
+    runs its batched forward (one launch per step for all its models), the
+    residuals, and its batched adjoint, then frees its store before the next
+    sub-batch starts.  Nothing is recomputed unless one model alone does not
+    fit, in which case that model keeps checkpoints (in `snapshot_dtype`)
+    for the steps that do not.  memory_budget: the bytes a sub-batch may
+    hold (default: the free device memory less 2 GiB and 5 %).  Under autograd (acoustic_forward_batched and
+    loss.backward()) every model's store must survive until the backward, so
+    an ensemble larger than the device memory recomputes its uncached steps;
+    this call does not.
+
+    Returns (losses (B,) tensor, [dL/dvp (nz, nx)] per model, and, with
+    with_rho, [dL/drho] per model).  The gradients equal those of the
+    autograd path, bit for bit, for the same imaging format.  Replaces the
+    per-particle forward + backward of InverseProblem.log_likelihood
+    (geobrain/core/inverse.py:104-110) for a whole ensemble."""
+    if imaging_dtype not in _lib.IMAGING_FORMATS:
+        raise ValueError(f"imaging_dtype must be one of {sorted(_lib.IMAGING_FORMATS)}")
+    if snapshot_dtype not in _lib.CKPT_FORMATS:
+        raise ValueError(f"snapshot_dtype must be one of {sorted(_lib.CKPT_FORMATS)}")
+    device = torch.device(device if device is not None else models[0]["vp"].device)
+    if device.type != "cuda":
+        raise ValueError(f"geobrain_b200 runs on CUDA devices only (device={device})")
+    prep = _Prepared(models, fd_order, device)
+    n = len(prep.plans)
+    vps = [_as_f32(m["vp"].detach() if torch.is_tensor(m["vp"]) else m["vp"], device, "vp") for m in models]
+    rhos = [_as_f32(m["rho"].detach() if torch.is_tensor(m["rho"]) else m["rho"], device, "rho") for m in models]
+    if memory_budget is not None:
+        avail = int(memory_budget)
+    else:
+        free, _ = torch.cuda.mem_get_info(device)
+        avail = free + torch.cuda.memory_reserved(device) - torch.cuda.memory_allocated(device)
+        avail -= (2 << 30) + avail // 20
+    sizes = [full_cache_bytes(p, with_rho, imaging_dtype) for p in prep.plans]
+    losses = torch.zeros(n, dtype=torch.float32, device=device)
+    grads_vp, grads_rho = [None] * n, [None] * n
+    L = _bind()
+    for group in plan_sub_batches(sizes, max(avail, 0)):
+        plans = [prep.plans[i] for i in group]
+        arr = _group_plan_array(plans)
+        sub = _Sub(prep, group, arr)
+        stores, keep = [], []
+        if len(group) == 1 and sizes[group[0]] > avail:
+            # one model larger than the memory: cache what fits, checkpoint the rest
+            p = plans[0]
+            K = engine.choose_checkpoint_every(p, 1, 0, snapshot_dtype, with_rho, imaging_dtype)
+            cached = engine.choose_cached_steps(p, "auto", with_rho, device, imaging_dtype, K, snapshot_dtype,
+                                                memory_budget)
+        else:
+            K, cached = max(p.geo.nt for p in plans), None
+        for p in plans:
+            c = p.geo.nt if cached is None else cached
+            k = min(K, p.geo.nt)
+            n_ck = -(-(p.geo.nt - c) // k)
+            ck = torch.empty(max(n_ck * p.checkpoint_bytes(p.geo.nt, snapshot_dtype), 256), dtype=torch.uint8,
+                             device=device)
+            img = torch.empty(max(p.imaging_bytes(c, with_rho, imaging_dtype), 256), dtype=torch.uint8,
+                              device=device)
+            stores.append(engine.make_store(ck if n_ck > 0 else None, K, snapshot_dtype, img if c > 0 else None,
+                                            c, with_rho, imaging_dtype))
+            keep.append((ck, img))
+        outs = _forward(sub, [vps[i] for i in group], [rhos[i] for i in group], False, stores)
+        res_list = []
+        for j, i in enumerate(group):
+            p_tr = outs[j][0][0]
+            loss_i, res_i = residual(i, p_tr)
+            losses[i] = loss_i.detach().to(torch.float32)
+            res_list.append(res_i.detach().to(torch.float32).contiguous())
+        del outs
+        ios = (ModelIO * len(group))()
+        wkeep = []
+        for j, i in enumerate(group):
+            p, st = plans[j], stores[j]
+            g = p.geo
+            gvp = torch.empty((g.nz, g.nx), device=device)
+            grho = torch.empty((g.nz, g.nx), device=device) if with_rho else None
+            seg = max(1, min(st.checkpoint_every, g.nt - st.cached_steps))
+            ws = engine.workspace(p.gradient_workspace_bytes(with_rho, seg, imaging_dtype), device)
+            _, _, damp, w = prep.inputs[i]
+            io = ios[j]
+            io.vp, io.rho, io.damp, io.wavelet = vps[i].data_ptr(), rhos[i].data_ptr(), damp.data_ptr(), w.data_ptr()
+            io.res_p = res_list[j].data_ptr()
+            io.grad_vp, io.grad_rho = gvp.data_ptr(), _lib.ptr(grho)
+            io.store = ctypes.addressof(st)
+            io.workspace, io.workspace_bytes = ws.data_ptr(), ws.numel()
+            wkeep.append(ws)
+            grads_vp[i], grads_rho[i] = gvp, grho
+        bws = engine.workspace(L.gb_batch_workspace_bytes(arr, len(group)), device)
+        with torch.cuda.device(device):
+            rc = L.gb_batch_backward(arr, len(group), ios, bws.data_ptr(), bws.numel(), engine.stream_handle(device))
+        _lib.check(rc)
+        del keep, wkeep, res_list, bws
+    if with_rho:
+        return losses, grads_vp, grads_rho
+    return losses, grads_vp
+
+
+class _Sub:
+    """A sub-batch of a _Prepared batch (the plans and inputs of `group`)."""
+
+    def __init__(self, prep: _Prepared, group: Sequence[int], plan_arr):
+        self.device = prep.device
+        self.plans = [prep.plans[i] for i in group]
+        self.inputs = [prep.inputs[i] for i in group]
+        self.plan_arr = plan_arr
 
 
 class AcousticBatch:

@@ -168,7 +168,8 @@ class Plan:
         _lib.check(self._lib.gb_plan_get_config(self.h, ctypes.byref(tz), ctypes.byref(spc), ctypes.byref(streams),
                                                 ctypes.byref(graph), ctypes.byref(chunks)))
         return {"tile_rows": tz.value, "shots_per_cta": spc.value, "group_streams": bool(streams.value),
-                "graph_steps": graph.value, "stream_chunks": chunks.value}
+                "graph_steps": graph.value, "stream_chunks": chunks.value,
+                "resident_rows": self.resident()["tile_rows"]}
 
     def set_absorbing(self, mode: str = "damping", vmax: float = 0.0) -> None:
         """'damping' (the reference's damping PML) or 'cpml' (memory-variable
@@ -178,6 +179,20 @@ class Plan:
         if mode not in modes:
             raise ValueError(f"absorbing must be one of {sorted(modes)}, got {mode!r}")
         _lib.check(self._lib.gb_plan_set_absorbing(self.h, modes[mode], float(vmax)))
+
+    def set_resident(self, mode, tile_rows: int = 0) -> None:
+        """Resident forward: 'auto' (default), False (off) or True (on, for
+        every tiling that fits); tile_rows 0 (smallest that fits) or one of
+        8, 16, 24, 32, 40, 48."""
+        m = {"auto": -1, False: 0, True: 1}[mode]
+        _lib.check(self._lib.gb_plan_set_resident(self.h, m, int(tile_rows)))
+
+    def resident(self) -> dict:
+        """The resident forward's tile rows (0: the tile kernel runs) and
+        shots per launch."""
+        tz, spl = ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._lib.gb_plan_get_resident(self.h, ctypes.byref(tz), ctypes.byref(spl)))
+        return {"tile_rows": tz.value, "shots_per_launch": spl.value}
 
     def set_streaming(self, enable: bool, seg_chunks: int = 0) -> None:
         """Forward steps by the streaming kernel (0 chunks = automatic)."""

@@ -139,9 +139,36 @@ def ensemble_forward(template: dict, model_shape, **kw) -> Callable[[torch.Tenso
     return forward_batch
 
 
-def sharded_log_likelihood(theta: torch.Tensor, forward_batch: Callable[[torch.Tensor], torch.Tensor],
+def ensemble_value_and_grad(template: dict, model_shape, observed: torch.Tensor, noise_std: float = 1.0,
+                            **kw) -> Callable[[torch.Tensor], Tuple[torch.Tensor, torch.Tensor]]:
+    """value_and_grad for sharded_log_likelihood on the CUDA engine: the
+    Gaussian log-likelihoods ll_i = -½ ‖(F(θ_i) − D) / σ‖² of a batch of
+    velocity particles and d ll_i / d θ_i, by acoustic_gradient_batched (the
+    misfit is applied between the batched forward and the batched adjoint,
+    in sub-batches that keep every step's imaging fields, so nothing is
+    recomputed).  Same values as autograd through ensemble_forward."""
+    from .batched import acoustic_gradient_batched
+
+    def value_and_grad(theta_local: torch.Tensor):
+        models = [dict(template, vp=t.detach().reshape(model_shape).float()) for t in theta_local]
+        obs = observed.reshape(-1)
+        inv_var = 1.0 / (noise_std * noise_std)
+
+        def residual(i, p):
+            r = p.reshape(-1) - obs.to(p.dtype)
+            return 0.5 * inv_var * (r * r).sum(), (inv_var * r).reshape(p.shape)
+
+        losses, grads = acoustic_gradient_batched(models, residual, **kw)
+        return -losses.to(theta_local.dtype), -torch.stack([g.reshape(-1) for g in grads]).reshape(
+            theta_local.shape).to(theta_local.dtype)
+
+    return value_and_grad
+
+
+def sharded_log_likelihood(theta: torch.Tensor, forward_batch: Optional[Callable[[torch.Tensor], torch.Tensor]],
                            observed: torch.Tensor, noise_std: float = 1.0, group=None,
-                           weights: Optional[Sequence[float]] = None, with_grad: bool = True):
+                           weights: Optional[Sequence[float]] = None, with_grad: bool = True,
+                           value_and_grad: Optional[Callable] = None):
     """Gaussian log-likelihoods (and their gradients) of a batch of
     particles, particles split over ranks (InverseProblem.log_likelihood,
     geobrain/core/inverse.py:81-110, without its per-particle loop).
@@ -150,13 +177,20 @@ def sharded_log_likelihood(theta: torch.Tensor, forward_batch: Callable[[torch.T
     predictions in one call (acoustic_forward_batched for an ensemble of
     velocity models).  ll_i = -½ ‖(F(θ_i) − D) / σ‖².  Returns (ll, grad):
     ll of shape (B,), grad = d ll_i / d θ_i of theta's shape (None without
-    with_grad), the same on every rank."""
+    with_grad), the same on every rank.  With value_and_grad (for instance
+    ensemble_value_and_grad), value_and_grad(theta_local) gives the local
+    (ll, grad) directly and forward_batch is used only without with_grad."""
     world, rank = _world(group)
     B = theta.shape[0]
     mine = partition(weights if weights is not None else [1.0] * B, world, rank)
     ll_full = torch.zeros(B, dtype=theta.dtype, device=theta.device)
     grad_full = torch.zeros_like(theta) if with_grad else None
-    if mine:
+    if mine and with_grad and value_and_grad is not None:
+        idx = torch.as_tensor(mine, dtype=torch.long, device=theta.device)
+        ll, g = value_and_grad(theta.detach()[idx])
+        grad_full[idx] = g.to(grad_full.dtype)
+        ll_full[idx] = ll.detach().to(ll_full.dtype)
+    elif mine:
         idx = torch.as_tensor(mine, dtype=torch.long, device=theta.device)
         th = theta.detach()[idx].clone().requires_grad_(with_grad)
         with torch.set_grad_enabled(with_grad):

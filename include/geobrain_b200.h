@@ -164,6 +164,26 @@ int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const flo
                      const float *wavelet, void *workspace, size_t workspace_bytes, int32_t steps,
                      void *stream, float *best_ms_per_step);
 
+/* Resident forward (plain gb_forward without a store, damping layers only):
+ * one cooperative launch runs many time steps, each CTA keeping a 120-column
+ * x tile_rows tile of one shot, plus its halo, in shared memory, and
+ * exchanging the halo strips with its four neighbours through global memory
+ * and flags (bounded waits) after the pressure and the velocity updates.
+ * It is the plain forward's fast path when a step is too small to fill the
+ * GPU: few shots, or a small grid.  The traces are those of the tile kernel,
+ * bit for bit.  mode: -1 automatic (the default: on when every shot's tiles
+ * fit on the device's SMs at once, one CTA per SM), 0 off, 1 on (whenever
+ * a tiling fits; shots beyond one launch run in further launches).
+ * tile_rows: 8, 16, 24, 32, 40 or 48, or 0 for the smallest that fits.
+ * With a free surface, rows fs-1 .. fs+1 must fall in one tile.
+ * GB_E_UNSUPPORTED when mode 1 finds no tiling (or the plan uses CPML); the
+ * plan then stays automatic.  The workspace (gb_plan_workspace_bytes) grows
+ * by the exchange strips and flags. */
+int gb_plan_set_resident(gb_plan *plan, int mode, int tile_rows);
+/* Tile rows of the resident forward in use (0: the tile kernel runs) and
+ * shots per cooperative launch. */
+int gb_plan_get_resident(const gb_plan *plan, int *tile_rows, int *shots_per_launch);
+
 /* Run each group of shots on its own stream (forked from and joined back to
  * the caller's stream; on by default).  Groups never interact, so their
  * kernels fill each other's tails. */

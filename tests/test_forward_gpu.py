@@ -90,17 +90,16 @@ def test_ragged_grids_against_oracle(cuda_device, shape, fd_order):
 def test_tilings_are_bit_identical(cuda_device, tiling):
     """Tile height and shots-per-CTA change the schedule, never the numbers
     (except the energy sums' association order)."""
-    from geobrain_b200.wave import engine
-    from geobrain_b200.wave.kernel import acoustic_forward_kernel
     c = synthetic_case(90, 250, 10, 60, 7, seed=11)
-    base = run_cuda(c, cuda_device, fd_order=8)
-    geo = engine.Geometry(c["nz"], c["nx"], c["nabc"], c["nt"], c["dt"], c["dx"], 4, False)
-    plan = engine.get_plan(geo, c["src_x"], c["src_z"], c["rcv_x"], c["rcv_z"])
-    plan.set_tiling(*tiling)
+    plan = _plan_of(c, 4)
+    plan.set_resident(False)          # the tile kernel's schedules are what is compared
     try:
+        base = run_cuda(c, cuda_device, fd_order=8)
+        plan.set_tiling(*tiling)
         out = run_cuda(c, cuda_device, fd_order=8)
     finally:
         plan.set_tiling(32, 0)
+        plan.set_resident("auto")
     for k in ("p", "vx", "vz"):
         np.testing.assert_array_equal(out[k], base[k])
     for k in ("forward_wavefield_p", "forward_wavefield_vx", "forward_wavefield_vz"):
@@ -122,6 +121,7 @@ def test_graph_replay_is_bit_identical(cuda_device, nt, snapshot_every, streams)
     cached graph, a call with new buffers captures again."""
     c = synthetic_case(60, 250, 10, nt, 5, seed=3)
     plan = _plan_of(c, 4)
+    plan.set_resident(False)               # graphs drive the tile kernel
     plan.set_tiling(16, 2)                 # three groups
     plan.set_group_streams(streams)
     try:
@@ -133,6 +133,7 @@ def test_graph_replay_is_bit_identical(cuda_device, nt, snapshot_every, streams)
         plan.set_graph_steps(16)
         plan.set_group_streams(True)
         plan.set_tiling(16, 0)
+        plan.set_resident("auto")
     for out in outs:
         for k in ("p", "vx", "vz"):
             np.testing.assert_array_equal(out[k], base[k])
@@ -163,12 +164,13 @@ def test_autotune_picks_a_configuration_and_keeps_results(cuda_device):
         assert cfg is not None and cfg["ms_per_step"] > 0
         assert cfg["tile_rows"] in (16, 32) and cfg["graph_steps"] in (0, 16)
         assert plan.config() == {k: cfg[k] for k in ("tile_rows", "shots_per_cta", "group_streams", "graph_steps",
-                                                     "stream_chunks")}
+                                                     "stream_chunks", "resident_rows")}
     finally:
         plan.set_graph_steps(16)
         plan.set_streaming(False)
         plan.set_group_streams(True)
         plan.set_tiling(16, 0)
+        plan.set_resident("auto")
     for k in ("p", "vx", "vz"):
         np.testing.assert_array_equal(tuned[k], base[k])
 
@@ -233,13 +235,15 @@ def test_streaming_kernel_is_bit_identical(cuda_device, shape, chunks, order):
     c = synthetic_case(*shape, seed=21)
     plan = _plan_of(c, order // 2)
     plan.set_tiling(16, 0)
-    base = run_cuda(c, cuda_device, fd_order=order, snapshot_every=16)
-    plan.set_streaming(True, chunks)
+    plan.set_resident(False)
     try:
+        base = run_cuda(c, cuda_device, fd_order=order, snapshot_every=16)
+        plan.set_streaming(True, chunks)
         assert plan.config()["stream_chunks"] > 0
         out = run_cuda(c, cuda_device, fd_order=order, snapshot_every=16)
     finally:
         plan.set_streaming(False)
+        plan.set_resident("auto")
     for k in ("p", "vx", "vz"):
         np.testing.assert_array_equal(out[k], base[k])
     np.testing.assert_array_equal(out["snapshots"], base["snapshots"])
@@ -250,11 +254,14 @@ def test_streaming_kernel_is_bit_identical(cuda_device, shape, chunks, order):
 def test_streaming_kernel_is_not_used_with_a_free_surface(cuda_device):
     c = dict(synthetic_case(60, 250, 10, 30, 2, seed=4), free_surface=True)
     plan = _plan_of(c, 4)
+    plan.set_resident(False)
     plan.set_streaming(True, 0)
     try:
         assert plan.config()["stream_chunks"] == 0          # the tile kernel runs
         out = run_cuda(c, cuda_device, fd_order=8)
+        plan.set_streaming(False)
+        base = run_cuda(c, cuda_device, fd_order=8)
     finally:
         plan.set_streaming(False)
-    base = run_cuda(c, cuda_device, fd_order=8)
+        plan.set_resident("auto")
     np.testing.assert_array_equal(out["p"], base["p"])

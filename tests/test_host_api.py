@@ -174,3 +174,11 @@ def test_courant_number_and_input_checks():
         engine.check_model_inputs(vp, -rho, w, 1e-3, 10.0, 8)
     with pytest.raises(ValueError, match="src_v has non-finite"):
         engine.check_model_inputs(vp, rho, w + float("inf"), 1e-3, 10.0, 8)
+
+
+def test_plan_sub_batches():
+    """Consecutive sub-batches of the fused batched gradient, by memory."""
+    from geobrain_b200.wave.batched import plan_sub_batches
+    assert plan_sub_batches([3, 3, 3, 3], 7) == [[0, 1], [2, 3]]
+    assert plan_sub_batches([5, 9, 1], 6) == [[0], [1], [2]]
+    assert plan_sub_batches([1, 1, 1], 100) == [[0, 1, 2]]
