@@ -1050,7 +1050,7 @@ int gb_plan_set_resident(gb_plan *p, int mode, int tile_rows)
     if (mode < -1 || mode > 1) return fail(GB_E_ARG, "mode must be -1 (automatic), 0 (off) or 1 (on)");
     bool known = tile_rows == 0;
     for (int tz : kResidentRows) known |= tz == tile_rows;
-    if (!known) return fail(GB_E_ARG, "tile_rows must be 0, 8, 16, 24, 32, 40 or 48");
+    if (!known) return fail(GB_E_ARG, "tile_rows must be 0, 4, 8, 12, 16, 24, 32, 36, 40 or 48");
     p->res_mode = mode;
     p->res_tz_req = tile_rows;
     p->res_choose();

@@ -34,9 +34,9 @@ StepKernel adj_batch_kernel_for(int R, bool fs, bool rho);
 namespace gb {
 namespace host {
 
-// resident_fwd_kernel<R, NW, LV> (gb_resident.cuh) for tile rows tz = NW x LV
-// in kResidentRows; fn is null for other tile heights.  gb_pick_resident.cu.
-constexpr int kResidentRows[] = {8, 16, 24, 32, 40, 48};
+// resident_fwd_kernel<R, NW, TZ> (gb_resident.cuh) for the tile heights in
+// kResidentRows; fn is null for other heights.  gb_pick_resident.cu.
+constexpr int kResidentRows[] = {4, 8, 12, 16, 24, 32, 36, 40, 48};
 struct ResidentKernel {
     void *fn = nullptr;
     size_t smem = 0;

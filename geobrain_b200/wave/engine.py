@@ -183,7 +183,7 @@ class Plan:
     def set_resident(self, mode, tile_rows: int = 0) -> None:
         """Resident forward: 'auto' (default), False (off) or True (on, for
         every tiling that fits); tile_rows 0 (smallest that fits) or one of
-        8, 16, 24, 32, 40, 48."""
+        4, 8, 12, 16, 24, 32, 36, 40, 48."""
         m = {"auto": -1, False: 0, True: 1}[mode]
         _lib.check(self._lib.gb_plan_set_resident(self.h, m, int(tile_rows)))
 

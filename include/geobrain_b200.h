@@ -174,7 +174,9 @@ int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const flo
  * bit for bit.  mode: -1 automatic (the default: on when every shot's tiles
  * fit on the device's SMs at once, one CTA per SM), 0 off, 1 on (whenever
  * a tiling fits; shots beyond one launch run in further launches).
- * tile_rows: 8, 16, 24, 32, 40 or 48, or 0 for the smallest that fits.
+ * tile_rows: 4, 8, 12, 16, 24, 32, 36, 40 or 48, or 0 for the smallest that
+ * fits.  Each step updates the cells next to the tile edges first, posts
+ * them, and updates the rest while the neighbours' strips travel.
  * With a free surface, rows fs-1 .. fs+1 must fall in one tile.
  * GB_E_UNSUPPORTED when mode 1 finds no tiling (or the plan uses CPML); the
  * plan then stays automatic.  The workspace (gb_plan_workspace_bytes) grows
