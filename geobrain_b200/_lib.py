@@ -66,6 +66,7 @@ SIGNATURES = {
     "gb_plan_set_group_streams": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_plan_set_graph_steps": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_plan_set_resident": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
+    "gb_plan_launch_calls": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "gb_plan_get_resident": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "gb_trace_misfit": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P, _P, _P]),
     "gb3_workspace_bytes": (_SZ, [ctypes.POINTER(Desc3)]),

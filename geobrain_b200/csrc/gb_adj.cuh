@@ -47,6 +47,12 @@ struct AdjArgs {
     // (acoustic_2d.py:228-237); sources lie on the p mask (checked on the host)
     float *grad_wavelet;
     const int *src_z, *src_x;                // padded source cells
+    // graph replay: with step_base set, the step is *step_base - it, and the
+    // imaging fields of step t are at img_base + (t - img_t0) * img_step elements
+    const int *step_base;
+    float *img_base;
+    long long img_step;
+    int img_t0;
 };
 
 __device__ __forceinline__ void neumaier_add(float &s, float &c, float x)
@@ -89,6 +95,14 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
     }
     grid_dependency_wait();
     grid_launch_dependents();
+    // a CUDA graph replays the same launches for every chunk of steps (in
+    // reverse); the chunk's top step comes from device memory
+    const int it = A.step_base ? *reinterpret_cast<const volatile int *>(A.step_base) - A.it : A.it;
+    const float *const img_ptr =
+        A.step_base ? reinterpret_cast<const float *>(reinterpret_cast<const char *>(A.img_base) +
+                                                      (long long)(it - A.img_t0) * A.img_step *
+                                                          (img_fmt == kImgBF16 ? 2 : img_fmt == kImgF24 ? 3 : 4))
+                    : A.img;
     const bool fast = A.tile_fast[tile] != 0;
     const int rcv0 = A.rcv_ptr[tile], rcv1 = A.rcv_ptr[tile + 1];
     const bool has_rcv = rcv1 > rcv0 && (A.res_p || A.res_vx || A.res_vz);
@@ -132,10 +146,10 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
             const int gz = z0 + vb + u;
             const bool ok = vlane && u < vcnt && gz < g.Nz && gx0 < g.Nx;
             const long long io = (long long)s * g.plane + (long long)gz * g.pitch + gx0;
-            im[u] = ok ? load_img_raw(A.img, io, img_fmt) : img_raw_zero();
+            im[u] = ok ? load_img_raw(img_ptr, io, img_fmt) : img_raw_zero();
             if (RHO) {
-                jx[u] = ok ? load_img_raw(A.img, io + A.img_field_stride, img_fmt) : img_raw_zero();
-                jz[u] = ok ? load_img_raw(A.img, io + 2 * A.img_field_stride, img_fmt) : img_raw_zero();
+                jx[u] = ok ? load_img_raw(img_ptr, io + A.img_field_stride, img_fmt) : img_raw_zero();
+                jz[u] = ok ? load_img_raw(img_ptr, io + 2 * A.img_field_stride, img_fmt) : img_raw_zero();
             }
         }
         if (!__syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1))) {
@@ -157,7 +171,7 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
             for (int e = rcv0 + threadIdx.x; e < rcv1; e += NTHR) {
                 const int4 en = A.rcv_ent[e];
                 const int gz = en.x, gx = en.y;
-                const long long t = ((long long)s * g.nt + A.it) * g.n_rcv + en.z;
+                const long long t = ((long long)s * g.nt + it) * g.n_rcv + en.z;
                 const long long o = (long long)gz * g.pitch + gx;
                 if (A.res_p && gz >= g.p_r0 && gz <= g.p_r1 && gx >= g.p_c0 && gx <= g.p_c1) {
                     const int r = gz - (z0 - R), c = gx - (x0 - 4);
@@ -226,7 +240,7 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
             const int sz = A.src_z[s], sx = A.src_x[s];
             if (sz >= z0 && sz < z0 + TZ && sx >= x0 && sx < x0 + TX) {
                 const int r = sz - (z0 - R), c = sx - (x0 - 4);
-                A.grad_wavelet[(long long)s * g.nt + A.it] = g.dt * (sP[r * RW + c] / sA1[r * RW + c]);
+                A.grad_wavelet[(long long)s * g.nt + it] = g.dt * (sP[r * RW + c] / sA1[r * RW + c]);
             }
         }
 

@@ -47,11 +47,15 @@ __device__ __forceinline__ float *img_step(const BatchModel &M, float *base, int
 constexpr int kBatchForward = 0;
 constexpr int kBatchRecompute = 1;
 
+// clock: a device step counter when the launch is replayed from a CUDA graph
+// (tau then counts from it: *clock + tau forward, *clock - tau in the
+// adjoint), or null.
 template <int R, int TZ, bool FS, bool ENERGY, int IMG>
 __global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
 fwd_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ models,
-                 const BatchMaps *__restrict__ maps, int tau, int mode, int t0)
+                 const BatchMaps *__restrict__ maps, int tau, int mode, int t0, const int *clock)
 {
+    if (clock) tau += *reinterpret_cast<const volatile int *>(clock);
     const int4 item = items[blockIdx.x];   // (model, tile, group, 0)
     const BatchModel &M = models[item.x];
     const int t_end = mode == kBatchForward ? M.nt : min(M.nt, M.t_cache);
@@ -81,8 +85,9 @@ fwd_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ 
 template <int R, int TZ, bool FS, bool RHO>
 __global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
 adj_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ models,
-                 const BatchMaps *__restrict__ maps, int tau)
+                 const BatchMaps *__restrict__ maps, int tau, const int *clock)
 {
+    if (clock) tau = *reinterpret_cast<const volatile int *>(clock) - tau;
     const int4 item = items[blockIdx.x];
     const BatchModel &M = models[item.x];
     if (tau >= M.nt) return;

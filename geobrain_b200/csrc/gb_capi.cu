@@ -156,6 +156,21 @@ struct gb_plan {
     cudaStream_t cap_stream = nullptr;                         // capture origin (never the legacy stream)
     cudaGraphExec_t gexec = nullptr;
     std::vector<uintptr_t> gkey;                               // what the instantiated graph baked in
+    // CUDA graphs of chunks of gradient steps (each with what it baked in):
+    // the forward steps that keep their imaging fields, the adjoint steps
+    // over them, and the batched forward / adjoint steps (on a batch's first plan)
+    struct GraphSlot {
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uintptr_t> key;
+        void release()
+        {
+            if (exec) cudaGraphExecDestroy(exec);
+            exec = nullptr;
+            key.clear();
+        }
+    };
+    GraphSlot g_fwd_img, g_adj, g_batch_fwd, g_batch_adj;
+    long long api_launches = 0;                                // host launch calls (kernels and graph replays)
 
     ~gb_plan()
     {
@@ -168,6 +183,10 @@ struct gb_plan {
         if (gexec) cudaGraphExecDestroy(gexec);
         gexec = nullptr;
         gkey.clear();
+        g_fwd_img.release();
+        g_adj.release();
+        g_batch_fwd.release();
+        g_batch_adj.release();
     }
     void release_streams()
     {
@@ -512,6 +531,7 @@ int launch_step(gb_plan *P, const StepKernel &K, const Maps &maps, Args A, int g
                     (void *)&A};
     GB_CUDA(launch_pdl(K.fn, dim3(P->n_tiles * grp_count), K.smem, args, st));
     ++P->launches;
+    ++P->api_launches;
     return GB_OK;
 }
 
@@ -530,6 +550,7 @@ int launch_step(gb_plan *P, const StepKernel &K, const Maps &maps, FwdArgs A, in
                     (void *)&maps.sa2, (void *)&A,         (void *)&SA};
     GB_CUDA(launch_pdl(K.fn, dim3((unsigned)P->tiles_x * SA.n_seg * SA.n_shots), K.smem, args, st));
     ++P->launches;
+    ++P->api_launches;
     return GB_OK;
 }
 
@@ -646,6 +667,53 @@ int capture_forward_chunk(gb_plan *P, const StepKernel &K, const Maps (&maps)[2]
     const cudaError_t ei = cudaGraphInstantiate(out, graph, 0);
     cudaGraphDestroy(graph);
     if (ei != cudaSuccess) return fail(GB_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    return GB_OK;
+}
+
+// Capture `C` steps of a step loop into `slot` (unless it already holds a
+// graph for `key`): launch(j, gs) launches step j of the chunk on the group
+// streams gs, and after the steps the device counter ctr moves by `advance`;
+// the step kernels read their step index from that counter.
+template <class Launch>
+int capture_chunk(gb_plan *P, gb_plan::GraphSlot &slot, const std::vector<uintptr_t> &key, int C, int *ctr,
+                  int advance, bool group_streams_on, Launch launch)
+{
+    if (slot.exec && slot.key == key) return GB_OK;
+    slot.release();
+    GroupStreams gs;
+    if (group_streams_on) {
+        if (int rc = group_streams(P, nullptr, &gs)) return rc;   // (re)creating the group streams drops cap_stream
+    } else {
+        gs.P = P;
+        gs.n = 1;
+    }
+    if (!P->cap_stream) GB_CUDA(cudaStreamCreateWithFlags(&P->cap_stream, cudaStreamNonBlocking));
+    gs.main = P->cap_stream;
+    const long long launches = P->launches, api = P->api_launches;
+    GB_CUDA(cudaStreamBeginCapture(P->cap_stream, cudaStreamCaptureModeThreadLocal));
+    int rc = group_streams_on ? fork(gs) : GB_OK;
+    for (int j = 0; j < C && rc == GB_OK; ++j) rc = launch(j, gs);
+    if (rc == GB_OK && group_streams_on) rc = join(gs);
+    if (rc == GB_OK) {
+        step_advance_kernel<<<1, 1, 0, P->cap_stream>>>(ctr, advance);
+        if (cudaGetLastError() != cudaSuccess) rc = fail(GB_E_CUDA, "graph capture: launch failed");
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(P->cap_stream, &graph);   // always end the capture
+    P->launches = launches;
+    P->api_launches = api;
+    if (rc != GB_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ec != cudaSuccess) return fail(GB_E_CUDA, std::string("graph capture: ") + cudaGetErrorString(ec));
+    const cudaError_t ei = cudaGraphInstantiate(&slot.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        slot.exec = nullptr;
+        return fail(GB_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+    }
+    slot.key = key;
     return GB_OK;
 }
 
@@ -848,6 +916,7 @@ int forward_resident(gb_plan *P, const Layout &L, char *ws, const Setup &Su, flo
             GB_CUDA(cudaLaunchCooperativeKernel(K.fn, dim3((unsigned)(P->res_n * ns)), dim3(K.threads), args, K.smem,
                                                 st));
             ++P->launches;
+            ++P->api_launches;
             if (snaps) {
                 GB_CUDA(cudaMemcpy2DAsync(snapshots + (size_t)snap_i * d.nz * d.nx, (size_t)d.nx * 4,
                                           buf + (size_t)d.nabc * P->pitch + d.nabc, (size_t)P->pitch * 4,
@@ -1281,6 +1350,7 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
         for (int k = 0; k < n_chunks; ++k) {
             GB_CUDA(cudaGraphLaunch(P->gexec, st));
             P->launches += (long long)C * gs.n + 1;
+            ++P->api_launches;
             const int last = (k + 1) * C - 1;
             if (snapshot_every > 0 && snapshots && ((last + 1) % snapshot_every == 0 || last == d.nt - 1)) {
                 GB_CUDA(cudaMemcpy2DAsync(snapshots + (size_t)snap_i * d.nz * d.nx, (size_t)d.nx * 4,
@@ -1292,7 +1362,7 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
         it_first = n_chunks * C;
         if (int rc = fork(gs)) return rc;
     }
-    for (int it = it_first; it < d.nt; ++it) {
+    auto one_step = [&](int it) -> int {
         const int b = it & 1;
         A.it = it;
         A.out = buf[b ^ 1];
@@ -1320,7 +1390,62 @@ int gb_forward(gb_plan *P, const float *vp, const float *rho, const float *damp,
                 ++snap_i;
             }
         }
+        return GB_OK;
+    };
+    int it = it_first;
+    // the steps that keep their imaging fields (a gradient's forward): chunks
+    // of C steps replayed from one CUDA graph, from an even step on (the
+    // state level of step j of a chunk is j & 1); the imaging fields' address
+    // comes from the device step counter
+    if (store && C > 0 && (snapshot_every <= 0 || !snapshots) && !P->stream_usable() && d.nt - t_cache >= C) {
+        for (; it < d.nt && (it < t_cache || (it & 1)); ++it)
+            if (int rc = one_step(it)) return rc;
+        if (d.nt - it >= C) {
+            if (int rc = join(gs)) return rc;
+            int *step_ctr = reinterpret_cast<int *>(ws + L.err + 128);
+            int dev = -1;
+            GB_CUDA(cudaGetDevice(&dev));
+            const std::vector<uintptr_t> key = {
+                (uintptr_t)dev, (uintptr_t)ws, (uintptr_t)wavelet, (uintptr_t)trace_p, (uintptr_t)trace_vx,
+                (uintptr_t)trace_vz, (uintptr_t)want_energy, (uintptr_t)C, (uintptr_t)P->tz, (uintptr_t)P->spc_eff,
+                (uintptr_t)P->n_groups, (uintptr_t)gs.n, (uintptr_t)KI.fn, (uintptr_t)store->imaging,
+                (uintptr_t)t_cache, (uintptr_t)store->imaging_format, (uintptr_t)store->with_rho};
+            FwdArgs B = A;
+            B.step_base = step_ctr;
+            B.img_base = reinterpret_cast<float *>(store->imaging);
+            B.img_step = (long long)step_img;
+            B.img_t0 = t_cache;
+            B.imaging = reinterpret_cast<float *>(store->imaging);
+            if (int rc = capture_chunk(P, P->g_fwd_img, key, C, step_ctr, C, true, [&](int j, const GroupStreams &g) {
+                    FwdArgs Bj = B;
+                    Bj.it = j;
+                    Bj.out = buf[(j & 1) ^ 1];
+                    if (Su.cpml) {
+                        Bj.psi_in = Su.psi[j & 1];
+                        Bj.psi_out = Su.psi[(j & 1) ^ 1];
+                    }
+                    for (int i = 0; i < g.n; ++i) {
+                        int g0, gc;
+                        launch_groups(g, i, P->n_groups, &g0, &gc);
+                        if (int rc = launch_step(P, KI, maps[j & 1], Bj, g0, gc, g.at(i))) return rc;
+                    }
+                    return GB_OK;
+                }))
+                return rc;
+            step_set_kernel<<<1, 1, 0, st>>>(step_ctr, it);
+            GB_CUDA(cudaGetLastError());
+            ++P->launches;
+            ++P->api_launches;
+            for (; d.nt - it >= C; it += C) {
+                GB_CUDA(cudaGraphLaunch(P->g_fwd_img.exec, st));
+                P->launches += (long long)C * gs.n + 1;
+                ++P->api_launches;
+            }
+            if (int rc = fork(gs)) return rc;
+        }
     }
+    for (; it < d.nt; ++it)
+        if (int rc = one_step(it)) return rc;
     if (int rc = join(gs)) return rc;
     float *eouts[3] = {energy_p, energy_vx, energy_vz};
     for (int f = 0; f < 3; ++f)
@@ -1579,11 +1704,16 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
     int cur = 0;   // adjoint state lives in mu[cur]
 
     // adjoint sweep over [t0, t1) in reverse, imaging fields at img_base[(it - t0)]
-    auto adjoint_sweep = [&](int t0, int t1, void *img_base, int img_fmt) -> int {
+    const int C = P->graph_steps;
+    int *step_ctr = reinterpret_cast<int *>(ws + L.err + 128);
+    // with `graph`, chunks of C steps that start on adjoint level 0 are
+    // replayed from one CUDA graph (the step index and the imaging fields'
+    // address come from a device counter counting down)
+    auto adjoint_sweep = [&](int t0, int t1, void *img_base, int img_fmt, bool graph) -> int {
         P->mark(2, true, st);
         P->phase_steps[2] += t1 - t0;
         if (int rc = fork(gs)) return rc;
-        for (int it = t1 - 1; it >= t0; --it) {
+        auto one_step = [&](int it) -> int {
             A.it = it;
             A.out = mu[cur ^ 1];
             A.img = img_at(img_base, (size_t)(it - t0) * step_img, img_esize(img_fmt));
@@ -1594,7 +1724,53 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
                 if (int rc = launch_step(P, KA, amaps[cur], A, g0, gc, gs.at(i))) return rc;
             }
             cur ^= 1;
+            return GB_OK;
+        };
+        int it = t1 - 1;
+        if (graph && C > 0 && t1 - t0 >= C) {
+            for (; it >= t0 && cur != 0; --it)
+                if (int rc = one_step(it)) return rc;
+            if (it - t0 + 1 >= C) {
+                if (int rc = join(gs)) return rc;
+                int dev = -1;
+                GB_CUDA(cudaGetDevice(&dev));
+                const std::vector<uintptr_t> key = {
+                    (uintptr_t)dev, (uintptr_t)ws, (uintptr_t)res_p, (uintptr_t)res_vx, (uintptr_t)res_vz,
+                    (uintptr_t)img_base, (uintptr_t)img_fmt, (uintptr_t)t0, (uintptr_t)grad_wavelet, (uintptr_t)C,
+                    (uintptr_t)P->tz, (uintptr_t)P->spc_eff, (uintptr_t)P->n_groups, (uintptr_t)gs.n,
+                    (uintptr_t)KA.fn, (uintptr_t)rho_fields};
+                AdjArgs B = A;
+                B.step_base = step_ctr;
+                B.img_base = reinterpret_cast<float *>(img_base);
+                B.img_step = (long long)step_img;
+                B.img_t0 = t0;
+                B.img_fmt = img_fmt;
+                if (int rc = capture_chunk(P, P->g_adj, key, C, step_ctr, -C, true, [&](int j, const GroupStreams &g) {
+                        AdjArgs Bj = B;
+                        Bj.it = j;
+                        Bj.out = mu[(j & 1) ^ 1];
+                        for (int i = 0; i < g.n; ++i) {
+                            int g0, gc;
+                            launch_groups(g, i, P->n_groups, &g0, &gc);
+                            if (int rc = launch_step(P, KA, amaps[j & 1], Bj, g0, gc, g.at(i))) return rc;
+                        }
+                        return GB_OK;
+                    }))
+                    return rc;
+                step_set_kernel<<<1, 1, 0, st>>>(step_ctr, it);
+                GB_CUDA(cudaGetLastError());
+                ++P->launches;
+                ++P->api_launches;
+                for (; it - t0 + 1 >= C; it -= C) {
+                    GB_CUDA(cudaGraphLaunch(P->g_adj.exec, st));
+                    P->launches += (long long)C * gs.n + 1;
+                    ++P->api_launches;
+                }
+                if (int rc = fork(gs)) return rc;
+            }
         }
+        for (; it >= t0; --it)
+            if (int rc = one_step(it)) return rc;
         if (int rc = join(gs)) return rc;
         P->mark(2, false, st);
         return GB_OK;
@@ -1602,7 +1778,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
 
     // 1. steps whose imaging fields the forward kept
     if (store->cached_steps > 0)
-        if (int rc = adjoint_sweep(t_cache, d.nt, store->imaging, store->imaging_format)) return rc;
+        if (int rc = adjoint_sweep(t_cache, d.nt, store->imaging, store->imaging_format, true)) return rc;
     // 2. earlier steps, one checkpoint segment at a time: fp32 recompute from
     //    the checkpoint (writing the imaging fields), then the adjoint sweep
     const int n_seg = (t_cache + K - 1) / K;
@@ -1631,7 +1807,7 @@ int gb_backward(gb_plan *P, const float *vp, const float *rho, const float *damp
         }
         if (int rc = join(gs)) return rc;
         P->mark(1, false, st);
-        if (int rc = adjoint_sweep(t0, t1, wimg, ifmt)) return rc;
+        if (int rc = adjoint_sweep(t0, t1, wimg, ifmt, false)) return rc;
     }
     grad_finish_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, G1, C1, G2, C2, P->n_groups, P->plane, d.nz, d.nx, d.nabc,
                                                 P->pitch, grad_vp, grad_rho);
@@ -1669,12 +1845,20 @@ int gb_selftest_bounded_wait(void *workspace, size_t workspace_bytes, int32_t co
     return gb_workspace_status(workspace, stream);
 }
 
+int gb_plan_launch_calls(const gb_plan *P, long long *calls)
+{
+    if (!P || !calls) return fail(GB_E_ARG, "null argument");
+    *calls = P->api_launches;
+    return GB_OK;
+}
+
 int gb_plan_set_profiling(gb_plan *P, int enable)
 {
     if (!P) return fail(GB_E_ARG, "null plan");
     P->prof = enable != 0;
     P->clear_events();
     P->launches = 0;
+    P->api_launches = 0;
     for (auto &n : P->phase_steps) n = 0;
     return GB_OK;
 }
@@ -1712,7 +1896,7 @@ int gb_plan_profile(gb_plan *P, double *ms_forward, double *ms_recompute, double
 namespace {
 
 struct BatchLayout {
-    size_t models, maps, items, total;
+    size_t models, maps, items, clock, total;
     long long n_items;
 };
 
@@ -1725,6 +1909,7 @@ BatchLayout batch_layout(gb_plan *const *plans, int n)
     B.models = o; o = align256(o + (size_t)n * sizeof(BatchModel));
     B.maps = o; o = align256(o + (size_t)n * sizeof(BatchMaps));
     B.items = o; o = align256(o + (size_t)std::max<long long>(B.n_items, 1) * 16);
+    B.clock = o; o = align256(o + 4);            // step counter of graph-replayed chunks
     B.total = o;
     return B;
 }
@@ -1784,6 +1969,30 @@ int launch_batch(gb_plan *P0, const StepKernel &K, long long n_items, void **arg
 {
     GB_CUDA(cudaLaunchKernel(K.fn, dim3((unsigned)n_items), dim3(NTHR), args, K.smem, st));
     ++P0->launches;
+    ++P0->api_launches;
+    return GB_OK;
+}
+
+// A batched step loop in chunks of C steps replayed from the CUDA graph in
+// `slot` (captured once per key): launch(j, stream) launches step j of a
+// chunk, the kernels reading the batch clock at `clock`, which starts at
+// `first` and moves by `dir` * C after each chunk.
+template <class Launch>
+int batch_graph_chunks(gb_plan *P0, gb_plan::GraphSlot &slot, const std::vector<uintptr_t> &key, int C, int *clock,
+                       int first, int dir, int n_chunks, cudaStream_t st, Launch launch)
+{
+    if (int rc = capture_chunk(P0, slot, key, C, clock, dir * C, false,
+                               [&](int j, const GroupStreams &g) { return launch(j, g.main); }))
+        return rc;
+    step_set_kernel<<<1, 1, 0, st>>>(clock, first);
+    GB_CUDA(cudaGetLastError());
+    ++P0->launches;
+    ++P0->api_launches;
+    for (int k = 0; k < n_chunks; ++k) {
+        GB_CUDA(cudaGraphLaunch(slot.exec, st));
+        P0->launches += C + 1;
+        ++P0->api_launches;
+    }
     return GB_OK;
 }
 
@@ -1869,8 +2078,21 @@ int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *
     const BatchModel *dmodels = reinterpret_cast<const BatchModel *>(bws + B.models);
     const BatchMaps *dmaps = reinterpret_cast<const BatchMaps *>(bws + B.maps);
     int mode = kBatchForward, t0 = 0;
+    int *clock = reinterpret_cast<int *>(bws + B.clock);
+    const int *no_clock = nullptr;
     P0->phase_steps[0] += maxnt;
-    for (int tau = 0; tau < maxnt; ++tau) {
+    // a checkpoint of some model falls at step tau
+    auto saves_at = [&](int tau) {
+        for (int m = 0; m < n; ++m)
+            if (io[m].store && tau < std::min(models[m].t_cache, models[m].nt) && tau % models[m].K == 0) return true;
+        return false;
+    };
+    const int C = P0->graph_steps;
+    int dev = -1;
+    GB_CUDA(cudaGetDevice(&dev));
+    const std::vector<uintptr_t> key = {(uintptr_t)dev, (uintptr_t)bws, (uintptr_t)B.n_items, (uintptr_t)K0.fn,
+                                        (uintptr_t)C, (uintptr_t)kBatchForward};
+    for (int tau = 0; tau < maxnt;) {
         for (int m = 0; m < n; ++m) {
             const gb_grad_store *sto = io[m].store;
             if (sto && tau < std::min(models[m].t_cache, models[m].nt) && tau % models[m].K == 0) {
@@ -1881,9 +2103,35 @@ int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *
                     return rc;
             }
         }
+        // chunks of C steps with no checkpoint inside: one graph replay each
+        // (a checkpoint at the first step of the first chunk is saved above)
+        int n_chunks = 0;
+        if (C > 0)
+            while (tau + (n_chunks + 1) * C <= maxnt) {
+                bool clear = true;
+                for (int t = tau + n_chunks * C + (n_chunks ? 0 : 1); t < tau + (n_chunks + 1) * C && clear; ++t)
+                    clear = !saves_at(t);
+                if (!clear) break;
+                ++n_chunks;
+            }
+        if (n_chunks > 0) {
+            if (int rc = batch_graph_chunks(P0, P0->g_batch_fwd, key, C, clock, tau, 1, n_chunks, st,
+                                            [&](int j, cudaStream_t s2) {
+                                                int tau_v = j;
+                                                void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps,
+                                                                (void *)&tau_v, (void *)&mode, (void *)&t0,
+                                                                (void *)&clock};
+                                                return launch_batch(P0, K0, B.n_items, args, s2);
+                                            }))
+                return rc;
+            tau += n_chunks * C;
+            continue;
+        }
         int tau_v = tau;
-        void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps, (void *)&tau_v, (void *)&mode, (void *)&t0};
+        void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps, (void *)&tau_v, (void *)&mode, (void *)&t0,
+                        (void *)&no_clock};
         if (int rc = launch_batch(P0, K0, B.n_items, args, st)) return rc;
+        ++tau;
     }
     for (int m = 0; m < n; ++m) {
         const gb_model_io &x = io[m];
@@ -2000,6 +2248,12 @@ int gb_batch_backward(gb_plan *const *plans, int n, const gb_model_io *io, void 
     const BatchModel *dmodels = reinterpret_cast<const BatchModel *>(bws + B.models);
     const BatchMaps *dmaps = reinterpret_cast<const BatchMaps *>(bws + B.maps);
 
+    int *clock = reinterpret_cast<int *>(bws + B.clock);
+    const int C = P0->graph_steps;
+    int dev = -1;
+    GB_CUDA(cudaGetDevice(&dev));
+    const std::vector<uintptr_t> akey = {(uintptr_t)dev, (uintptr_t)bws, (uintptr_t)B.n_items, (uintptr_t)KA.fn,
+                                         (uintptr_t)C};
     // batch-wide segments of K steps; a model recomputes a segment only for
     // its steps below min(nt, t_cache)
     const int Kb = std::min(K, maxnt);
@@ -2020,19 +2274,35 @@ int gb_batch_backward(gb_plan *const *plans, int n, const gb_model_io *io, void 
             P0->mark(1, true, st);
             P0->phase_steps[1] += rec_end - t0;
             int mode = kBatchRecompute, tz0 = t0;
+            const int *no_clock = nullptr;
             for (int tau = t0; tau < rec_end; ++tau) {
                 int tau_v = tau;
                 void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps, (void *)&tau_v, (void *)&mode,
-                                (void *)&tz0};
+                                (void *)&tz0, (void *)&no_clock};
                 if (int rc = launch_batch(P0, KF, B.n_items, args, st)) return rc;
             }
             P0->mark(1, false, st);
         }
         P0->mark(2, true, st);
         P0->phase_steps[2] += t1 - t0;
-        for (int tau = t1 - 1; tau >= t0; --tau) {
+        int tau = t1 - 1;
+        // chunks of C steps replayed from one graph (the clock counts down)
+        const int n_chunks = C > 0 ? (t1 - t0) / C : 0;
+        if (n_chunks > 0) {
+            if (int rc = batch_graph_chunks(P0, P0->g_batch_adj, akey, C, clock, tau, -1, n_chunks, st,
+                                            [&](int j, cudaStream_t s2) {
+                                                int tau_v = j;
+                                                void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps,
+                                                                (void *)&tau_v, (void *)&clock};
+                                                return launch_batch(P0, KA, B.n_items, args, s2);
+                                            }))
+                return rc;
+            tau -= n_chunks * C;
+        }
+        for (; tau >= t0; --tau) {
             int tau_v = tau;
-            void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps, (void *)&tau_v};
+            const int *no_clock = nullptr;
+            void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps, (void *)&tau_v, (void *)&no_clock};
             if (int rc = launch_batch(P0, KA, B.n_items, args, st)) return rc;
         }
         P0->mark(2, false, st);

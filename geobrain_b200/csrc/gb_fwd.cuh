@@ -55,6 +55,11 @@ struct FwdArgs {
     float *imaging;                  // [S][plane] -div(v) on the p mask, or null
     long long img_field_stride;      // IMG == 2: dx(p), dz(p) blocks follow at this stride (elements)
     int img_fmt;                     // storage format of the imaging fields (kImg*)
+    // graph replay (step_base set): the imaging fields of step it are at
+    // img_base + (it - img_t0) * img_step elements, when img_base is set
+    float *img_base;
+    long long img_step;
+    int img_t0;
     int grp0, grp_count;             // shot groups this launch covers
     int *err;
     // CPML option (null otherwise): profiles [bz, az (integer rows), bz, az
@@ -137,6 +142,11 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
     // a CUDA graph replays the same launches for every chunk of steps; the
     // chunk's first step comes from device memory
     const int it = A.step_base ? *reinterpret_cast<const volatile int *>(A.step_base) + A.it : A.it;
+    float *const imaging = A.step_base && A.img_base
+                               ? reinterpret_cast<float *>(reinterpret_cast<char *>(A.img_base) +
+                                                           (long long)(it - A.img_t0) * A.img_step *
+                                                               (A.img_fmt == kImgBF16 ? 2 : A.img_fmt == kImgF24 ? 3 : 4))
+                               : A.imaging;
     __syncthreads();
     if (threadIdx.x == 0) {
         mbar_arrive_expect_tx(&bars[2], SM::COEF_BYTES);
@@ -217,8 +227,8 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                         divergence4<R>(sVX + r * VXW, lane, wz, u, g.c, D);
 #pragma unroll
                         for (int q = 0; q < 4; ++q) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], at(pv, q));
-                        if (tile_cell && A.imaging)
-                            store_img4(A.imaging, (long long)s * g.plane + (long long)gz * g.pitch + gx0,
+                        if (tile_cell && imaging)
+                            store_img4(imaging, (long long)s * g.plane + (long long)gz * g.pitch + gx0,
                                        A.img_fmt, make_float4(-D[0], -D[1], -D[2], -D[3]));
                     } else {
                         const bool row_in = gz >= g.p_r0 && gz <= g.p_r1;
@@ -261,8 +271,8 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                                     if (m) at(pv, q) = __fmaf_rn(-at(a1, q), D[q], (1.f - at(k1, q)) * at(pv, q));
                                 }
                             }
-                            if (tile_cell && A.imaging)
-                                store_img4(A.imaging, (long long)s * g.plane + o, A.img_fmt, img);
+                            if (tile_cell && imaging)
+                                store_img4(imaging, (long long)s * g.plane + o, A.img_fmt, img);
                         }
                     }
                     if (gz == sz && sx >= gx0 && sx < gx0 + 4) {
@@ -367,9 +377,9 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                                 }
                             }
                         }
-                        if (IMG == 2 && A.imaging) {
-                            store_img4(A.imaging, (long long)s * g.plane + A.img_field_stride + o, A.img_fmt, jx);
-                            store_img4(A.imaging, (long long)s * g.plane + 2 * A.img_field_stride + o, A.img_fmt,
+                        if (IMG == 2 && imaging) {
+                            store_img4(imaging, (long long)s * g.plane + A.img_field_stride + o, A.img_fmt, jx);
+                            store_img4(imaging, (long long)s * g.plane + 2 * A.img_field_stride + o, A.img_fmt,
                                        jz);
                         }
                         float *outs = A.out + (long long)s * 3 * g.plane + o;

@@ -117,12 +117,14 @@ class Plan:
         """Milliseconds per phase (forward loop, recompute, adjoint) and kernel
         launches since the last call (needs set_profiling(True))."""
         f, r, a = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
-        n = ctypes.c_longlong()
+        n, calls = ctypes.c_longlong(), ctypes.c_longlong()
         steps = (ctypes.c_longlong * 3)()
+        _lib.check(self._lib.gb_plan_launch_calls(self.h, ctypes.byref(calls)))
         _lib.check(self._lib.gb_plan_profile(self.h, ctypes.byref(f), ctypes.byref(r), ctypes.byref(a),
                                              ctypes.byref(n), steps))
         return {"forward_ms": f.value, "recompute_ms": r.value, "adjoint_ms": a.value, "launches": n.value,
-                "forward_steps": steps[0], "recompute_steps": steps[1], "adjoint_steps": steps[2]}
+                "launch_calls": calls.value, "forward_steps": steps[0], "recompute_steps": steps[1],
+                "adjoint_steps": steps[2]}
 
     def workspace_bytes(self, with_gradient: bool = False, checkpoint_every: int = 0) -> int:
         return int(self._lib.gb_plan_workspace_bytes(self.h, int(with_gradient), int(checkpoint_every)))

@@ -108,7 +108,11 @@ int gb_plan_set_tiling(gb_plan *plan, int tile_rows, int shots_per_cta);
 
 /* Plain forward (gb_forward without a gradient store) as replays of one
  * CUDA graph of `steps` time steps (even, at most 64; 0 = one launch per
- * step and group; 16 by default).  The graph holds the step kernels of every shot group,
+ * step and group; 16 by default).  The same chunk length drives the graphs
+ * of the gradient (the forward steps that keep their imaging fields and the
+ * adjoint steps over them) and of the batched forward and adjoint; each of
+ * those graphs is captured on the first call and kept while the buffers are
+ * the same.  The graph holds the step kernels of every shot group,
  * with their fork and join, and a step-counter update.  It is captured on
  * the first call, kept on the plan and replayed nt / steps times; the
  * remaining steps launch one by one.  A call with other buffers (workspace,
@@ -261,6 +265,13 @@ int gb_backward(gb_plan *plan, const float *vp, const float *rho, const float *d
  * steps per phase (forward, recompute, adjoint; array of 3) since the last
  * call, and resets them.  Any output pointer may be NULL. */
 int gb_plan_set_profiling(gb_plan *plan, int enable);
+/* Host-side launch calls (step-kernel launches and CUDA graph replays) since
+ * profiling was last enabled; gb_plan_profile does not reset it.  The plain
+ * forward, the gradient's forward and adjoint over the steps whose imaging
+ * fields the forward kept, and the batched forward and adjoint run in
+ * chunks of gb_plan_set_graph_steps steps replayed from CUDA graphs, so
+ * this is about that many times smaller than the kernel launch count. */
+int gb_plan_launch_calls(const gb_plan *plan, long long *calls);
 int gb_plan_profile(gb_plan *plan, double *ms_forward, double *ms_recompute, double *ms_adjoint,
                     long long *launches, long long *phase_steps);
 
