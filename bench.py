@@ -586,8 +586,8 @@ def plain_forward_rates(torch, wave, synthetic, dev):
         out[name] = {"gcell_updates_per_s": rate, "ms": ms, "fd_order": w.fd_order, "nt": w.nt,
                      "shots": w.n_shots, "absorbing": absorbing, "bytes_per_unit": b_unit,
                      "achieved_gbs": rate * b_unit, "frac": rate * b_unit / peak,
-                     "kernel": (f"resident ({res['tile_rows']}-row tiles, one cooperative launch)"
-                                if res["tile_rows"] else "tile kernel, one launch per step")}
+                     "kernel": (f"resident ({res['tile_rows']}-row tiles, {res['exchange']} exchange, "
+                                "one launch)" if res["tile_rows"] else "tile kernel, one launch per step")}
     return out
 
 

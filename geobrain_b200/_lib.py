@@ -67,7 +67,8 @@ SIGNATURES = {
     "gb_plan_set_graph_steps": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_plan_set_resident": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_launch_calls": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
-    "gb_plan_get_resident": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "gb_plan_get_resident": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
     "gb_trace_misfit": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P, _P, _P]),
     "gb3_workspace_bytes": (_SZ, [ctypes.POINTER(Desc3)]),
     "gb3_forward": (ctypes.c_int, [ctypes.POINTER(Desc3)] + [_P] * 6 + [_P] * 4 + [_P] * 8 + [_P, _I32] +

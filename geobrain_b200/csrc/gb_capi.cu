@@ -268,9 +268,13 @@ struct gb_plan {
     }
     int spc_eff = 1;
 
-    // Resident forward (gb_resident.cuh): -1 automatic, 0 off, 1 on; the tile
+    // Resident forward (gb_resident.cuh): -1 automatic, 0 off, 1 on with the
+    // exchange through global memory and flags, 2 on with the exchange
+    // through distributed shared memory in one cluster per shot; the tile
     // rows asked for (0 = automatic) and in use (0 = the tile kernel runs)
     int res_mode = -1, res_tz_req = 0, res_tz = 0;
+    bool res_cluster = false;                                          // the exchange in use
+    static constexpr int kMaxClusterTiles = 16;                        // CTAs of one (non-portable) cluster
     int res_tiles_x = 0, res_tiles_z = 0, res_n = 0, res_shots = 0;   // tiling; shots per cooperative launch
     std::vector<int> res_ptr;                                          // CSR over resident tiles
     std::vector<int4> res_ent;
@@ -285,30 +289,40 @@ struct gb_plan {
         if (d.free_surface && (fs - 1) / tz != (fs + 1) / tz) return false;
         return true;
     }
-    // Choose the resident tiling.  Automatic mode runs it when all shots fit
-    // in one cooperative launch (few shots or a small grid: the cases where
-    // the per-step tile kernel is launch- and latency-bound), with the
-    // smallest tile height that fits; more shots keep the tile kernel.
+    // Choose the resident tiling.  Automatic mode runs it when every shot's
+    // tiles fit on the SMs at once (few shots or a small grid: the cases
+    // where the per-step tile kernel is launch- and latency-bound), with the
+    // cluster exchange when one shot's tiles fit in one cluster, else the
+    // exchange through global memory; each with the smallest tile height
+    // that fits.  More shots keep the tile kernel.
     void res_choose()
     {
         res_tz = 0;
+        res_cluster = false;
         if (res_mode == 0 || cpml) return;
         const int sms = sm_count();
         int best = 0;
-        for (int tz : kResidentRows) {
-            if (res_tz_req && tz != res_tz_req) continue;
-            if (!res_fits(tz, sms)) continue;
-            const long long n = (long long)((Nx + TX - 1) / TX) * ((Nz + tz - 1) / tz);
-            if (res_mode < 0 && n * d.n_shots > sms) continue;
-            best = tz;
-            break;
+        for (int pass = 0; pass < 2 && !best; ++pass) {
+            const bool cl = pass == 0;
+            if ((cl && res_mode == 1) || (!cl && res_mode == 2)) continue;
+            for (int tz : kResidentRows) {
+                if (res_tz_req && tz != res_tz_req) continue;
+                if (!res_fits(tz, sms)) continue;
+                const long long n = (long long)((Nx + TX - 1) / TX) * ((Nz + tz - 1) / tz);
+                if (cl && n > kMaxClusterTiles) continue;
+                if (res_mode < 0 && n * d.n_shots > sms) continue;
+                best = tz;
+                res_cluster = cl;
+                break;
+            }
         }
         if (!best) return;
         res_tz = best;
         res_tiles_x = (Nx + TX - 1) / TX;
         res_tiles_z = (Nz + best - 1) / best;
         res_n = res_tiles_x * res_tiles_z;
-        res_shots = std::max(1, std::min(d.n_shots, sms / res_n));
+        // clusters never wait on each other: one launch takes every shot
+        res_shots = res_cluster ? d.n_shots : std::max(1, std::min(d.n_shots, sms / res_n));
         res_ptr.assign(res_n + 1, 0);
         for (int r = 0; r < d.n_rcv; ++r) res_ptr[(rcv_z[r] / best) * res_tiles_x + rcv_x[r] / TX + 1]++;
         for (int t = 0; t < res_n; ++t) res_ptr[t + 1] += res_ptr[t];
@@ -402,7 +416,7 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
         L.psi = o; o = align256(o + 2 * S * 4 * p->plane * 4);   // two levels of the memory variables
     }
     if (p->res_tz > 0 && with_gradient == 0) {
-        const ResidentKernel k = resident_kernel(p->R, p->res_tz);
+        const ResidentKernel k = resident_kernel(p->R, p->res_tz, false);
         L.res_ptr = o; o = align256(o + (p->res_n + 1) * 4);
         L.res_ent = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 16);
         L.res_x = o; o = align256(o + S * p->res_n * kResParts * k.part_floats * 4);
@@ -877,9 +891,10 @@ int forward_resident(gb_plan *P, const Layout &L, char *ws, const Setup &Su, flo
 {
     const gb_model_desc &d = P->d;
     const int S = d.n_shots;
-    const ResidentKernel K = resident_kernel(P->R, P->res_tz);
+    const ResidentKernel K = resident_kernel(P->R, P->res_tz, P->res_cluster);
     if (!K.fn) return fail(GB_E_UNSUPPORTED, "no resident kernel for this tile height");
     GB_CUDA(cudaFuncSetAttribute(K.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem));
+    if (P->res_cluster && P->res_n > 8) GB_CUDA(cudaFuncSetAttribute(K.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     int *d_ptr = reinterpret_cast<int *>(ws + L.res_ptr);
     int4 *d_ent = reinterpret_cast<int4 *>(ws + L.res_ent);
     unsigned int *flags = reinterpret_cast<unsigned int *>(ws + L.res_fl);
@@ -913,8 +928,30 @@ int forward_resident(gb_plan *P, const Layout &L, char *ws, const Setup &Su, flo
             A.it0 = it0;
             A.it1 = it1;
             void *args[] = {(void *)&A};
-            GB_CUDA(cudaLaunchCooperativeKernel(K.fn, dim3((unsigned)(P->res_n * ns)), dim3(K.threads), args, K.smem,
-                                                st));
+            if (P->res_cluster) {
+                // one cluster of res_n CTAs per shot (cluster rank = tile)
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)(P->res_n * ns));
+                cfg.blockDim = dim3(K.threads);
+                cfg.dynamicSmemBytes = K.smem;
+                cfg.stream = st;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeClusterDimension;
+                attr[0].val.clusterDim.x = (unsigned)P->res_n;
+                attr[0].val.clusterDim.y = 1;
+                attr[0].val.clusterDim.z = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                int n_clusters = 0;
+                GB_CUDA(cudaOccupancyMaxActiveClusters(&n_clusters, K.fn, &cfg));
+                if (n_clusters < 1)
+                    return fail(GB_E_UNSUPPORTED, "this device cannot schedule a cluster of " +
+                                                      std::to_string(P->res_n) + " resident tiles");
+                GB_CUDA(cudaLaunchKernelExC(&cfg, K.fn, args));
+            } else {
+                GB_CUDA(cudaLaunchCooperativeKernel(K.fn, dim3((unsigned)(P->res_n * ns)), dim3(K.threads), args,
+                                                    K.smem, st));
+            }
             ++P->launches;
             ++P->api_launches;
             if (snaps) {
@@ -1116,14 +1153,15 @@ int gb_plan_set_tiling(gb_plan *p, int tile_rows, int shots_per_cta)
 int gb_plan_set_resident(gb_plan *p, int mode, int tile_rows)
 {
     if (!p) return fail(GB_E_ARG, "null plan");
-    if (mode < -1 || mode > 1) return fail(GB_E_ARG, "mode must be -1 (automatic), 0 (off) or 1 (on)");
+    if (mode < -1 || mode > 2)
+        return fail(GB_E_ARG, "mode must be -1 (automatic), 0 (off), 1 (global exchange) or 2 (cluster exchange)");
     bool known = tile_rows == 0;
     for (int tz : kResidentRows) known |= tz == tile_rows;
     if (!known) return fail(GB_E_ARG, "tile_rows must be 0, 4, 8, 12, 16, 24, 32, 36, 40 or 48");
     p->res_mode = mode;
     p->res_tz_req = tile_rows;
     p->res_choose();
-    if (mode == 1 && p->res_tz == 0) {
+    if (mode >= 1 && p->res_tz == 0) {
         p->res_mode = -1;
         p->res_tz_req = 0;
         p->res_choose();
@@ -1133,11 +1171,12 @@ int gb_plan_set_resident(gb_plan *p, int mode, int tile_rows)
     return GB_OK;
 }
 
-int gb_plan_get_resident(const gb_plan *p, int *tile_rows, int *shots_per_launch)
+int gb_plan_get_resident(const gb_plan *p, int *tile_rows, int *shots_per_launch, int *cluster)
 {
     if (!p) return fail(GB_E_ARG, "null plan");
     if (tile_rows) *tile_rows = p->res_tz;
     if (shots_per_launch) *shots_per_launch = p->res_tz ? p->res_shots : 0;
+    if (cluster) *cluster = p->res_tz && p->res_cluster ? 1 : 0;
     return GB_OK;
 }
 
@@ -1511,9 +1550,10 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         bool streams;
         int graph;
         bool stream;
-        int res;    // resident forward tile rows, 0 = the tile kernel
+        int res;    // resident forward tile rows (negative: the cluster exchange), 0 = the tile kernel
     };
-    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps, P->stream, P->res_tz};
+    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps, P->stream,
+                       P->res_cluster ? -P->res_tz : P->res_tz};
     const int saved_res_mode = P->res_mode, saved_res_req = P->res_tz_req;
     const bool prof = P->prof;
     const int nt = P->d.nt;
@@ -1536,7 +1576,11 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         }
     if (!P->cpml)
         for (int tz : kResidentRows)
-            if (P->res_fits(tz, gb_plan::sm_count())) cands.push_back({saved.tz, saved.spc, true, 0, false, tz});
+            if (P->res_fits(tz, gb_plan::sm_count())) {
+                cands.push_back({saved.tz, saved.spc, true, 0, false, tz});
+                const long long n = (long long)((P->Nx + TX - 1) / TX) * ((P->Nz + tz - 1) / tz);
+                if (n <= gb_plan::kMaxClusterTiles) cands.push_back({saved.tz, saved.spc, true, 0, false, -tz});
+            }
     cudaEvent_t e0, e1;
     GB_CUDA(cudaEventCreate(&e0));
     GB_CUDA(cudaEventCreate(&e1));
@@ -1552,11 +1596,11 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         P->group_streams = k.streams;
         P->graph_steps = k.graph;
         P->stream = k.stream;
-        P->res_mode = k.res ? 1 : 0;
-        P->res_tz_req = k.res;
+        P->res_mode = k.res > 0 ? 1 : k.res < 0 ? 2 : 0;
+        P->res_tz_req = std::abs(k.res);
         P->res_choose();
         P->release_graph();
-        if (k.res && P->res_tz != k.res) continue;
+        if (k.res && P->res_tz != std::abs(k.res)) continue;
         if (gb_plan_workspace_bytes(P, 0, 0) > workspace_bytes) continue;
         if (!k.res && k.streams && P->n_groups == 1) continue;      // same as without
         float ms = -1.f;
@@ -1592,8 +1636,8 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         P->res_mode = saved_res_mode;
         P->res_tz_req = saved_res_req;
     } else {
-        P->res_mode = win.res ? 1 : 0;
-        P->res_tz_req = win.res;
+        P->res_mode = win.res > 0 ? 1 : win.res < 0 ? 2 : 0;
+        P->res_tz_req = std::abs(win.res);
     }
     P->res_choose();
     P->release_graph();                // captured with the shortened step count

@@ -43,7 +43,9 @@ struct ResidentKernel {
     int threads = 0;
     size_t part_floats = 0;     // floats per exchange strip
 };
-ResidentKernel resident_kernel(int R, int tz);
+// cluster: the variant that exchanges through distributed shared memory
+// within one thread-block cluster per shot (tiles of a shot <= 16).
+ResidentKernel resident_kernel(int R, int tz, bool cluster);
 
 }  // namespace host
 }  // namespace gb

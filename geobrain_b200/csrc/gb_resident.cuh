@@ -31,6 +31,15 @@
 // Every CTA must be resident at once: the launch is cooperative (one CTA per
 // SM at most), and every wait on a neighbour's flag is bounded; a wait that
 // gives up, or sees another CTA's error, sets the status word and returns.
+//
+// When one shot's tiles fit in one thread-block cluster (16 CTAs at most),
+// the cluster variant (CL) exchanges through distributed shared memory
+// instead: a CTA reads its neighbours' boundary rows and columns straight
+// from their shared memory, and the two exchanges of a step become the two
+// halves of hardware cluster barriers (arrive after posting, wait before
+// reading), with the interior work between them.  No global strips, no
+// flags, and no cooperative launch: each shot is one cluster, and clusters
+// never wait on each other.
 #pragma once
 
 #include "gb_fwd.cuh"
@@ -173,6 +182,42 @@ __device__ __forceinline__ void res_fetch(float *rows_f, float *cols_f, const fl
     }
 }
 
+// Cluster barrier halves (every thread of every CTA of the cluster takes
+// part; the hardware barrier needs no bound: every CTA runs the same
+// sequence of arrivals and waits, which a launch of whole clusters keeps
+// co-scheduled).
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
+// The address of the same shared-memory location in CTA `rank` of the cluster.
+__device__ __forceinline__ const float *cluster_map(const float *p, int rank)
+{
+    uint64_t r;
+    asm volatile("mapa.u64 %0, %1, %2;" : "=l"(r) : "l"(reinterpret_cast<uint64_t>(p)), "r"(rank));
+    return reinterpret_cast<const float *>(r);
+}
+
+// The neighbours' boundary rows and columns copied from their shared memory
+// into the halo (the cluster variant of res_fetch): rows [0, R) from the
+// upper tile's rows [TZ, TZ + R), rows [TZ + R, TZ + 2R) from the lower
+// tile's rows [R, 2R), columns 0..3 / 124..127 from the left tile's columns
+// 120..123 / the right tile's columns 4..7 (owned rows).
+template <int R, int NW, int TZ>
+__device__ __forceinline__ void res_fetch_cluster(float *rows_f, float *cols_f, const int (&nb)[4])
+{
+    using G = ResGeo<R, NW, TZ>;
+    for (int e = threadIdx.x; e < R * 32; e += G::NTH) {
+        const int r = e >> 5, l = e & 31;
+        if (nb[0] >= 0) sts4(rows_f + r * RW + 4 * l, lds4(cluster_map(rows_f + (TZ + r) * RW + 4 * l, nb[0])));
+        if (nb[1] >= 0)
+            sts4(rows_f + (TZ + R + r) * RW + 4 * l, lds4(cluster_map(rows_f + (R + r) * RW + 4 * l, nb[1])));
+    }
+    for (int r = threadIdx.x; r < TZ; r += G::NTH) {
+        if (nb[2] >= 0) sts4(cols_f + (R + r) * RW, lds4(cluster_map(cols_f + (R + r) * RW + 120, nb[2])));
+        if (nb[3] >= 0) sts4(cols_f + (R + r) * RW + 124, lds4(cluster_map(cols_f + (R + r) * RW + 4, nb[3])));
+    }
+}
+
 // What the cell updates of one CTA share.
 struct ResCtx {
     float *sP, *sVX, *sVZ;
@@ -275,7 +320,9 @@ __device__ __forceinline__ void res_item(int i, int &r, int &l)
     }
 }
 
-template <int R, int NW, int TZ>
+// CL: exchange through distributed shared memory within one cluster per
+// shot (the launch's cluster is the shot's n_tiles CTAs, rank = tile).
+template <int R, int NW, int TZ, bool CL>
 __global__ void __launch_bounds__(NW * 32, 1) resident_fwd_kernel(const ResArgs A)
 {
     using G = ResGeo<R, NW, TZ>;
@@ -358,6 +405,7 @@ __global__ void __launch_bounds__(NW * 32, 1) resident_fwd_kernel(const ResArgs 
 #pragma unroll
     for (int u = 0; u < G::LE; ++u) e_p[u] = e_vx[u] = e_vz[u] = zero4();
     __syncthreads();
+    if (CL) cluster_arrive();   // the first step's p exchange waits on this phase
 
     for (int it = A.it0; it < A.it1; ++it) {
         // ---- p interior (reads the tile's own v only) ---------------------
@@ -370,7 +418,10 @@ __global__ void __launch_bounds__(NW * 32, 1) resident_fwd_kernel(const ResArgs 
                 if (ri + u < TZ) res_p_cells<R>(A, C, ri + u, lane, wz, u, it);
         }
         // ---- the neighbours' v strips of the previous step ----------------
-        if (it > A.it0) {
+        if (CL) {
+            cluster_wait();
+            if (it > A.it0) res_fetch_cluster<R, NW, TZ>(sVZ, sVX, nb);
+        } else if (it > A.it0) {
             if (!res_wait(fl, nb, 32, (unsigned)it, A.err)) return;
             // (a mirror row in the halo arrives mirrored: its owner posts it after the mirror)
             res_fetch<R, NW, TZ>(sVZ, sVX, xb, nb, 4, 6);
@@ -391,7 +442,8 @@ __global__ void __launch_bounds__(NW * 32, 1) resident_fwd_kernel(const ResArgs 
             for (int c = threadIdx.x; c < RW; c += G::NTH) sP[rm * RW + c] = -sP[(rm + 2) * RW + c];
             __syncthreads();
         }
-        res_post<R, NW, TZ>(sP, sP, my, 0, 2, my_fl, (unsigned)it + 1u);
+        if (CL) cluster_arrive();
+        else res_post<R, NW, TZ>(sP, sP, my, 0, 2, my_fl, (unsigned)it + 1u);
         // ---- v interior (reads the tile's own p only) ---------------------
         if (G::NI > 0 && ilane && ri < TZ) {
             float4 wp[G::LI + 2 * R - 1];
@@ -402,8 +454,13 @@ __global__ void __launch_bounds__(NW * 32, 1) resident_fwd_kernel(const ResArgs 
                 if (ri + u < TZ) res_v_cells<R>(A, C, ri + u, lane, wp, u);
         }
         // ---- the neighbours' p strips --------------------------------------
-        if (!res_wait(fl, nb, 0, (unsigned)it + 1u, A.err)) return;
-        res_fetch<R, NW, TZ>(sP, sP, xb, nb, 0, 2);
+        if (CL) {
+            cluster_wait();
+            res_fetch_cluster<R, NW, TZ>(sP, sP, nb);
+        } else {
+            if (!res_wait(fl, nb, 0, (unsigned)it + 1u, A.err)) return;
+            res_fetch<R, NW, TZ>(sP, sP, xb, nb, 0, 2);
+        }
         __syncthreads();
         // ---- v boundary, mirror ---------------------------------------------
         for (int i = threadIdx.x; i < G::NITEM; i += G::NTH) {
@@ -453,8 +510,12 @@ __global__ void __launch_bounds__(NW * 32, 1) resident_fwd_kernel(const ResArgs 
             }
         }
         // ---- post the v strips ---------------------------------------------
-        if (it + 1 < A.it1) res_post<R, NW, TZ>(sVZ, sVX, my, 4, 6, my_fl + 32, (unsigned)it + 1u);
+        if (CL) cluster_arrive();
+        else if (it + 1 < A.it1) res_post<R, NW, TZ>(sVZ, sVX, my, 4, 6, my_fl + 32, (unsigned)it + 1u);
     }
+    // the neighbours may still be reading this CTA's rows: none leaves the
+    // cluster before all are done
+    if (CL) cluster_wait();
 
     // the owned cells back to the state; the energy sums into the padded maps
     __syncthreads();

@@ -183,18 +183,20 @@ class Plan:
         _lib.check(self._lib.gb_plan_set_absorbing(self.h, modes[mode], float(vmax)))
 
     def set_resident(self, mode, tile_rows: int = 0) -> None:
-        """Resident forward: 'auto' (default), False (off) or True (on, for
-        every tiling that fits); tile_rows 0 (smallest that fits) or one of
-        4, 8, 12, 16, 24, 32, 36, 40, 48."""
-        m = {"auto": -1, False: 0, True: 1}[mode]
+        """Resident forward: 'auto' (default), False (off), True or 'global'
+        (on, halo strips through global memory and flags), or 'cluster' (on,
+        strips through distributed shared memory, one cluster of at most 16
+        CTAs per shot); tile_rows 0 (smallest that fits) or one of 4, 8, 12,
+        16, 24, 32, 36, 40, 48."""
+        m = {"auto": -1, False: 0, True: 1, "global": 1, "cluster": 2}[mode]
         _lib.check(self._lib.gb_plan_set_resident(self.h, m, int(tile_rows)))
 
     def resident(self) -> dict:
-        """The resident forward's tile rows (0: the tile kernel runs) and
-        shots per launch."""
-        tz, spl = ctypes.c_int(), ctypes.c_int()
-        _lib.check(self._lib.gb_plan_get_resident(self.h, ctypes.byref(tz), ctypes.byref(spl)))
-        return {"tile_rows": tz.value, "shots_per_launch": spl.value}
+        """The resident forward's tile rows (0: the tile kernel runs), shots
+        per launch, and exchange ('cluster' or 'global')."""
+        tz, spl, cl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _lib.check(self._lib.gb_plan_get_resident(self.h, ctypes.byref(tz), ctypes.byref(spl), ctypes.byref(cl)))
+        return {"tile_rows": tz.value, "shots_per_launch": spl.value, "exchange": "cluster" if cl.value else "global"}
 
     def set_streaming(self, enable: bool, seg_chunks: int = 0) -> None:
         """Forward steps by the streaming kernel (0 chunks = automatic)."""

@@ -176,8 +176,12 @@ int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const flo
  * It is the plain forward's fast path when a step is too small to fill the
  * GPU: few shots, or a small grid.  The traces are those of the tile kernel,
  * bit for bit.  mode: -1 automatic (the default: on when every shot's tiles
- * fit on the device's SMs at once, one CTA per SM), 0 off, 1 on (whenever
- * a tiling fits; shots beyond one launch run in further launches).
+ * fit on the device's SMs at once, one CTA per SM, with the cluster exchange
+ * when one shot's tiles fit in one cluster), 0 off, 1 on with the exchange
+ * through global memory and flags (whenever a tiling fits; shots beyond one
+ * cooperative launch run in further launches), 2 on with the exchange
+ * through distributed shared memory: one thread-block cluster of at most 16
+ * CTAs per shot, hardware cluster barriers in place of the flags.
  * tile_rows: 4, 8, 12, 16, 24, 32, 36, 40 or 48, or 0 for the smallest that
  * fits.  Each step updates the cells next to the tile edges first, posts
  * them, and updates the rest while the neighbours' strips travel.
@@ -186,9 +190,10 @@ int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const flo
  * plan then stays automatic.  The workspace (gb_plan_workspace_bytes) grows
  * by the exchange strips and flags. */
 int gb_plan_set_resident(gb_plan *plan, int mode, int tile_rows);
-/* Tile rows of the resident forward in use (0: the tile kernel runs) and
- * shots per cooperative launch. */
-int gb_plan_get_resident(const gb_plan *plan, int *tile_rows, int *shots_per_launch);
+/* Tile rows of the resident forward in use (0: the tile kernel runs),
+ * shots per launch, and whether the cluster exchange runs (1) or the
+ * exchange through global memory (0).  Any pointer may be NULL. */
+int gb_plan_get_resident(const gb_plan *plan, int *tile_rows, int *shots_per_launch, int *cluster);
 
 /* Run each group of shots on its own stream (forked from and joined back to
  * the caller's stream; on by default).  Groups never interact, so their

@@ -13,7 +13,7 @@ from test_forward_gpu import _plan_of, run_cuda, synthetic_case
 pytestmark = pytest.mark.gpu
 
 
-def _compare(c, device, fd_order, tile_rows=0, snapshot_every=0, mode=True):
+def _compare(c, device, fd_order, tile_rows=0, snapshot_every=0, mode="global"):
     plan = _plan_of(c, fd_order // 2)
     try:
         plan.set_resident(False)
@@ -92,12 +92,33 @@ def test_eighth_order_against_oracle(cuda_device):
         assert orc.rel_l2(out[k], ref[k]) < 1e-5, k
 
 
+@pytest.mark.parametrize("fd_order", [4, 8])
+@pytest.mark.parametrize("shape,tile_rows", [((37, 53, 4, 70, 1), 0), ((60, 250, 10, 90, 3), 0),
+                                             ((90, 121, 12, 64, 2), 0), ((100, 200, 20, 120, 1), 0),
+                                             ((150, 330, 10, 50, 2), 36), ((150, 330, 10, 50, 2), 48)])
+def test_cluster_exchange_matches_tile_kernel(cuda_device, shape, tile_rows, fd_order):
+    """The cluster exchange (one thread-block cluster per shot, halo strips
+    read from the neighbours' shared memory, cluster barriers): the tile
+    kernel's traces and snapshots bit for bit."""
+    nabc = max(shape[2], fd_order // 2)
+    c = synthetic_case(shape[0], shape[1], nabc, shape[3], shape[4], seed=43)
+    info = _compare(c, cuda_device, fd_order, tile_rows=tile_rows, snapshot_every=16, mode="cluster")
+    assert info["exchange"] == "cluster"
+
+
+@pytest.mark.parametrize("fd_order", [4, 8])
+def test_cluster_exchange_free_surface(cuda_device, fd_order):
+    c = dict(synthetic_case(70, 260, 12, 80, 3, seed=45), free_surface=True)
+    info = _compare(c, cuda_device, fd_order, snapshot_every=20, mode="cluster")
+    assert info["exchange"] == "cluster"
+
+
 def test_invalid_settings(cuda_device):
     """Unknown modes and tile heights are refused; the plan keeps its
     automatic choice."""
     from geobrain_b200 import _lib
     c = synthetic_case(40, 90, 10, 20, 1, seed=41)
     plan = _plan_of(c, 4)
-    for mode, rows in ((2, 0), (1, 10), (-2, 0)):
+    for mode, rows in ((3, 0), (1, 10), (-2, 0)):
         assert plan._lib.gb_plan_set_resident(plan.h, mode, rows) == _lib.GB_E_ARG
     assert plan.resident()["tile_rows"] > 0
