@@ -57,8 +57,9 @@ def parse():
     ap.add_argument("--shots-per-cta", type=int, default=0, help="--slice: shots per CTA of the tile kernel")
     ap.add_argument("--energy", action="store_true", help="--slice: forward with the energy sums")
     ap.add_argument("--absorbing", choices=["damping", "cpml"], default="damping", help="--slice: absorbing layers")
-    ap.add_argument("--resident", choices=["auto", "on", "off"], default="auto",
-                    help="--slice: resident forward (plain forward only)")
+    ap.add_argument("--resident", choices=["auto", "on", "off", "global", "cluster"], default="auto",
+                    help="--slice: resident forward (plain forward only) and its exchange")
+    ap.add_argument("--resident-rows", type=int, default=0, help="--slice: resident tile rows (0 = automatic)")
     return ap.parse_args()
 
 
@@ -92,7 +93,8 @@ def run_slice(args):
     plan.set_absorbing(args.absorbing, float(w.vp.max()) if args.absorbing == "cpml" else 0.0)
     if args.tile_rows or args.shots_per_cta:
         plan.set_tiling(args.tile_rows, args.shots_per_cta)
-    plan.set_resident({"auto": "auto", "on": True, "off": False}[args.resident])
+    plan.set_resident({"auto": "auto", "on": True, "off": False, "global": "global", "cluster": "cluster"}[args.resident],
+                      args.resident_rows)
     vp = torch.tensor(w.vp, device=dev)
     rho = torch.tensor(w.rho, device=dev)
     src_v = torch.tensor(np.tile(w.wavelet, (w.n_shots, 1)), device=dev)
@@ -310,6 +312,16 @@ def large_gradient_check(torch, wave, synthetic, dev, K, formats, shot=7):
     return out
 
 
+def workload_config(w, world, imaging_dtype):
+    """The workload's `config`, printed identically by both arms."""
+    return {"workload": "fwi_400x1200", "grid": [w.nz, w.nx], "nabc": w.nabc, "dx": w.dx, "dt": w.dt,
+            "nt": w.nt, "fd_order": w.fd_order, "n_shots_per_gpu": w.n_shots, "n_receivers": int(w.rcv_x.size),
+            "misfit": "L2 on pressure", "checkpoints": "fp32, auto segment length",
+            "imaging_cache": f"{imaging_dtype}, auto budget",
+            "l2": "inputs larger than L2 (fields 2 x 222 MB per state, no flush needed)",
+            "parallelism": f"shots{world}" if world > 1 else "single GPU"}
+
+
 def run_reference_arm(args):
     """--impl reference: the reference algorithm's CPU restatement on the host
     cores, same metric and config, bounded sample per step."""
@@ -331,9 +343,8 @@ def run_reference_arm(args):
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "fwi_400x1200", "fd_order": 8, "n_shots": 32, "nt": args.nt,
-                   "grid": [400, 1200], "nabc": 30, "sample": sample},
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian-field model, Ricker shots)",
+        "config": workload_config(w, args.gpus, args.imaging_dtype),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -521,12 +532,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Gaussian-field model, Ricker shots)",
-        "config": {"workload": "fwi_400x1200", "grid": [w.nz, w.nx], "nabc": w.nabc, "dx": w.dx, "dt": w.dt,
-                   "nt": w.nt, "fd_order": w.fd_order, "n_shots_per_gpu": S, "n_receivers": int(w.rcv_x.size),
-                   "misfit": "L2 on pressure", "checkpoints": "fp32, auto segment length",
-                   "imaging_cache": f"{args.imaging_dtype}, auto budget ({cached_frac:.0%} of steps cached)",
-                   "l2": "inputs larger than L2 (fields 2 x 222 MB per state, no flush needed)",
-                   "parallelism": f"shots{world}" if world > 1 else "single GPU"},
+        "config": workload_config(w, world, args.imaging_dtype),
         "e2e": {"value": units / (ms_e2e * 1e-3) / 1e9, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e2e},
         "roofline": roofline,
