@@ -52,7 +52,9 @@ def parse():
     ap.add_argument("--slice", choices=["forward", "gradient"], default=None,
                     help="run nt steps of the forward (or forward + adjoint) once and exit (for ncu)")
     ap.add_argument("--shots", type=int, default=32, help="--slice: shots of the 400 x 1200 model")
-    ap.add_argument("--model", choices=["2d", "3d", "100x200"], default="2d", help="--slice: which workload")
+    ap.add_argument("--model", choices=["2d", "3d", "100x200", "ensemble"], default="2d",
+                    help="--slice: which workload")
+    ap.add_argument("--models", type=int, default=6, help="--slice --model ensemble: particles of 256 x 512")
     ap.add_argument("--tile-rows", type=int, default=0, help="--slice: tile kernel rows (16 or 32)")
     ap.add_argument("--shots-per-cta", type=int, default=0, help="--slice: shots per CTA of the tile kernel")
     ap.add_argument("--energy", action="store_true", help="--slice: forward with the energy sums")
@@ -67,8 +69,10 @@ def run_slice(args):
     """A short slice of a benchmark workload, for profilers: nt steps of the
     400 x 1200 / 8th-order model (--shots of its 32 shots; --model 100x200 for
     the 4th-order plain forward workload, --model 3d for a 200^3 model with 4
-    shots), forward or forward + adjoint, once; synchronises and exits 0.
-    Everything stays on the device; nothing is timed.  The gradient keeps
+    shots, --model ensemble for --models particles of the 256 x 512 ensemble
+    through the batched engine), forward or forward + adjoint, once;
+    synchronises and exits 0.  Everything stays on the device; nothing is
+    timed.  The gradient keeps
     every step's imaging fields in --imaging-dtype (fp24 by default, as the
     benchmark does); --absorbing cpml uses the CPML layers."""
     import torch
@@ -77,6 +81,18 @@ def run_slice(args):
     dev = torch.device("cuda:0")
     if args.model == "3d":
         _slice_3d(torch, wave, args, dev)
+        torch.cuda.synchronize()
+        print("slice: ok")
+        return
+    if args.model == "ensemble":
+        ws = synthetic.ensemble_256x512(n_particles=args.models, nt=args.nt)
+        ms = [_model_kwargs(torch, wave, w, dev) for w in ws]
+        if args.slice == "forward":
+            with torch.no_grad():
+                wave.acoustic_forward_batched(ms, fd_order=8, want_energy=args.energy, device=dev)
+        else:
+            wave.acoustic_gradient_batched(ms, lambda i, p: (0.5 * (p * p).sum(), p), fd_order=8, device=dev,
+                                           imaging_dtype=args.imaging_dtype)
         torch.cuda.synchronize()
         print("slice: ok")
         return

@@ -578,11 +578,13 @@ struct GroupStreams {
     cudaStream_t at(int grp) const { return n == 1 ? main : P->gstream[grp]; }
 };
 
-int group_streams(gb_plan *P, cudaStream_t main, GroupStreams *gs)
+// want < 0: one stream per shot group when group streams are on; else
+// `want` streams (the lanes of a batch)
+int group_streams(gb_plan *P, cudaStream_t main, GroupStreams *gs, int want = -1)
 {
     gs->P = P;
     gs->main = main;
-    gs->n = (P->group_streams && P->n_groups > 1) ? P->n_groups : 1;
+    gs->n = want >= 0 ? std::max(1, want) : (P->group_streams && P->n_groups > 1) ? P->n_groups : 1;
     if (gs->n == 1) return GB_OK;
     int dev = -1;
     GB_CUDA(cudaGetDevice(&dev));
@@ -690,13 +692,14 @@ int capture_forward_chunk(gb_plan *P, const StepKernel &K, const Maps (&maps)[2]
 // the step kernels read their step index from that counter.
 template <class Launch>
 int capture_chunk(gb_plan *P, gb_plan::GraphSlot &slot, const std::vector<uintptr_t> &key, int C, int *ctr,
-                  int advance, bool group_streams_on, Launch launch)
+                  int advance, bool group_streams_on, Launch launch, int n_streams = -1)
 {
     if (slot.exec && slot.key == key) return GB_OK;
     slot.release();
     GroupStreams gs;
     if (group_streams_on) {
-        if (int rc = group_streams(P, nullptr, &gs)) return rc;   // (re)creating the group streams drops cap_stream
+        // (re)creating the group streams drops cap_stream
+        if (int rc = group_streams(P, nullptr, &gs, n_streams)) return rc;
     } else {
         gs.P = P;
         gs.n = 1;
@@ -2017,16 +2020,56 @@ int launch_batch(gb_plan *P0, const StepKernel &K, long long n_items, void **arg
     return GB_OK;
 }
 
+// The lanes of a batch: its models split into up to kBatchLanes runs of
+// consecutive models with about equal work items.  Inside a step graph each
+// lane's launches go to a stream of their own, so a lane starts its next
+// step while the others finish this one (no model depends on another).
+constexpr int kBatchLanes = 4;
+struct BatchLanes {
+    int n = 1;
+    long long off[kBatchLanes] = {0}, cnt[kBatchLanes] = {0};
+};
+
+BatchLanes batch_lanes(gb_plan *const *plans, int n_models, long long n_items)
+{
+    BatchLanes L;
+    const int want = std::min(kBatchLanes, n_models);
+    L.cnt[0] = n_items;
+    if (want < 2) return L;
+    long long acc = 0;
+    int lane = 0;
+    L.off[0] = 0;
+    for (int m = 0; m < n_models; ++m) {
+        const long long w = (long long)plans[m]->n_tiles * plans[m]->n_groups;
+        // close the lane once it holds its share (keeping a model for each later lane)
+        if (lane + 1 < want && acc > 0 && acc + w / 2 > n_items * (lane + 1) / want &&
+            n_models - m >= want - lane - 1) {
+            L.cnt[lane] = acc - L.off[lane];
+            L.off[++lane] = acc;
+        }
+        acc += w;
+    }
+    L.cnt[lane] = acc - L.off[lane];
+    L.n = lane + 1;
+    return L;
+}
+
 // A batched step loop in chunks of C steps replayed from the CUDA graph in
-// `slot` (captured once per key): launch(j, stream) launches step j of a
-// chunk, the kernels reading the batch clock at `clock`, which starts at
-// `first` and moves by `dir` * C after each chunk.
+// `slot` (captured once per key): launch(j, lane, stream) launches step j of
+// a chunk for one lane, the kernels reading the batch clock at `clock`,
+// which starts at `first` and moves by `dir` * C after each chunk.
 template <class Launch>
 int batch_graph_chunks(gb_plan *P0, gb_plan::GraphSlot &slot, const std::vector<uintptr_t> &key, int C, int *clock,
-                       int first, int dir, int n_chunks, cudaStream_t st, Launch launch)
+                       int first, int dir, int n_chunks, const BatchLanes &lanes, cudaStream_t st, Launch launch)
 {
-    if (int rc = capture_chunk(P0, slot, key, C, clock, dir * C, false,
-                               [&](int j, const GroupStreams &g) { return launch(j, g.main); }))
+    if (int rc = capture_chunk(
+            P0, slot, key, C, clock, dir * C, lanes.n > 1,
+            [&](int j, const GroupStreams &g) {
+                for (int i = 0; i < lanes.n; ++i)
+                    if (int rc = launch(j, i, lanes.n > 1 ? g.at(i) : g.main)) return rc;
+                return (int)GB_OK;
+            },
+            lanes.n))
         return rc;
     step_set_kernel<<<1, 1, 0, st>>>(clock, first);
     GB_CUDA(cudaGetLastError());
@@ -2034,7 +2077,7 @@ int batch_graph_chunks(gb_plan *P0, gb_plan::GraphSlot &slot, const std::vector<
     ++P0->api_launches;
     for (int k = 0; k < n_chunks; ++k) {
         GB_CUDA(cudaGraphLaunch(slot.exec, st));
-        P0->launches += C + 1;
+        P0->launches += (long long)C * lanes.n + 1;
         ++P0->api_launches;
     }
     return GB_OK;
@@ -2134,8 +2177,9 @@ int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *
     const int C = P0->graph_steps;
     int dev = -1;
     GB_CUDA(cudaGetDevice(&dev));
+    const BatchLanes lanes = batch_lanes(plans, n, B.n_items);
     const std::vector<uintptr_t> key = {(uintptr_t)dev, (uintptr_t)bws, (uintptr_t)B.n_items, (uintptr_t)K0.fn,
-                                        (uintptr_t)C, (uintptr_t)kBatchForward};
+                                        (uintptr_t)C, (uintptr_t)kBatchForward, (uintptr_t)lanes.n};
     for (int tau = 0; tau < maxnt;) {
         for (int m = 0; m < n; ++m) {
             const gb_grad_store *sto = io[m].store;
@@ -2159,13 +2203,14 @@ int gb_batch_forward(gb_plan *const *plans, int n, const gb_model_io *io, void *
                 ++n_chunks;
             }
         if (n_chunks > 0) {
-            if (int rc = batch_graph_chunks(P0, P0->g_batch_fwd, key, C, clock, tau, 1, n_chunks, st,
-                                            [&](int j, cudaStream_t s2) {
+            if (int rc = batch_graph_chunks(P0, P0->g_batch_fwd, key, C, clock, tau, 1, n_chunks, lanes, st,
+                                            [&](int j, int lane, cudaStream_t s2) {
                                                 int tau_v = j;
-                                                void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps,
+                                                const int4 *it_l = items + lanes.off[lane];
+                                                void *args[] = {(void *)&it_l, (void *)&dmodels, (void *)&dmaps,
                                                                 (void *)&tau_v, (void *)&mode, (void *)&t0,
                                                                 (void *)&clock};
-                                                return launch_batch(P0, K0, B.n_items, args, s2);
+                                                return launch_batch(P0, K0, lanes.cnt[lane], args, s2);
                                             }))
                 return rc;
             tau += n_chunks * C;
@@ -2296,8 +2341,9 @@ int gb_batch_backward(gb_plan *const *plans, int n, const gb_model_io *io, void 
     const int C = P0->graph_steps;
     int dev = -1;
     GB_CUDA(cudaGetDevice(&dev));
+    const BatchLanes lanes = batch_lanes(plans, n, B.n_items);
     const std::vector<uintptr_t> akey = {(uintptr_t)dev, (uintptr_t)bws, (uintptr_t)B.n_items, (uintptr_t)KA.fn,
-                                         (uintptr_t)C};
+                                         (uintptr_t)C, (uintptr_t)lanes.n};
     // batch-wide segments of K steps; a model recomputes a segment only for
     // its steps below min(nt, t_cache)
     const int Kb = std::min(K, maxnt);
@@ -2333,12 +2379,13 @@ int gb_batch_backward(gb_plan *const *plans, int n, const gb_model_io *io, void 
         // chunks of C steps replayed from one graph (the clock counts down)
         const int n_chunks = C > 0 ? (t1 - t0) / C : 0;
         if (n_chunks > 0) {
-            if (int rc = batch_graph_chunks(P0, P0->g_batch_adj, akey, C, clock, tau, -1, n_chunks, st,
-                                            [&](int j, cudaStream_t s2) {
+            if (int rc = batch_graph_chunks(P0, P0->g_batch_adj, akey, C, clock, tau, -1, n_chunks, lanes, st,
+                                            [&](int j, int lane, cudaStream_t s2) {
                                                 int tau_v = j;
-                                                void *args[] = {(void *)&items, (void *)&dmodels, (void *)&dmaps,
+                                                const int4 *it_l = items + lanes.off[lane];
+                                                void *args[] = {(void *)&it_l, (void *)&dmodels, (void *)&dmaps,
                                                                 (void *)&tau_v, (void *)&clock};
-                                                return launch_batch(P0, KA, B.n_items, args, s2);
+                                                return launch_batch(P0, KA, lanes.cnt[lane], args, s2);
                                             }))
                 return rc;
             tau -= n_chunks * C;

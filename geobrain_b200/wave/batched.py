@@ -309,8 +309,9 @@ def acoustic_gradient_batched(models: Sequence[dict], residual, *, fd_order: int
     sub-batch starts.  Nothing is recomputed unless one model alone does not
     fit, in which case that model keeps checkpoints (in `snapshot_dtype`)
     for the steps that do not.  memory_budget: the bytes a sub-batch may
-    hold (default: the free device memory less 2 GiB and 5 %).  Under autograd (acoustic_forward_batched and
-    loss.backward()) every model's store must survive until the backward, so
+    hold (default: the free device memory less 2 GiB and 5 %).  Under
+    autograd (acoustic_forward_batched and loss.backward()) every model's
+    store must survive until the backward, so
     an ensemble larger than the device memory recomputes its uncached steps;
     this call does not.
 
