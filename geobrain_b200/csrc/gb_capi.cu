@@ -234,15 +234,24 @@ struct gb_plan {
         const int use_spc = spc > 0 ? spc : default_spc();
         n_groups = (d.n_shots + use_spc - 1) / use_spc;
         spc_eff = use_spc;
-        rcv_ptr.assign(n_tiles + 1, 0);
-        for (int r = 0; r < d.n_rcv; ++r) rcv_ptr[(rcv_z[r] / tz) * tiles_x + rcv_x[r] / TX + 1]++;
-        for (int t = 0; t < n_tiles; ++t) rcv_ptr[t + 1] += rcv_ptr[t];
-        rcv_ent.assign(d.n_rcv, int4{0, 0, 0, 0});
-        std::vector<int> fill(rcv_ptr.begin(), rcv_ptr.end() - 1);
+        // (tile, (row in tile, col in tile, receiver, what)): what = 1 records
+        // p and vx, 2 records vz, 3 both.  A receiver in row fs-1 under a
+        // free surface records vz after the mirror vz[fs-1] = vz[fs]
+        // (acoustic_2d.py:268-274), i.e. vz of row fs, which the tile that
+        // owns row fs updates in the same step: its vz entry goes there.
+        std::vector<std::pair<int, int4>> ents;
         for (int r = 0; r < d.n_rcv; ++r) {
-            const int t = (rcv_z[r] / tz) * tiles_x + rcv_x[r] / TX;
-            rcv_ent[fill[t]++] = int4{rcv_z[r] - (rcv_z[r] / tz) * tz, rcv_x[r] - (rcv_x[r] / TX) * TX, r, 0};
+            const int z = rcv_z[r], x = rcv_x[r], bx = x / TX;
+            const bool split = d.free_surface && z == fs - 1;
+            ents.push_back({(z / tz) * tiles_x + bx, int4{z - (z / tz) * tz, x - bx * TX, r, split ? 1 : 3}});
+            if (split) ents.push_back({((z + 1) / tz) * tiles_x + bx, int4{z + 1 - ((z + 1) / tz) * tz, x - bx * TX, r, 2}});
         }
+        rcv_ptr.assign(n_tiles + 1, 0);
+        for (const auto &e : ents) rcv_ptr[e.first + 1]++;
+        for (int t = 0; t < n_tiles; ++t) rcv_ptr[t + 1] += rcv_ptr[t];
+        rcv_ent.assign(ents.size(), int4{0, 0, 0, 0});
+        std::vector<int> fill(rcv_ptr.begin(), rcv_ptr.end() - 1);
+        for (const auto &e : ents) rcv_ent[fill[e.first]++] = e.second;
         // adjoint: every tile whose halo rectangles [z0-2R, z0+tz+2R) x
         // [x0-8, x0+TX+8) contain the receiver injects it into its copy
         arcv_ptr.assign(n_tiles + 1, 0);
@@ -292,9 +301,10 @@ struct gb_plan {
     // Choose the resident tiling.  Automatic mode runs it when every shot's
     // tiles fit on the SMs at once (few shots or a small grid: the cases
     // where the per-step tile kernel is launch- and latency-bound), with the
-    // cluster exchange when one shot's tiles fit in one cluster, else the
-    // exchange through global memory; each with the smallest tile height
-    // that fits.  More shots keep the tile kernel.
+    // exchange through global memory and the smallest tile height that fits
+    // (the most CTAs); the cluster exchange, limited to 16 CTAs a shot,
+    // measured no faster, and runs when asked for.  More shots keep the tile
+    // kernel.
     void res_choose()
     {
         res_tz = 0;
@@ -303,7 +313,8 @@ struct gb_plan {
         const int sms = sm_count();
         int best = 0;
         for (int pass = 0; pass < 2 && !best; ++pass) {
-            const bool cl = pass == 0;
+            const bool cl = pass == 1;
+            if (cl && res_mode < 0) continue;
             if ((cl && res_mode == 1) || (!cl && res_mode == 2)) continue;
             for (int tz : kResidentRows) {
                 if (res_tz_req && tz != res_tz_req) continue;
@@ -386,7 +397,7 @@ namespace {
 // Workspace layout (offsets in bytes from the 256-aligned base).
 struct Layout {
     size_t err, coef, fields, energy, src, rcv_ptr, rcv_ent, tile_fast, amax, cpml, psi, total;
-    size_t res_ptr, res_ent, res_x, res_fl;   // resident forward: receiver CSR, exchange strips, flags
+    size_t res_ptr, res_ent, res_x;           // resident forward: receiver CSR, exchange strips
     // gradient only
     size_t mu, img, g1, c1, g2, c2, arcv_ptr, arcv_ent, cprcv, cpcoef;
     int n_img;
@@ -408,7 +419,7 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
     L.energy = o; o = align256(o + 3 * p->plane * 4);
     L.src = o; o = align256(o + 2 * S * 4);
     L.rcv_ptr = o; o = align256(o + (p->n_tiles + 1) * 4);
-    L.rcv_ent = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 16);
+    L.rcv_ent = o; o = align256(o + std::max<size_t>(p->rcv_ent.size(), 1) * 16);
     L.tile_fast = o; o = align256(o + (size_t)p->n_tiles * 4);
     L.amax = o; o = align256(o + S * 3 * 4);
     if (p->cpml) {
@@ -419,8 +430,7 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
         const ResidentKernel k = resident_kernel(p->R, p->res_tz, false);
         L.res_ptr = o; o = align256(o + (p->res_n + 1) * 4);
         L.res_ent = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 16);
-        L.res_x = o; o = align256(o + S * p->res_n * kResParts * k.part_floats * 4);
-        L.res_fl = o; o = align256(o + S * p->res_n * kResFlagStride * 4);
+        L.res_x = o; o = align256(o + S * p->res_n * kResParts * k.part_words * 8);
     }
     L.n_img = with_gradient >= 2 ? 3 : 1;
     if (with_gradient > 0) {
@@ -840,7 +850,8 @@ int common_setup(gb_plan *P, const Layout &L, char *ws, const float *vp, const f
     GB_CUDA(cudaMemcpyAsync(S->d_src, P->src_z.data(), d.n_shots * 4, cudaMemcpyHostToDevice, st));
     GB_CUDA(cudaMemcpyAsync(S->d_src + d.n_shots, P->src_x.data(), d.n_shots * 4, cudaMemcpyHostToDevice, st));
     GB_CUDA(cudaMemcpyAsync(S->d_rptr, P->rcv_ptr.data(), (P->n_tiles + 1) * 4, cudaMemcpyHostToDevice, st));
-    if (d.n_rcv) GB_CUDA(cudaMemcpyAsync(S->d_rent, P->rcv_ent.data(), d.n_rcv * 16, cudaMemcpyHostToDevice, st));
+    if (!P->rcv_ent.empty())
+        GB_CUDA(cudaMemcpyAsync(S->d_rent, P->rcv_ent.data(), P->rcv_ent.size() * 16, cudaMemcpyHostToDevice, st));
     coef_kernel<<<4 * 148, 256, 0, st>>>(vp, rho, damp, d.nz, d.nx, d.nabc, P->Nz, P->Nx, P->pitch, P->fs, d.dt, d.dx,
                                          S->a1, S->k1, S->a2, S->k2, S->k3);
     GB_CUDA(cudaGetLastError());
@@ -900,10 +911,11 @@ int forward_resident(gb_plan *P, const Layout &L, char *ws, const Setup &Su, flo
     if (P->res_cluster && P->res_n > 8) GB_CUDA(cudaFuncSetAttribute(K.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     int *d_ptr = reinterpret_cast<int *>(ws + L.res_ptr);
     int4 *d_ent = reinterpret_cast<int4 *>(ws + L.res_ent);
-    unsigned int *flags = reinterpret_cast<unsigned int *>(ws + L.res_fl);
     GB_CUDA(cudaMemcpyAsync(d_ptr, P->res_ptr.data(), (P->res_n + 1) * 4, cudaMemcpyHostToDevice, st));
     if (d.n_rcv) GB_CUDA(cudaMemcpyAsync(d_ent, P->res_ent.data(), d.n_rcv * 16, cudaMemcpyHostToDevice, st));
-    GB_CUDA(cudaMemsetAsync(flags, 0, (size_t)S * P->res_n * kResFlagStride * 4, st));
+    // the strips' tags start at 0, which no step's tag is
+    if (!P->res_cluster)
+        GB_CUDA(cudaMemsetAsync(ws + L.res_x, 0, (size_t)S * P->res_n * kResParts * K.part_words * 8, st));
     ResArgs A{};
     A.g = P->geom();
     A.tiles_x = P->res_tiles_x;
@@ -918,8 +930,7 @@ int forward_resident(gb_plan *P, const Layout &L, char *ws, const Setup &Su, flo
     A.rcv_ptr = d_ptr; A.rcv_ent = d_ent;
     A.tr_p = trace_p; A.tr_vx = trace_vx; A.tr_vz = trace_vz;
     A.energy_map = want_energy ? energy : nullptr;
-    A.xbuf = reinterpret_cast<float *>(ws + L.res_x);
-    A.flags = flags;
+    A.xbuf = reinterpret_cast<uint2 *>(ws + L.res_x);
     A.err = Su.err;
     int snap_i = 0;
     for (int s0 = 0; s0 < S; s0 += P->res_shots) {
@@ -1160,7 +1171,7 @@ int gb_plan_set_resident(gb_plan *p, int mode, int tile_rows)
         return fail(GB_E_ARG, "mode must be -1 (automatic), 0 (off), 1 (global exchange) or 2 (cluster exchange)");
     bool known = tile_rows == 0;
     for (int tz : kResidentRows) known |= tz == tile_rows;
-    if (!known) return fail(GB_E_ARG, "tile_rows must be 0, 4, 8, 12, 16, 24, 32, 36, 40 or 48");
+    if (!known) return fail(GB_E_ARG, "tile_rows must be 0, 4, 8, 12, 16, 24, 32, 36 or 40");
     p->res_mode = mode;
     p->res_tz_req = tile_rows;
     p->res_choose();

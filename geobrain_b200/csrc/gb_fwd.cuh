@@ -49,7 +49,7 @@ struct FwdArgs {
     const int *src_z, *src_x;        // padded source cells
     const float *wavelet;            // [S][nt]
     const int *rcv_ptr;              // CSR over tiles
-    const int4 *rcv_ent;             // (row in tile, col in tile, receiver, 0)
+    const int4 *rcv_ent;             // (row in tile, col in tile, receiver, 1: p and vx / 2: vz / 3: all)
     float *tr_p, *tr_vx, *tr_vz;     // [S][nt][n_rcv] or null
     float *energy;                   // [3][plane] padded accumulators or null
     float *imaging;                  // [S][plane] -div(v) on the p mask, or null
@@ -413,9 +413,11 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
                 const int4 en = A.rcv_ent[e];
                 const int rr = en.x + R, cc = en.y + 4;
                 const long long t = ((long long)s * g.nt + it) * g.n_rcv + en.z;
-                if (A.tr_p) A.tr_p[t] = sP[rr * RW + cc];
-                if (A.tr_vx) A.tr_vx[t] = sVX[rr * VXW + cc + 4];
-                if (A.tr_vz) A.tr_vz[t] = sVZ[(en.x + 2 * R) * RW + cc];
+                if (en.w & 1) {
+                    if (A.tr_p) A.tr_p[t] = sP[rr * RW + cc];
+                    if (A.tr_vx) A.tr_vx[t] = sVX[rr * VXW + cc + 4];
+                }
+                if ((en.w & 2) && A.tr_vz) A.tr_vz[t] = sVZ[(en.x + 2 * R) * RW + cc];
             }
         }
         // order this iteration's generic-proxy shared-memory writes before the

@@ -36,12 +36,12 @@ namespace host {
 
 // resident_fwd_kernel<R, NW, TZ> (gb_resident.cuh) for the tile heights in
 // kResidentRows; fn is null for other heights.  gb_pick_resident.cu.
-constexpr int kResidentRows[] = {4, 8, 12, 16, 24, 32, 36, 40, 48};
+constexpr int kResidentRows[] = {4, 8, 12, 16, 24, 32, 36, 40};
 struct ResidentKernel {
     void *fn = nullptr;
     size_t smem = 0;
     int threads = 0;
-    size_t part_floats = 0;     // floats per exchange strip
+    size_t part_words = 0;      // 8-byte (value, tag) words per exchange strip
 };
 // cluster: the variant that exchanges through distributed shared memory
 // within one thread-block cluster per shot (tiles of a shot <= 16).

@@ -1,7 +1,9 @@
 // Instantiates the resident forward kernels (gb_resident.cuh) for each tile
-// height: 4 warps for 4-row tiles, 8 for 8 and 12, 12 for 36, 16 otherwise;
-// each with the exchange through global memory and flags, and through
-// distributed shared memory within a cluster.
+// height: 4 warps for 4-row tiles, 8 for 8 and 12, 12 for 36, 16 otherwise
+// (measured against one boundary item per thread and two interior rows per
+// warp, which ran 7 % slower on the 400 x 1200 grid and 26 % on 100 x 200
+// with 8-row tiles); each with the exchange through global memory ((value,
+// tag) words), and through distributed shared memory within a cluster.
 #include "gb_kernels.h"
 #include "gb_resident.cuh"
 
@@ -19,7 +21,7 @@ ResidentKernel make()
     k.fn = (void *)&resident_fwd_kernel<R, NW, TZ, CL>;
     k.smem = G::SMEM;
     k.threads = G::NTH;
-    k.part_floats = G::PART;
+    k.part_words = G::PART;
     return k;
 }
 
@@ -35,7 +37,6 @@ ResidentKernel pick(int tz)
     case 32: return make<R, 16, 32, CL>();
     case 36: return make<R, 12, 36, CL>();
     case 40: return make<R, 16, 40, CL>();
-    case 48: return make<R, 16, 48, CL>();
     default: return ResidentKernel{};
     }
 }

@@ -321,9 +321,11 @@ fwd_stream_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant_
                 const int4 en = A.rcv_ent[e];
                 const int zr = a + en.x, cc = en.y + 4;
                 const long long t = ((long long)s * g.nt + it) * g.n_rcv + en.z;
-                if (A.tr_p) A.tr_p[t] = sP[ring_row(zr, base_p) * RW + cc];
-                if (A.tr_vx) A.tr_vx[t] = sVX[ring_row(zr, base_p) * VXW + cc + 4];
-                if (A.tr_vz) A.tr_vz[t] = sVZ[ring_row(zr, base_vz) * RW + cc];
+                if (en.w & 1) {
+                    if (A.tr_p) A.tr_p[t] = sP[ring_row(zr, base_p) * RW + cc];
+                    if (A.tr_vx) A.tr_vx[t] = sVX[ring_row(zr, base_p) * VXW + cc + 4];
+                }
+                if ((en.w & 2) && A.tr_vz) A.tr_vz[t] = sVZ[ring_row(zr, base_vz) * RW + cc];
             }
         }
         // order this chunk's generic-proxy shared-memory writes before the TMA

@@ -184,10 +184,10 @@ class Plan:
 
     def set_resident(self, mode, tile_rows: int = 0) -> None:
         """Resident forward: 'auto' (default), False (off), True or 'global'
-        (on, halo strips through global memory and flags), or 'cluster' (on,
-        strips through distributed shared memory, one cluster of at most 16
-        CTAs per shot); tile_rows 0 (smallest that fits) or one of 4, 8, 12,
-        16, 24, 32, 36, 40, 48."""
+        (on, edge cells through global memory as (value, tag) words), or
+        'cluster' (on, edge cells stored into the neighbours' shared memory,
+        one cluster of at most 16 CTAs per shot); tile_rows 0 (smallest that
+        fits) or one of 4, 8, 12, 16, 24, 32, 36, 40."""
         m = {"auto": -1, False: 0, True: 1, "global": 1, "cluster": 2}[mode]
         _lib.check(self._lib.gb_plan_set_resident(self.h, m, int(tile_rows)))
 

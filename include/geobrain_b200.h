@@ -169,26 +169,27 @@ int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const flo
                      void *stream, float *best_ms_per_step);
 
 /* Resident forward (plain gb_forward without a store, damping layers only):
- * one cooperative launch runs many time steps, each CTA keeping a 120-column
- * x tile_rows tile of one shot, plus its halo, in shared memory, and
- * exchanging the halo strips with its four neighbours through global memory
- * and flags (bounded waits) after the pressure and the velocity updates.
+ * one launch runs many time steps, each CTA keeping a 120-column x
+ * tile_rows tile of one shot, plus its halo, in shared memory.  The thread
+ * that updates a cell next to a tile edge sends it to the neighbouring
+ * tile, and the rest of the tile is updated while it travels.
  * It is the plain forward's fast path when a step is too small to fill the
  * GPU: few shots, or a small grid.  The traces are those of the tile kernel,
  * bit for bit.  mode: -1 automatic (the default: on when every shot's tiles
- * fit on the device's SMs at once, one CTA per SM, with the cluster exchange
- * when one shot's tiles fit in one cluster), 0 off, 1 on with the exchange
- * through global memory and flags (whenever a tiling fits; shots beyond one
- * cooperative launch run in further launches), 2 on with the exchange
- * through distributed shared memory: one thread-block cluster of at most 16
- * CTAs per shot, hardware cluster barriers in place of the flags.
- * tile_rows: 4, 8, 12, 16, 24, 32, 36, 40 or 48, or 0 for the smallest that
- * fits.  Each step updates the cells next to the tile edges first, posts
- * them, and updates the rest while the neighbours' strips travel.
- * With a free surface, rows fs-1 .. fs+1 must fall in one tile.
+ * fit on the device's SMs at once, one CTA per SM, with the exchange through
+ * global memory and the smallest tile height that fits), 0 off, 1 on with
+ * the exchange
+ * through global memory (a cooperative launch; each float travels as an
+ * 8-byte (value, tag) word the receiver polls, bounded; shots beyond one
+ * launch run in further launches), 2 on with the exchange through
+ * distributed shared memory: one thread-block cluster of at most 16 CTAs per
+ * shot, the sender storing into the neighbour's halo, hardware cluster
+ * barriers in place of the tags.
+ * tile_rows: 4, 8, 12, 16, 24, 32, 36 or 40, or 0 for the smallest that
+ * fits.  With a free surface, rows fs-1 .. fs+1 must fall in one tile.
  * GB_E_UNSUPPORTED when mode 1 finds no tiling (or the plan uses CPML); the
  * plan then stays automatic.  The workspace (gb_plan_workspace_bytes) grows
- * by the exchange strips and flags. */
+ * by the exchange strips. */
 int gb_plan_set_resident(gb_plan *plan, int mode, int tile_rows);
 /* Tile rows of the resident forward in use (0: the tile kernel runs),
  * shots per launch, and whether the cluster exchange runs (1) or the

@@ -52,10 +52,13 @@ def _plan(lib, **over):
 def test_plan_create_and_sizes(lib):
     rc, h = _plan(lib)
     assert rc == 0, lib.gb_last_error()
-    fwd = lib.gb_plan_workspace_bytes(h, 0, 0)
+    fwd = lib.gb_plan_workspace_bytes(h, 0, 0)      # with the resident forward's exchange strips
     grad = lib.gb_plan_workspace_bytes(h, 1, 10)
     grad_rho = lib.gb_plan_workspace_bytes(h, 2, 10)
-    assert 0 < fwd < grad < grad_rho
+    assert lib.gb_plan_set_resident(h, 0, 0) == 0
+    fwd_tile = lib.gb_plan_workspace_bytes(h, 0, 0)
+    assert lib.gb_plan_set_resident(h, -1, 0) == 0
+    assert 0 < fwd_tile < fwd and fwd_tile < grad < grad_rho
     ck32 = lib.gb_plan_checkpoint_bytes(h, 10, 0)
     ck16 = lib.gb_plan_checkpoint_bytes(h, 10, 1)
     assert ck16 < ck32 and ck32 == 5 * 2 * 3 * (40 + 16) * 96 * 4

@@ -265,3 +265,39 @@ def test_streaming_kernel_is_not_used_with_a_free_surface(cuda_device):
         plan.set_streaming(False)
         plan.set_resident("auto")
     np.testing.assert_array_equal(out["p"], base["p"])
+
+
+@pytest.mark.parametrize("nabc,tile_rows,resident", [(12, 16, False), (16, 16, False), (16, 32, False),
+                                                     (12, 0, True)])
+def test_receivers_above_the_free_surface(cuda_device, nabc, tile_rows, resident):
+    """Receivers in row fs-1 (one above the surface) record vz after the
+    mirror vz[fs-1] = vz[fs] of the same step (acoustic_2d.py:268-274): the
+    tile kernel takes their vz from the tile that updates row fs (the same
+    tile, or, with nabc = 16 and 16-row tiles, the next one).  Every
+    receiver's traces against the float64 oracle; receivers in rows fs-1,
+    fs and fs+1."""
+    c = dict(synthetic_case(50, 200, nabc, 150, 2, seed=7), free_surface=True)
+    rx = np.arange(0, 200, 7)
+    c["rcv_x"] = np.concatenate([rx, rx, rx])
+    c["rcv_z"] = np.concatenate([np.full(rx.size, -1), np.zeros(rx.size, np.int64), np.ones(rx.size, np.int64)])
+    c["src_z"] = np.array([0, 3])
+    c["src_x"] = np.array([40, 150])
+    plan = _plan_of(c, 4)
+    plan.set_resident(resident)
+    if tile_rows:
+        plan.set_tiling(tile_rows, 0)
+    try:
+        out = run_cuda(c, cuda_device, fd_order=8)
+        if resident:
+            assert plan.resident()["tile_rows"] > 0
+    finally:
+        plan.set_tiling(0, 0)
+        plan.set_resident("auto")
+    ref = orc.forward(**oracle_kwargs(c), half=4, dtype=np.float64)
+    for k in ("p", "vx", "vz"):
+        # per receiver, relative to its own trace (or to a thousandth of the
+        # field's, for traces the wave has barely reached)
+        floor = 1e-3 * np.linalg.norm(ref[k]) / np.sqrt(c["rcv_x"].size)
+        for r in range(c["rcv_x"].size):
+            err = np.linalg.norm(out[k][:, :, r] - ref[k][:, :, r]) / max(np.linalg.norm(ref[k][:, :, r]), floor)
+            assert err < TOL, (k, r, c["rcv_z"][r], err)
