@@ -69,13 +69,13 @@ __device__ __forceinline__ void neumaier_add(float &s, float &c, float x)
 // A.img_fmt at run time (batched launches, where it varies per model).
 template <int R, int TZ, bool FS, bool RHO, int IMGF>
 __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMap *mVX, const CUtensorMap *mVZ,
-                                         const CUtensorMap *mA1, const CUtensorMap *mA2, const AdjArgs &A,
-                                         const int group, const int tile)
+                                         const CUtensorMap *mA1, const CUtensorMap *mA2,
+                                         const AdjArgs &__restrict__ A, const int group, const int tile)
 {
     const int img_fmt = IMGF >= 0 ? IMGF : A.img_fmt;
     using G = Geo<R, TZ>;
     using SM = StepSmem<R, TZ>;
-    const StepGeom &g = A.g;
+    const StepGeom &__restrict__ g = A.g;
     extern __shared__ __align__(128) float smem[];
     float *sA1 = smem + 2 * G::STAGE_FL;
     float *sA2 = sA1 + SM::A1_FL;

@@ -113,12 +113,12 @@ __device__ __forceinline__ bool tile_is_interior(const StepGeom &g, int z0, int 
 // a1 / a2 planes.
 template <int R, int TZ, bool FS, bool ENERGY, int IMG>
 __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMap *mVX, const CUtensorMap *mVZ,
-                                         const CUtensorMap *mA1, const CUtensorMap *mA2, const FwdArgs &A,
-                                         const int group, const int tile)
+                                         const CUtensorMap *mA1, const CUtensorMap *mA2,
+                                         const FwdArgs &__restrict__ A, const int group, const int tile)
 {
     using G = Geo<R, TZ>;
     using SM = StepSmem<R, TZ>;
-    const StepGeom &g = A.g;
+    const StepGeom &__restrict__ g = A.g;
     extern __shared__ __align__(128) float smem[];
     __shared__ int2 s_src[kMaxShotsPerCta];   // (z, x) source cell of each shot of this CTA
     float *sA1 = smem + 2 * G::STAGE_FL;
