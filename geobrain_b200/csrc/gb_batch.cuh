@@ -82,7 +82,9 @@ fwd_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ 
                                      item.y);
 }
 
-template <int R, int TZ, bool FS, bool RHO>
+// IMGF: the imaging format every model of the batch stores (kImg*), or -1
+// to read each model's at run time.
+template <int R, int TZ, bool FS, bool RHO, int IMGF>
 __global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
 adj_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ models,
                  const BatchMaps *__restrict__ maps, int tau, const int *clock)
@@ -103,7 +105,7 @@ adj_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ 
     }
     __syncthreads();
     const BatchMaps &mp = maps[item.x];
-    adj_body<R, TZ, FS, RHO, -1>(&mp.mu[par][0], &mp.mu[par][1], &mp.mu[par][2], &mp.a1, &mp.a2, A, item.z, item.y);
+    adj_body<R, TZ, FS, RHO, IMGF>(&mp.mu[par][0], &mp.mu[par][1], &mp.mu[par][2], &mp.a1, &mp.a2, A, item.z, item.y);
 }
 
 }  // namespace gb

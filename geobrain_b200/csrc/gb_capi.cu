@@ -2341,7 +2341,10 @@ int gb_batch_backward(gb_plan *const *plans, int n, const gb_model_io *io, void 
     }
     if (int rc = upload_batch(plans, n, models, maps, bws, B, st)) return rc;
     const StepKernel KF = fwd_batch_kernel_for(P0->R, fs, false, rho ? 2 : 1);
-    const StepKernel KA = adj_batch_kernel_for(P0->R, fs, rho);
+    int imgf = io[0].store->imaging_format;
+    for (int m = 1; m < n; ++m)
+        if (io[m].store->imaging_format != imgf) imgf = -1;
+    const StepKernel KA = adj_batch_kernel_for(P0->R, fs, rho, imgf);
     if (int rc = prepare_kernel(KF)) return rc;
     if (int rc = prepare_kernel(KA)) return rc;
     const int4 *items = reinterpret_cast<const int4 *>(bws + B.items);

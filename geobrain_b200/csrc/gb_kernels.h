@@ -26,7 +26,8 @@ StepKernel adj_tile_kernel_r2(int tz, bool fs, bool rho, int img_fmt);
 StepKernel adj_tile_kernel_r4(int tz, bool fs, bool rho, int img_fmt);
 // fwd_batch_kernel / adj_batch_kernel (gb_batch.cuh), 16-row tiles.  gb_pick_batch.cu.
 StepKernel fwd_batch_kernel_for(int R, bool fs, bool en, int img);
-StepKernel adj_batch_kernel_for(int R, bool fs, bool rho);
+// imgf: the imaging format all models of the batch store, or -1 (per model)
+StepKernel adj_batch_kernel_for(int R, bool fs, bool rho, int imgf);
 
 }  // namespace host
 }  // namespace gb

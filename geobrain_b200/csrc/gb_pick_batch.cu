@@ -1,4 +1,5 @@
-// Instantiates the batched step kernels (gb_batch.cuh), 16-row tiles.
+// Instantiates the batched forward step kernels (gb_batch.cuh), 16-row tiles
+// (the adjoint ones: gb_pick_batch_adj.cu).
 #include "gb_batch.cuh"
 #include "gb_kernels.h"
 
@@ -16,12 +17,6 @@ void *pick_fwd(bool en, int img)
     return en ? (void *)&fwd_batch_kernel<R, 16, FS, true, 0> : (void *)&fwd_batch_kernel<R, 16, FS, false, 0>;
 }
 
-template <int R, bool FS>
-void *pick_adj(bool rho)
-{
-    return rho ? (void *)&adj_batch_kernel<R, 16, FS, true> : (void *)&adj_batch_kernel<R, 16, FS, false>;
-}
-
 }  // namespace
 
 StepKernel fwd_batch_kernel_for(int R, bool fs, bool en, int img)
@@ -33,19 +28,6 @@ StepKernel fwd_batch_kernel_for(int R, bool fs, bool en, int img)
     } else if (R == 4) {
         k.fn = fs ? pick_fwd<4, true>(en, img) : pick_fwd<4, false>(en, img);
         k.smem = fwd_smem_bytes<4, 16>();
-    }
-    return k;
-}
-
-StepKernel adj_batch_kernel_for(int R, bool fs, bool rho)
-{
-    StepKernel k;
-    if (R == 2) {
-        k.fn = fs ? pick_adj<2, true>(rho) : pick_adj<2, false>(rho);
-        k.smem = adj_smem_bytes<2, 16>();
-    } else if (R == 4) {
-        k.fn = fs ? pick_adj<4, true>(rho) : pick_adj<4, false>(rho);
-        k.smem = adj_smem_bytes<4, 16>();
     }
     return k;
 }
