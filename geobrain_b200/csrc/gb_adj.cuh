@@ -173,19 +173,26 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
                 const int gz = en.x, gx = en.y;
                 const long long t = ((long long)s * g.nt + it) * g.n_rcv + en.z;
                 const long long o = (long long)gz * g.pitch + gx;
-                if (A.res_p && gz >= g.p_r0 && gz <= g.p_r1 && gx >= g.p_c0 && gx <= g.p_c1) {
-                    const int r = gz - (z0 - R), c = gx - (x0 - 4);
-                    if (r >= 0 && r < G::PR && c >= 0 && c < RW) atomicAdd(&sP[r * RW + c], A.a1[o] * A.res_p[t]);
+                // a receiver in the mirror row fs-1 records p[fs-1] = -p[fs+1]
+                // and vz[fs-1] = vz[fs] (acoustic_2d.py:240-241, 268-274):
+                // its adjoint sources go to those rows
+                const bool mir = FS && gz == g.fs - 1;
+                const int zp = mir ? g.fs + 1 : gz, zv = mir ? g.fs : gz;
+                if (A.res_p && zp >= g.p_r0 && zp <= g.p_r1 && gx >= g.p_c0 && gx <= g.p_c1) {
+                    const int r = zp - (z0 - R), c = gx - (x0 - 4);
+                    const long long op = (long long)zp * g.pitch + gx;
+                    const float src = A.a1[op] * A.res_p[t];
+                    if (r >= 0 && r < G::PR && c >= 0 && c < RW) atomicAdd(&sP[r * RW + c], mir ? -src : src);
                 }
                 if (A.res_vx && gz >= g.vx_r0 && gz <= g.vx_r1 && gx >= g.vx_c0 && gx <= g.vx_c1) {
                     const int r = gz - (z0 - R), c = gx - (x0 - 8);
                     if (r >= 0 && r < G::PR && c >= 0 && c < VXW)
                         atomicAdd(&sVX[r * VXW + c], A.a2[o] * A.res_vx[t]);
                 }
-                if (A.res_vz && gz >= g.vz_r0 && gz <= g.vz_r1 && gx >= g.vz_c0 && gx <= g.vz_c1) {
-                    const int r = gz - (z0 - 2 * R), c = gx - (x0 - 4);
+                if (A.res_vz && zv >= g.vz_r0 && zv <= g.vz_r1 && gx >= g.vz_c0 && gx <= g.vz_c1) {
+                    const int r = zv - (z0 - 2 * R), c = gx - (x0 - 4);
                     if (r >= 0 && r < G::ZR && c >= 0 && c < RW)
-                        atomicAdd(&sVZ[r * RW + c], A.a2[o] * A.res_vz[t]);
+                        atomicAdd(&sVZ[r * RW + c], A.a2[(long long)zv * g.pitch + gx] * A.res_vz[t]);
                 }
             }
             __syncthreads();

@@ -259,13 +259,16 @@ struct gb_plan {
         std::vector<std::vector<int4>> per(n_tiles);
         for (int r = 0; r < d.n_rcv; ++r) {
             const int z = rcv_z[r], x = rcv_x[r];
+            // rows whose adjoint takes this receiver's sources: its own, or,
+            // in the mirror row fs-1 under a free surface, rows fs and fs+1
+            const int zl = z, zh = (d.free_surface && z == fs - 1) ? z + 2 : z;
             // candidate tiles (a superset; the test below is exact)
-            const int tz_lo = std::max(0, (z - 2 * R) / tz - 1), tz_hi = std::min(tiles_z - 1, (z + 2 * R) / tz + 1);
+            const int tz_lo = std::max(0, (zl - 2 * R) / tz - 1), tz_hi = std::min(tiles_z - 1, (zh + 2 * R) / tz + 1);
             const int tx_lo = std::max(0, (x - 8) / TX - 1), tx_hi = std::min(tiles_x - 1, (x + 8) / TX + 1);
             for (int a = tz_lo; a <= tz_hi; ++a)
                 for (int b = tx_lo; b <= tx_hi; ++b) {
                     const int z0 = a * tz, x0 = b * TX;
-                    if (z >= z0 - 2 * R && z < z0 + tz + 2 * R && x >= x0 - 8 && x < x0 + TX + 8)
+                    if (zh >= z0 - 2 * R && zl < z0 + tz + 2 * R && x >= x0 - 8 && x < x0 + TX + 8)
                         per[a * tiles_x + b].push_back(int4{z, x, r, 0});
                 }
         }

@@ -259,3 +259,24 @@ def test_wavelet_gradient_refuses_sources_outside_the_update_region(cuda_device)
     c = dict(c, src_z=np.array([1, 1, -c["nabc"]]))          # the last shot on the outermost padded row
     with pytest.raises(NotImplementedError):
         _wavelet_run(c, cuda_device, 4, False)
+
+
+@pytest.mark.parametrize("nabc", [12, 16])
+def test_gradient_with_receivers_above_the_free_surface(cuda_device, nabc):
+    """Receivers in rows fs-1, fs and fs+1 under a free surface, a loss linear
+    in all three traces: the vz trace in row fs-1 is vz[fs] after the mirror,
+    so its adjoint source lands in row fs.  Against the float64 oracle; with
+    nabc = 16 the surface falls on a 16-row tile edge."""
+    from test_forward_gpu import synthetic_case
+    c = dict(synthetic_case(50, 200, nabc, 150, 2, seed=9), free_surface=True)
+    rx = np.arange(0, 200, 7)
+    c["rcv_x"] = np.concatenate([rx, rx, rx])
+    c["rcv_z"] = np.concatenate([np.full(rx.size, -1), np.zeros(rx.size, np.int64), np.ones(rx.size, np.int64)])
+    c["src_z"], c["src_x"] = np.array([2, 5]), np.array([40, 150])
+    rng = np.random.default_rng(10)
+    lin = {k: rng.standard_normal((2, 150, c["rcv_x"].size)) for k in ("p", "vx", "vz")}
+    gvp, grho, _ = cuda_grad(c, cuda_device, fd_order=8, lin=lin)
+    rvp, rrho, _ = orc.gradient(**oracle_kwargs(c), res_p=lin["p"], res_vx=lin["vx"], res_vz=lin["vz"], half=4,
+                                dtype=np.float64)
+    assert orc.rel_l2(gvp, rvp) < GTOL
+    assert orc.rel_l2(grho, rrho) < GTOL
