@@ -1036,7 +1036,7 @@ int backward_cpml(gb_plan *P, const float *vp, const float *rho, const float *da
     A.free_surface = fs;
     const bool inject = d.n_rcv > 0 && (res_p || res_vx || res_vz);
     const size_t step_img = (size_t)(rho_fields ? 3 : 1) * S * P->plane;
-    const dim3 block(32, 4), grid((P->Nx + 127) / 128, (P->Nz + 3) / 4);
+    const dim3 block(32, 4), grid((P->Nx + 127) / 128, (P->Nz + 4 * kCpLZ - 1) / (4 * kCpLZ), P->n_groups);
     const int fold_blocks = (int)std::min<long long>(1024, ((long long)S * P->Nx + 255) / 256);
     P->mark(2, true, st);
     P->phase_steps[2] += d.nt;

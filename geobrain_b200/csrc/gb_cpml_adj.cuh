@@ -153,7 +153,7 @@ struct CpmlAdjArgs4 {
     const float *img;           // this step's I [S][plane], then Jx, Jz at img_field_stride
     long long img_field_stride;
     int img_fmt;
-    float *G1, *C1, *G2, *C2;   // one [plane] each (group 0 of the gradient planes)
+    float *G1, *C1, *G2, *C2;   // [n_groups][plane] each: shot group g adds into plane g
     int free_surface;
 };
 
@@ -172,169 +172,210 @@ __device__ __forceinline__ float4 fms4(const float4 &a, const float4 &x, const f
     return make_float4(a.x * x.x - b.x * y.x, a.y * x.y - b.y * y.y, a.z * x.z - b.z * y.z, a.w * x.w - b.w * y.w);
 }
 
-// block (32, 4): 4 adjacent cells of one row per thread, looping over the
-// shots, so each cell of the gradient planes has one owner.  Reads lam_vx,
-// lam_vz and the psi_v slot psi_in (at neighbours), writes lam_p in place
-// and the psi_v slot psi_out.
+// Rows per thread of the two adjoint kernels: a thread updates 4 adjacent
+// cells of kCpLZ consecutive rows and keeps the z-direction operand of its
+// rows and their 2R - 1 neighbours in a register window, so a row of the
+// memory variable and its field is read once per kCpLZ output rows (2R
+// times per row with one row per thread).  Two rows: at four the window and
+// the per-row gradient sums spilled (280-476 bytes at 8th order).
+constexpr int kCpLZ = 2;
+
+// block (32, 4), grid (x, z, shot group): a thread owns 4 x kCpLZ cells and
+// loops over the shots of its group, so each cell of the group's gradient
+// planes has one owner.  Reads lam_vx, lam_vz and the psi_v slot psi_in (at
+// neighbours), writes lam_p in place and the psi_v slot psi_out.
 template <int R>
 __global__ void __launch_bounds__(128, 4) cpml_adj_v_kernel(const CpmlAdjArgs4 A)
 {
+    constexpr int LZ = kCpLZ, NWZ = LZ + 2 * R - 1;
     const StepGeom &g = A.g;
     const int x0 = 4 * (blockIdx.x * 32 + threadIdx.x);
-    const int z = blockIdx.y * 4 + threadIdx.y;
-    if (x0 >= g.Nx || z >= g.Nz) return;
-    const long long P = g.plane, o = (long long)z * g.pitch + x0;
+    const int z0 = (blockIdx.y * 4 + threadIdx.y) * LZ;
+    if (x0 >= g.Nx || z0 >= g.Nz) return;
+    const int grp = blockIdx.z, s0 = grp * g.shots_per_cta, s1 = min(g.n_shots, s0 + g.shots_per_cta);
+    const long long P = g.plane;
     const float *WX = A.cp, *AX = A.cp + P, *BX = A.cp + 2 * P, *WZ = A.cp + 3 * P, *AZ = A.cp + 4 * P,
                 *BZ = A.cp + 5 * P;
     const bool lok = x0 >= 4, rok = x0 + 4 < g.pitch;
-    // the x taps' coefficients, the same for every shot
-    const float4 wxl = cp_ld4(WX, o - 4, lok), wxc = cp_ld4(WX, o, true), wxr = cp_ld4(WX, o + 4, rok);
-    const float4 axl = cp_ld4(AX, o - 4, lok), axc = cp_ld4(AX, o, true), axr = cp_ld4(AX, o + 4, rok);
-    const float4 bxc = cp_ld4(BX, o, true), wzc = cp_ld4(WZ, o, true), bzc = cp_ld4(BZ, o, true);
-    const float4 a2 = cp_ld4(A.a2, o, true);
-    bool mp[4], mvx[4], mvz[4];
+    float g2[LZ][4], c2[LZ][4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int x = x0 + q;
-        mp[q] = x < g.Nx && (cp_in_p(g, z, x) || (A.free_surface && z == g.fs - 1));   // mirror row: folded next
-        mvx[q] = x < g.Nx && cp_in_vx(g, z, x);
-        mvz[q] = x < g.Nx && cp_in_vz(g, z, x);
-    }
-    float g2[4] = {0.f, 0.f, 0.f, 0.f}, c2[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int s = 0; s < g.n_shots; ++s) {
+    for (int u = 0; u < LZ; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) g2[u][q] = c2[u][q] = 0.f;
+    for (int s = s0; s < s1; ++s) {
         float *L = A.lam + (long long)s * kCpmlPlanes * P;
         const float *Lvx = L + kLamVX * P, *Lvz = L + kLamVZ * P;
         const float *Lsvx = L + A.psi_in * P, *Lsvz = L + (A.psi_in + 1) * P;
-        if (s + 1 < g.n_shots) cp_prefetch(L + kCpmlPlanes * P, P, o, A.psi_in, A.psi_in + 1);
-        // wx = AX lam_psi_vx - WX lam_vx at x0-4 .. x0+7
-        float wx[12];
-        {
-            const float4 l = fms4(axl, cp_ld4(Lsvx, o - 4, lok), wxl, cp_ld4(Lvx, o - 4, lok));
-            const float4 c = fms4(axc, cp_ld4(Lsvx, o, true), wxc, cp_ld4(Lvx, o, true));
-            const float4 r = fms4(axr, cp_ld4(Lsvx, o + 4, rok), wxr, cp_ld4(Lvx, o + 4, rok));
-            const float t[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
+        if (s + 1 < s1)
 #pragma unroll
-            for (int i = 0; i < 12; ++i) wx[i] = t[i];
+            for (int u = 0; u < LZ; ++u)
+                if (z0 + u < g.Nz)
+                    cp_prefetch(L + kCpmlPlanes * P, P, (long long)(z0 + u) * g.pitch + x0, A.psi_in, A.psi_in + 1);
+        // wz = AZ lam_psi_vz - WZ lam_vz on rows z0-R .. z0+LZ+R-2
+        float4 wz[NWZ];
+#pragma unroll
+        for (int t = 0; t < NWZ; ++t) {
+            const int zr = z0 - R + t;
+            const long long q = (long long)zr * g.pitch + x0;
+            wz[t] = (zr >= 0 && zr < g.Nz)
+                        ? fms4(cp_ld4(AZ, q, true), cp_ld4(Lsvz, q, true), cp_ld4(WZ, q, true), cp_ld4(Lvz, q, true))
+                        : zero4();
         }
-        // wz = AZ lam_psi_vz - WZ lam_vz on rows z-R .. z+R-1
-        float4 wz[2 * R];
 #pragma unroll
-        for (int t = 0; t < 2 * R; ++t) {
-            const int zr = z - R + t;
-            const bool ok = zr >= 0 && zr < g.Nz;
-            const long long q = o + (long long)(t - R) * g.pitch;
-            wz[t] = ok ? fms4(cp_ld4(AZ, q, true), cp_ld4(Lsvz, q, true), cp_ld4(WZ, q, true), cp_ld4(Lvz, q, true))
-                       : zero4();
-        }
-        const float4 lp = cp_ldw4(L, o), lvx = cp_ld4(Lvx, o, true), lvz = cp_ld4(Lvz, o, true);
-        const float4 lsvx = cp_ld4(Lsvx, o, true), lsvz = cp_ld4(Lsvz, o, true);
-        float4 op, mvxv, mvzv;
+        for (int u = 0; u < LZ; ++u) {
+            const int z = z0 + u;
+            if (z >= g.Nz) break;
+            const long long o = (long long)z * g.pitch + x0;
+            // wx = AX lam_psi_vx - WX lam_vx at x0-4 .. x0+7
+            float wx[12];
+            {
+                const float4 l = fms4(cp_ld4(AX, o - 4, lok), cp_ld4(Lsvx, o - 4, lok), cp_ld4(WX, o - 4, lok),
+                                      cp_ld4(Lvx, o - 4, lok));
+                const float4 c = fms4(cp_ld4(AX, o, true), cp_ld4(Lsvx, o, true), cp_ld4(WX, o, true),
+                                      cp_ld4(Lvx, o, true));
+                const float4 r = fms4(cp_ld4(AX, o + 4, rok), cp_ld4(Lsvx, o + 4, rok), cp_ld4(WX, o + 4, rok),
+                                      cp_ld4(Lvx, o + 4, rok));
+                const float t[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            float t = 0.f;
+                for (int i = 0; i < 12; ++i) wx[i] = t[i];
+            }
+            const float4 lp = cp_ldw4(L, o), lvx = cp_ld4(Lvx, o, true), lvz = cp_ld4(Lvz, o, true);
+            const float4 lsvx = cp_ld4(Lsvx, o, true), lsvz = cp_ld4(Lsvz, o, true);
+            float4 op, mvxv, mvzv;
 #pragma unroll
-            for (int k = 0; k < R; ++k)
-                t += g.c[k] * ((wx[q + 3 - k] - wx[q + 4 + k]) + (at(wz[R - 1 - k], q) - at(wz[R + k], q)));
-            at(op, q) = mp[q] ? at(lp, q) + t : 0.f;
-            at(mvxv, q) = mvx[q] ? at(lvx, q) : 0.f;
-            at(mvzv, q) = mvz[q] ? at(lvz, q) : 0.f;
-        }
-        stg4(L + o, op);
-        stg4(L + A.psi_out * P + o, fms4(bxc, lsvx, wxc, lvx));
-        stg4(L + (A.psi_out + 1) * P + o, fms4(bzc, lsvz, wzc, lvz));
-        if (A.G2) {
-            const long long io = (long long)s * P + o;
-            const float4 jx = decode_img4(load_img_raw(A.img, A.img_field_stride + io, A.img_fmt), A.img_fmt);
-            const float4 jz = decode_img4(load_img_raw(A.img, 2 * A.img_field_stride + io, A.img_fmt), A.img_fmt);
+            for (int q = 0; q < 4; ++q) {
+                const int x = x0 + q;
+                const bool mp = x < g.Nx && (cp_in_p(g, z, x) || (A.free_surface && z == g.fs - 1));   // mirror row: folded next
+                float t = 0.f;
 #pragma unroll
-            for (int q = 0; q < 4; ++q)
-                neumaier_add(g2[q], c2[q], at(a2, q) * (at(mvxv, q) * at(jx, q) + at(mvzv, q) * at(jz, q)));
+                for (int k = 0; k < R; ++k)
+                    t += g.c[k] *
+                         ((wx[q + 3 - k] - wx[q + 4 + k]) + (at(wz[u + R - 1 - k], q) - at(wz[u + R + k], q)));
+                at(op, q) = mp ? at(lp, q) + t : 0.f;
+                at(mvxv, q) = (x < g.Nx && cp_in_vx(g, z, x)) ? at(lvx, q) : 0.f;
+                at(mvzv, q) = (x < g.Nx && cp_in_vz(g, z, x)) ? at(lvz, q) : 0.f;
+            }
+            stg4(L + o, op);
+            stg4(L + A.psi_out * P + o, fms4(cp_ld4(BX, o, true), lsvx, cp_ld4(WX, o, true), lvx));
+            stg4(L + (A.psi_out + 1) * P + o, fms4(cp_ld4(BZ, o, true), lsvz, cp_ld4(WZ, o, true), lvz));
+            if (A.G2) {
+                const float4 a2 = cp_ld4(A.a2, o, true);
+                const long long io = (long long)s * P + o;
+                const float4 jx = decode_img4(load_img_raw(A.img, A.img_field_stride + io, A.img_fmt), A.img_fmt);
+                const float4 jz =
+                    decode_img4(load_img_raw(A.img, 2 * A.img_field_stride + io, A.img_fmt), A.img_fmt);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    neumaier_add(g2[u][q], c2[u][q], at(a2, q) * (at(mvxv, q) * at(jx, q) + at(mvzv, q) * at(jz, q)));
+            }
         }
     }
     if (A.G2) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (x0 + q < g.Nx) neumaier_add(A.G2[o + q], A.C2[o + q], g2[q] + c2[q]);
+        for (int u = 0; u < LZ; ++u) {
+            const long long o = (long long)(z0 + u) * g.pitch + x0 + (long long)grp * P;
+            if (z0 + u < g.Nz)
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (x0 + q < g.Nx) neumaier_add(A.G2[o + q], A.C2[o + q], g2[u][q] + c2[u][q]);
+        }
     }
 }
 
 // Reads lam_p and the psi_p slot psi_in (at neighbours), writes lam_vx and
-// lam_vz in place and the psi_p slot psi_out.
+// lam_vz in place and the psi_p slot psi_out (the layout of
+// cpml_adj_v_kernel: 4 x kCpLZ cells per thread, shot groups in grid z).
 template <int R>
 __global__ void __launch_bounds__(128, 4) cpml_adj_p_kernel(const CpmlAdjArgs4 A)
 {
+    constexpr int LZ = kCpLZ, NWZ = LZ + 2 * R - 1;
     const StepGeom &g = A.g;
     const int x0 = 4 * (blockIdx.x * 32 + threadIdx.x);
-    const int z = blockIdx.y * 4 + threadIdx.y;
-    if (x0 >= g.Nx || z >= g.Nz) return;
-    const long long P = g.plane, o = (long long)z * g.pitch + x0;
+    const int z0 = (blockIdx.y * 4 + threadIdx.y) * LZ;
+    if (x0 >= g.Nx || z0 >= g.Nz) return;
+    const int grp = blockIdx.z, s0 = grp * g.shots_per_cta, s1 = min(g.n_shots, s0 + g.shots_per_cta);
+    const long long P = g.plane;
     const float *UX = A.cp + 6 * P, *PX = A.cp + 7 * P, *QX = A.cp + 8 * P, *UZ = A.cp + 9 * P,
                 *PZ = A.cp + 10 * P, *QZ = A.cp + 11 * P;
     const bool lok = x0 >= 4, rok = x0 + 4 < g.pitch;
-    const float4 uxl = cp_ld4(UX, o - 4, lok), uxc = cp_ld4(UX, o, true), uxr = cp_ld4(UX, o + 4, rok);
-    const float4 pxl = cp_ld4(PX, o - 4, lok), pxc = cp_ld4(PX, o, true), pxr = cp_ld4(PX, o + 4, rok);
-    const float4 qxc = cp_ld4(QX, o, true), uzc = cp_ld4(UZ, o, true), qzc = cp_ld4(QZ, o, true);
-    const float4 a1 = cp_ld4(A.a1, o, true);
-    bool mp[4], mvx[4], mvz[4];
+    float g1[LZ][4], c1[LZ][4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int x = x0 + q;
-        mp[q] = x < g.Nx && cp_in_p(g, z, x);
-        mvx[q] = x < g.Nx && cp_in_vx(g, z, x);
-        // the p update read vz[fs-1], which the previous step's mirror set (folded next step)
-        mvz[q] = x < g.Nx && (cp_in_vz(g, z, x) || (A.free_surface && z == g.fs - 1));
-    }
-    float g1[4] = {0.f, 0.f, 0.f, 0.f}, c1[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int s = 0; s < g.n_shots; ++s) {
+    for (int u = 0; u < LZ; ++u)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) g1[u][q] = c1[u][q] = 0.f;
+    for (int s = s0; s < s1; ++s) {
         float *L = A.lam + (long long)s * kCpmlPlanes * P;
         const float *Lspx = L + A.psi_in * P, *Lspz = L + (A.psi_in + 1) * P;
-        if (s + 1 < g.n_shots) cp_prefetch(L + kCpmlPlanes * P, P, o, A.psi_in, A.psi_in + 1);
-        // ux = PX lam_psi_px - UX lam_p at x0-4 .. x0+7
-        float ux[12];
-        {
-            const float4 l = fms4(pxl, cp_ld4(Lspx, o - 4, lok), uxl, cp_ld4(L, o - 4, lok));
-            const float4 c = fms4(pxc, cp_ld4(Lspx, o, true), uxc, cp_ld4(L, o, true));
-            const float4 r = fms4(pxr, cp_ld4(Lspx, o + 4, rok), uxr, cp_ld4(L, o + 4, rok));
-            const float t[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
+        if (s + 1 < s1)
 #pragma unroll
-            for (int i = 0; i < 12; ++i) ux[i] = t[i];
+            for (int u = 0; u < LZ; ++u)
+                if (z0 + u < g.Nz)
+                    cp_prefetch(L + kCpmlPlanes * P, P, (long long)(z0 + u) * g.pitch + x0, A.psi_in, A.psi_in + 1);
+        // uz = PZ lam_psi_pz - UZ lam_p on rows z0-R+1 .. z0+LZ+R-1
+        float4 uz[NWZ];
+#pragma unroll
+        for (int t = 0; t < NWZ; ++t) {
+            const int zr = z0 - R + 1 + t;
+            const long long q = (long long)zr * g.pitch + x0;
+            uz[t] = (zr >= 0 && zr < g.Nz)
+                        ? fms4(cp_ld4(PZ, q, true), cp_ld4(Lspz, q, true), cp_ld4(UZ, q, true), cp_ld4(L, q, true))
+                        : zero4();
         }
-        // uz = PZ lam_psi_pz - UZ lam_p on rows z-R+1 .. z+R
-        float4 uz[2 * R];
 #pragma unroll
-        for (int t = 0; t < 2 * R; ++t) {
-            const int zr = z - R + 1 + t;
-            const bool ok = zr >= 0 && zr < g.Nz;
-            const long long q = o + (long long)(t - R + 1) * g.pitch;
-            uz[t] = ok ? fms4(cp_ld4(PZ, q, true), cp_ld4(Lspz, q, true), cp_ld4(UZ, q, true), cp_ld4(L, q, true))
-                       : zero4();
-        }
-        const float4 lp = cp_ld4(L, o, true), lvx = cp_ldw4(L + kLamVX * P, o), lvz = cp_ldw4(L + kLamVZ * P, o);
-        const float4 lspx = cp_ld4(Lspx, o, true), lspz = cp_ld4(Lspz, o, true);
-        float4 ovx, ovz;
+        for (int u = 0; u < LZ; ++u) {
+            const int z = z0 + u;
+            if (z >= g.Nz) break;
+            const long long o = (long long)z * g.pitch + x0;
+            // ux = PX lam_psi_px - UX lam_p at x0-4 .. x0+7
+            float ux[12];
+            {
+                const float4 l = fms4(cp_ld4(PX, o - 4, lok), cp_ld4(Lspx, o - 4, lok), cp_ld4(UX, o - 4, lok),
+                                      cp_ld4(L, o - 4, lok));
+                const float4 c = fms4(cp_ld4(PX, o, true), cp_ld4(Lspx, o, true), cp_ld4(UX, o, true),
+                                      cp_ld4(L, o, true));
+                const float4 r = fms4(cp_ld4(PX, o + 4, rok), cp_ld4(Lspx, o + 4, rok), cp_ld4(UX, o + 4, rok),
+                                      cp_ld4(L, o + 4, rok));
+                const float t[12] = {l.x, l.y, l.z, l.w, c.x, c.y, c.z, c.w, r.x, r.y, r.z, r.w};
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            float tx = 0.f, tz = 0.f;
-#pragma unroll
-            for (int k = 0; k < R; ++k) {
-                tx += g.c[k] * (ux[q + 4 - k] - ux[q + 5 + k]);
-                tz += g.c[k] * (at(uz[R - 1 - k], q) - at(uz[R + k], q));
+                for (int i = 0; i < 12; ++i) ux[i] = t[i];
             }
-            at(ovx, q) = mvx[q] ? at(lvx, q) + tx : 0.f;
-            at(ovz, q) = mvz[q] ? at(lvz, q) + tz : 0.f;
-        }
-        stg4(L + kLamVX * P + o, ovx);
-        stg4(L + kLamVZ * P + o, ovz);
-        stg4(L + A.psi_out * P + o, fms4(qxc, lspx, uxc, lp));
-        stg4(L + (A.psi_out + 1) * P + o, fms4(qzc, lspz, uzc, lp));
-        const float4 im = decode_img4(load_img_raw(A.img, (long long)s * P + o, A.img_fmt), A.img_fmt);
+            const float4 lp = cp_ld4(L, o, true), lvx = cp_ldw4(L + kLamVX * P, o), lvz = cp_ldw4(L + kLamVZ * P, o);
+            const float4 lspx = cp_ld4(Lspx, o, true), lspz = cp_ld4(Lspz, o, true);
+            float4 ovx, ovz;
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (mp[q]) neumaier_add(g1[q], c1[q], at(a1, q) * at(lp, q) * at(im, q));
+            for (int q = 0; q < 4; ++q) {
+                const int x = x0 + q;
+                float tx = 0.f, tz = 0.f;
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    tx += g.c[k] * (ux[q + 4 - k] - ux[q + 5 + k]);
+                    tz += g.c[k] * (at(uz[u + R - 1 - k], q) - at(uz[u + R + k], q));
+                }
+                // the p update read vz[fs-1], which the previous step's mirror set (folded next step)
+                const bool mvz = x < g.Nx && (cp_in_vz(g, z, x) || (A.free_surface && z == g.fs - 1));
+                at(ovx, q) = (x < g.Nx && cp_in_vx(g, z, x)) ? at(lvx, q) + tx : 0.f;
+                at(ovz, q) = mvz ? at(lvz, q) + tz : 0.f;
+            }
+            stg4(L + kLamVX * P + o, ovx);
+            stg4(L + kLamVZ * P + o, ovz);
+            stg4(L + A.psi_out * P + o, fms4(cp_ld4(QX, o, true), lspx, cp_ld4(UX, o, true), lp));
+            stg4(L + (A.psi_out + 1) * P + o, fms4(cp_ld4(QZ, o, true), lspz, cp_ld4(UZ, o, true), lp));
+            const float4 a1 = cp_ld4(A.a1, o, true);
+            const float4 im = decode_img4(load_img_raw(A.img, (long long)s * P + o, A.img_fmt), A.img_fmt);
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (x0 + q < g.Nx && cp_in_p(g, z, x0 + q))
+                    neumaier_add(g1[u][q], c1[u][q], at(a1, q) * at(lp, q) * at(im, q));
+        }
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q)
-        if (x0 + q < g.Nx) neumaier_add(A.G1[o + q], A.C1[o + q], g1[q] + c1[q]);
+    for (int u = 0; u < LZ; ++u) {
+        const long long o = (long long)(z0 + u) * g.pitch + x0 + (long long)grp * P;
+        if (z0 + u < g.Nz)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (x0 + q < g.Nx) neumaier_add(A.G1[o + q], A.C1[o + q], g1[u][q] + c1[u][q]);
+    }
 }
 
 }  // namespace gb
