@@ -280,12 +280,15 @@ struct gb_plan {
     }
     int spc_eff = 1;
 
-    // Resident forward (gb_resident.cuh): -1 automatic, 0 off, 1 on with the
-    // exchange through global memory and flags, 2 on with the exchange
-    // through distributed shared memory in one cluster per shot; the tile
-    // rows asked for (0 = automatic) and in use (0 = the tile kernel runs)
+    // Resident forward (gb_resident.cuh, gb_resident_sx.cuh): -1 automatic,
+    // 0 off, 1 on with the exchange through global memory after the p and
+    // the v updates, 2 on with the exchange through distributed shared
+    // memory in one cluster per shot, 3 on with one exchange a step through
+    // global memory (4th order, no free surface); the tile rows asked for
+    // (0 = automatic) and in use (0 = the tile kernel runs)
     int res_mode = -1, res_tz_req = 0, res_tz = 0;
-    bool res_cluster = false;                                          // the exchange in use
+    bool res_cluster = false, res_single = false;                      // the exchange in use
+    int res_exchange() const { return res_cluster ? 1 : res_single ? 2 : 0; }
     static constexpr int kMaxClusterTiles = 16;                        // CTAs of one (non-portable) cluster
     int res_tiles_x = 0, res_tiles_z = 0, res_n = 0, res_shots = 0;   // tiling; shots per cooperative launch
     std::vector<int> res_ptr;                                          // CSR over resident tiles
@@ -304,21 +307,26 @@ struct gb_plan {
     // Choose the resident tiling.  Automatic mode runs it when every shot's
     // tiles fit on the SMs at once (few shots or a small grid: the cases
     // where the per-step tile kernel is launch- and latency-bound), with the
-    // exchange through global memory and the smallest tile height that fits
-    // (the most CTAs); the cluster exchange, limited to 16 CTAs a shot,
-    // measured no faster, and runs when asked for.  More shots keep the tile
+    // two exchanges through global memory and the smallest tile height that
+    // fits (the most CTAs).  The cluster exchange (16 CTAs a shot at most)
+    // and one exchange a step (which sends twice the cells to eight
+    // neighbours and updates p on twice the rows) measured no faster on the
+    // 100 x 200 grid; they run when asked for.  More shots keep the tile
     // kernel.
+    bool res_single_ok() const { return R == 2 && !d.free_surface; }
     void res_choose()
     {
         res_tz = 0;
-        res_cluster = false;
+        res_cluster = res_single = false;
         if (res_mode == 0 || cpml) return;
         const int sms = sm_count();
         int best = 0;
-        for (int pass = 0; pass < 2 && !best; ++pass) {
-            const bool cl = pass == 1;
-            if (cl && res_mode < 0) continue;
-            if ((cl && res_mode == 1) || (!cl && res_mode == 2)) continue;
+        // passes: one exchange a step, two through global memory, cluster
+        for (int pass = 0; pass < 3 && !best; ++pass) {
+            const bool sx = pass == 0, cl = pass == 2;
+            if (sx && !(res_single_ok() && res_mode == 3)) continue;
+            if (pass == 1 && !(res_mode < 0 || res_mode == 1)) continue;
+            if (cl && res_mode != 2) continue;
             for (int tz : kResidentRows) {
                 if (res_tz_req && tz != res_tz_req) continue;
                 if (!res_fits(tz, sms)) continue;
@@ -327,6 +335,7 @@ struct gb_plan {
                 if (res_mode < 0 && n * d.n_shots > sms) continue;
                 best = tz;
                 res_cluster = cl;
+                res_single = sx;
                 break;
             }
         }
@@ -430,10 +439,10 @@ Layout layout(const gb_plan *p, int with_gradient = 0, int checkpoint_every = 0,
         L.psi = o; o = align256(o + 2 * S * 4 * p->plane * 4);   // two levels of the memory variables
     }
     if (p->res_tz > 0 && with_gradient == 0) {
-        const ResidentKernel k = resident_kernel(p->R, p->res_tz, false);
+        const ResidentKernel k = resident_kernel(p->R, p->res_tz, p->res_single ? 2 : 0);
         L.res_ptr = o; o = align256(o + (p->res_n + 1) * 4);
         L.res_ent = o; o = align256(o + std::max<size_t>(p->d.n_rcv, 1) * 16);
-        L.res_x = o; o = align256(o + S * p->res_n * kResParts * k.part_words * 8);
+        L.res_x = o; o = align256(o + S * p->res_n * k.tile_words * 8);
     }
     L.n_img = with_gradient >= 2 ? 3 : 1;
     if (with_gradient > 0) {
@@ -908,7 +917,7 @@ int forward_resident(gb_plan *P, const Layout &L, char *ws, const Setup &Su, flo
 {
     const gb_model_desc &d = P->d;
     const int S = d.n_shots;
-    const ResidentKernel K = resident_kernel(P->R, P->res_tz, P->res_cluster);
+    const ResidentKernel K = resident_kernel(P->R, P->res_tz, P->res_exchange());
     if (!K.fn) return fail(GB_E_UNSUPPORTED, "no resident kernel for this tile height");
     GB_CUDA(cudaFuncSetAttribute(K.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K.smem));
     if (P->res_cluster && P->res_n > 8) GB_CUDA(cudaFuncSetAttribute(K.fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
@@ -918,7 +927,7 @@ int forward_resident(gb_plan *P, const Layout &L, char *ws, const Setup &Su, flo
     if (d.n_rcv) GB_CUDA(cudaMemcpyAsync(d_ent, P->res_ent.data(), d.n_rcv * 16, cudaMemcpyHostToDevice, st));
     // the strips' tags start at 0, which no step's tag is
     if (!P->res_cluster)
-        GB_CUDA(cudaMemsetAsync(ws + L.res_x, 0, (size_t)S * P->res_n * kResParts * K.part_words * 8, st));
+        GB_CUDA(cudaMemsetAsync(ws + L.res_x, 0, (size_t)S * P->res_n * K.tile_words * 8, st));
     ResArgs A{};
     A.g = P->geom();
     A.tiles_x = P->res_tiles_x;
@@ -1170,8 +1179,9 @@ int gb_plan_set_tiling(gb_plan *p, int tile_rows, int shots_per_cta)
 int gb_plan_set_resident(gb_plan *p, int mode, int tile_rows)
 {
     if (!p) return fail(GB_E_ARG, "null plan");
-    if (mode < -1 || mode > 2)
-        return fail(GB_E_ARG, "mode must be -1 (automatic), 0 (off), 1 (global exchange) or 2 (cluster exchange)");
+    if (mode < -1 || mode > 3)
+        return fail(GB_E_ARG, "mode must be -1 (automatic), 0 (off), 1 (global exchange), 2 (cluster exchange) "
+                              "or 3 (one global exchange a step)");
     bool known = tile_rows == 0;
     for (int tz : kResidentRows) known |= tz == tile_rows;
     if (!known) return fail(GB_E_ARG, "tile_rows must be 0, 4, 8, 12, 16, 24, 32, 36 or 40");
@@ -1182,8 +1192,11 @@ int gb_plan_set_resident(gb_plan *p, int mode, int tile_rows)
         p->res_mode = -1;
         p->res_tz_req = 0;
         p->res_choose();
-        return fail(GB_E_UNSUPPORTED, p->cpml ? "the resident forward does not run CPML plans"
-                                              : "no resident tiling of that height fits this grid on this device");
+        return fail(GB_E_UNSUPPORTED,
+                    p->cpml ? "the resident forward does not run CPML plans"
+                    : mode == 3 && !p->res_single_ok()
+                        ? "one exchange a step needs the 4th-order scheme without a free surface"
+                        : "no resident tiling of that height fits this grid on this device");
     }
     return GB_OK;
 }
@@ -1193,7 +1206,7 @@ int gb_plan_get_resident(const gb_plan *p, int *tile_rows, int *shots_per_launch
     if (!p) return fail(GB_E_ARG, "null plan");
     if (tile_rows) *tile_rows = p->res_tz;
     if (shots_per_launch) *shots_per_launch = p->res_tz ? p->res_shots : 0;
-    if (cluster) *cluster = p->res_tz && p->res_cluster ? 1 : 0;
+    if (cluster) *cluster = p->res_tz ? p->res_exchange() : 0;
     return GB_OK;
 }
 
@@ -1542,11 +1555,13 @@ size_t gb_plan_autotune_workspace_bytes(gb_plan *p)
         p->retile();
         m = std::max(m, gb_plan_workspace_bytes(p, 0, 0));
     }
-    p->res_mode = 1;
-    for (int t : kResidentRows) {
-        p->res_tz_req = t;
-        p->res_choose();
-        m = std::max(m, gb_plan_workspace_bytes(p, 0, 0));
+    for (int mode : {1, 3}) {
+        p->res_mode = mode;
+        for (int t : kResidentRows) {
+            p->res_tz_req = t;
+            p->res_choose();
+            m = std::max(m, gb_plan_workspace_bytes(p, 0, 0));
+        }
     }
     p->tz = tz;
     p->res_mode = rm;
@@ -1567,10 +1582,11 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         bool streams;
         int graph;
         bool stream;
-        int res;    // resident forward tile rows (negative: the cluster exchange), 0 = the tile kernel
+        int res;    // resident forward tile rows, 0 = the tile kernel
+        int xm;     // its gb_plan_set_resident mode (1 global, 2 cluster, 3 one exchange a step)
     };
-    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps, P->stream,
-                       P->res_cluster ? -P->res_tz : P->res_tz};
+    const Config saved{P->tz, P->spc, P->group_streams, P->graph_steps, P->stream, P->res_tz,
+                       P->res_exchange() == 1 ? 2 : P->res_exchange() == 2 ? 3 : 1};
     const int saved_res_mode = P->res_mode, saved_res_req = P->res_tz_req;
     const bool prof = P->prof;
     const int nt = P->d.nt;
@@ -1587,16 +1603,17 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
                 for (int streams = 1; streams >= 0; --streams)
                     for (int graph : {0, C}) {
                         if (graph > n) continue;
-                        cands.push_back({tz, spc, streams != 0, graph, stream != 0, 0});
+                        cands.push_back({tz, spc, streams != 0, graph, stream != 0, 0, 0});
                     }
             }
         }
     if (!P->cpml)
         for (int tz : kResidentRows)
             if (P->res_fits(tz, gb_plan::sm_count())) {
-                cands.push_back({saved.tz, saved.spc, true, 0, false, tz});
+                cands.push_back({saved.tz, saved.spc, true, 0, false, tz, 1});
+                if (P->res_single_ok()) cands.push_back({saved.tz, saved.spc, true, 0, false, tz, 3});
                 const long long n = (long long)((P->Nx + TX - 1) / TX) * ((P->Nz + tz - 1) / tz);
-                if (n <= gb_plan::kMaxClusterTiles) cands.push_back({saved.tz, saved.spc, true, 0, false, -tz});
+                if (n <= gb_plan::kMaxClusterTiles) cands.push_back({saved.tz, saved.spc, true, 0, false, tz, 2});
             }
     cudaEvent_t e0, e1;
     GB_CUDA(cudaEventCreate(&e0));
@@ -1613,11 +1630,11 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         P->group_streams = k.streams;
         P->graph_steps = k.graph;
         P->stream = k.stream;
-        P->res_mode = k.res > 0 ? 1 : k.res < 0 ? 2 : 0;
-        P->res_tz_req = std::abs(k.res);
+        P->res_mode = k.res ? k.xm : 0;
+        P->res_tz_req = k.res;
         P->res_choose();
         P->release_graph();
-        if (k.res && P->res_tz != std::abs(k.res)) continue;
+        if (k.res && P->res_tz != k.res) continue;
         if (gb_plan_workspace_bytes(P, 0, 0) > workspace_bytes) continue;
         if (!k.res && k.streams && P->n_groups == 1) continue;      // same as without
         float ms = -1.f;
@@ -1653,8 +1670,8 @@ int gb_plan_autotune(gb_plan *P, const float *vp, const float *rho, const float 
         P->res_mode = saved_res_mode;
         P->res_tz_req = saved_res_req;
     } else {
-        P->res_mode = win.res > 0 ? 1 : win.res < 0 ? 2 : 0;
-        P->res_tz_req = std::abs(win.res);
+        P->res_mode = win.res ? win.xm : 0;
+        P->res_tz_req = win.res;
     }
     P->res_choose();
     P->release_graph();                // captured with the shortened step count

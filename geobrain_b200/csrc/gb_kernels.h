@@ -42,11 +42,14 @@ struct ResidentKernel {
     void *fn = nullptr;
     size_t smem = 0;
     int threads = 0;
-    size_t part_words = 0;      // 8-byte (value, tag) words per exchange strip
+    size_t tile_words = 0;      // 8-byte (value, tag) exchange words per tile
 };
-// cluster: the variant that exchanges through distributed shared memory
-// within one thread-block cluster per shot (tiles of a shot <= 16).
-ResidentKernel resident_kernel(int R, int tz, bool cluster);
+// exchange: 0 through global memory after the p and the v updates; 1 through
+// distributed shared memory within one thread-block cluster per shot (tiles
+// of a shot <= 16); 2 through global memory once per step, p also updated on
+// the neighbours' edge rows and columns (gb_resident_sx.cuh: 4th order, no
+// free surface).
+ResidentKernel resident_kernel(int R, int tz, int exchange);
 
 }  // namespace host
 }  // namespace gb

@@ -3,9 +3,11 @@
 // (measured against one boundary item per thread and two interior rows per
 // warp, which ran 7 % slower on the 400 x 1200 grid and 26 % on 100 x 200
 // with 8-row tiles); each with the exchange through global memory ((value,
-// tag) words), and through distributed shared memory within a cluster.
+// tag) words), and through distributed shared memory within a cluster; and
+// the one-exchange-a-step kernels (gb_resident_sx.cuh, 4th order).
 #include "gb_kernels.h"
 #include "gb_resident.cuh"
+#include "gb_resident_sx.cuh"
 
 #include <cuda_runtime.h>
 
@@ -21,7 +23,7 @@ ResidentKernel make()
     k.fn = (void *)&resident_fwd_kernel<R, NW, TZ, CL>;
     k.smem = G::SMEM;
     k.threads = G::NTH;
-    k.part_words = G::PART;
+    k.tile_words = (size_t)kResParts * G::PART;
     return k;
 }
 
@@ -41,10 +43,40 @@ ResidentKernel pick(int tz)
     }
 }
 
+template <int NW, int TZ>
+ResidentKernel make_sx()
+{
+    using G = SxGeo<NW, TZ>;
+    ResidentKernel k;
+    k.fn = (void *)&resident_sx_kernel<NW, TZ>;
+    k.smem = G::SMEM;
+    k.threads = G::NTH;
+    k.tile_words = 2 * (size_t)G::SLOT;
+    return k;
+}
+
+// one exchange a step: 8 warps up to 16-row tiles, 16 above
+ResidentKernel pick_sx(int tz)
+{
+    switch (tz) {
+    case 4: return make_sx<8, 4>();
+    case 8: return make_sx<8, 8>();
+    case 12: return make_sx<8, 12>();
+    case 16: return make_sx<8, 16>();
+    case 24: return make_sx<16, 24>();
+    case 32: return make_sx<16, 32>();
+    case 36: return make_sx<16, 36>();
+    case 40: return make_sx<16, 40>();
+    default: return ResidentKernel{};
+    }
+}
+
 }  // namespace
 
-ResidentKernel resident_kernel(int R, int tz, bool cluster)
+ResidentKernel resident_kernel(int R, int tz, int exchange)
 {
+    if (exchange == 2) return R == 2 ? pick_sx(tz) : ResidentKernel{};
+    const bool cluster = exchange == 1;
     if (R == 2) return cluster ? pick<2, true>(tz) : pick<2, false>(tz);
     if (R == 4) return cluster ? pick<4, true>(tz) : pick<4, false>(tz);
     return ResidentKernel{};

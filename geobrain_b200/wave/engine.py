@@ -184,19 +184,23 @@ class Plan:
 
     def set_resident(self, mode, tile_rows: int = 0) -> None:
         """Resident forward: 'auto' (default), False (off), True or 'global'
-        (on, edge cells through global memory as (value, tag) words), or
-        'cluster' (on, edge cells stored into the neighbours' shared memory,
-        one cluster of at most 16 CTAs per shot); tile_rows 0 (smallest that
-        fits) or one of 4, 8, 12, 16, 24, 32, 36, 40."""
-        m = {"auto": -1, False: 0, True: 1, "global": 1, "cluster": 2}[mode]
+        (on, edge cells through global memory as (value, tag) words after the
+        p and the v updates), 'cluster' (on, edge cells stored into the
+        neighbours' shared memory, one cluster of at most 16 CTAs per shot),
+        or 'single' (on, one exchange a step: p also updated on the
+        neighbours' edge rows and columns; 4th order without a free surface);
+        tile_rows 0 (smallest that fits) or one of 4, 8, 12, 16, 24, 32, 36,
+        40."""
+        m = {"auto": -1, False: 0, True: 1, "global": 1, "cluster": 2, "single": 3}[mode]
         _lib.check(self._lib.gb_plan_set_resident(self.h, m, int(tile_rows)))
 
     def resident(self) -> dict:
         """The resident forward's tile rows (0: the tile kernel runs), shots
-        per launch, and exchange ('cluster' or 'global')."""
+        per launch, and exchange ('global', 'cluster' or 'single')."""
         tz, spl, cl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _lib.check(self._lib.gb_plan_get_resident(self.h, ctypes.byref(tz), ctypes.byref(spl), ctypes.byref(cl)))
-        return {"tile_rows": tz.value, "shots_per_launch": spl.value, "exchange": "cluster" if cl.value else "global"}
+        return {"tile_rows": tz.value, "shots_per_launch": spl.value,
+                "exchange": ("global", "cluster", "single")[cl.value]}
 
     def set_streaming(self, enable: bool, seg_chunks: int = 0) -> None:
         """Forward steps by the streaming kernel (0 chunks = automatic)."""

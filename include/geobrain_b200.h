@@ -177,14 +177,17 @@ int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const flo
  * GPU: few shots, or a small grid.  The traces are those of the tile kernel,
  * bit for bit.  mode: -1 automatic (the default: on when every shot's tiles
  * fit on the device's SMs at once, one CTA per SM, with the exchange through
- * global memory and the smallest tile height that fits), 0 off, 1 on with
- * the exchange
+ * global memory after each half-step and the smallest tile height that
+ * fits), 0 off, 1 on with the exchange
  * through global memory (a cooperative launch; each float travels as an
  * 8-byte (value, tag) word the receiver polls, bounded; shots beyond one
  * launch run in further launches), 2 on with the exchange through
  * distributed shared memory: one thread-block cluster of at most 16 CTAs per
  * shot, the sender storing into the neighbour's halo, hardware cluster
- * barriers in place of the tags.
+ * barriers in place of the tags; 3 on with one exchange a step through
+ * global memory, each tile also updating p on R rows and columns of its
+ * neighbours' cells from the same inputs (4th order without a free surface
+ * only).
  * tile_rows: 4, 8, 12, 16, 24, 32, 36 or 40, or 0 for the smallest that
  * fits.  With a free surface, rows fs-1 .. fs+1 must fall in one tile.
  * GB_E_UNSUPPORTED when mode 1 finds no tiling (or the plan uses CPML); the
@@ -192,8 +195,9 @@ int gb_plan_autotune(gb_plan *plan, const float *vp, const float *rho, const flo
  * by the exchange strips. */
 int gb_plan_set_resident(gb_plan *plan, int mode, int tile_rows);
 /* Tile rows of the resident forward in use (0: the tile kernel runs),
- * shots per launch, and whether the cluster exchange runs (1) or the
- * exchange through global memory (0).  Any pointer may be NULL. */
+ * shots per launch, and the exchange: 0 through global memory after each
+ * half-step, 1 through distributed shared memory, 2 once a step through
+ * global memory.  Any pointer may be NULL. */
 int gb_plan_get_resident(const gb_plan *plan, int *tile_rows, int *shots_per_launch, int *cluster);
 
 /* Run each group of shots on its own stream (forked from and joined back to

@@ -119,12 +119,38 @@ def test_cluster_exchange_free_surface(cuda_device, nabc, tile_rows, fd_order):
     assert info["exchange"] == "cluster"
 
 
+@pytest.mark.parametrize("shape,tile_rows", [((37, 53, 4, 70, 1), 0), ((60, 250, 10, 90, 3), 0),
+                                             ((90, 121, 12, 64, 2), 0), ((100, 200, 20, 120, 1), 0),
+                                             ((150, 330, 10, 50, 2), 4), ((150, 330, 10, 50, 2), 8),
+                                             ((150, 330, 10, 50, 2), 12), ((150, 330, 10, 50, 2), 16),
+                                             ((150, 330, 10, 50, 2), 24), ((150, 330, 10, 50, 2), 40)])
+def test_one_exchange_per_step_matches_tile_kernel(cuda_device, shape, tile_rows):
+    """4th order without a free surface: p also updated on the neighbours'
+    edge rows and columns, v exchanged once a step with all eight
+    neighbours; the tile kernel's traces and snapshots bit for bit."""
+    c = synthetic_case(shape[0], shape[1], shape[2], shape[3], shape[4], seed=47)
+    info = _compare(c, cuda_device, 4, tile_rows=tile_rows, snapshot_every=16, mode="single")
+    assert info["exchange"] == "single"
+
+
+def test_one_exchange_per_step_needs_4th_order_without_free_surface(cuda_device):
+    """Asked for only (it measured no faster than two exchanges on 100 x 200);
+    refused for the 8th order and with a free surface, and the plan stays
+    automatic."""
+    from geobrain_b200 import _lib
+    c = synthetic_case(100, 200, 20, 30, 1, seed=49)
+    assert _plan_of(c, 2).resident()["exchange"] == "global"
+    for plan in (_plan_of(c, 4), _plan_of(dict(c, free_surface=True), 2)):
+        assert plan._lib.gb_plan_set_resident(plan.h, 3, 0) == _lib.GB_E_UNSUPPORTED
+        assert plan.resident()["exchange"] == "global"
+
+
 def test_invalid_settings(cuda_device):
     """Unknown modes and tile heights are refused; the plan keeps its
     automatic choice."""
     from geobrain_b200 import _lib
     c = synthetic_case(40, 90, 10, 20, 1, seed=41)
     plan = _plan_of(c, 4)
-    for mode, rows in ((3, 0), (1, 10), (1, 48), (-2, 0)):
+    for mode, rows in ((4, 0), (1, 10), (1, 48), (-2, 0)):
         assert plan._lib.gb_plan_set_resident(plan.h, mode, rows) == _lib.GB_E_ARG
     assert plan.resident()["tile_rows"] > 0
