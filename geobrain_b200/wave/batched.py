@@ -280,18 +280,36 @@ def full_cache_bytes(plan, with_rho: bool, imaging_dtype: str) -> int:
 
 def plan_sub_batches(sizes: Sequence[int], avail: int) -> List[List[int]]:
     """Split models (in order) into consecutive sub-batches whose summed
-    sizes fit in `avail` bytes; a model larger than `avail` gets a sub-batch
-    of its own (it then keeps checkpoints for the steps that do not fit)."""
-    groups, cur, tot = [], [], 0
-    for i, b in enumerate(sizes):
-        if cur and tot + b > avail:
+    sizes fit in `avail` bytes, as few as fit and as even as they can be: a
+    greedy fill first counts the sub-batches, then the smallest per-batch cap
+    that still needs no more of them is taken (a greedy fill would leave the
+    last sub-batch a few models, too few to fill the GPU).  A model larger
+    than `avail` gets a sub-batch of its own (it then keeps checkpoints for
+    the steps that do not fit)."""
+    def fill(cap: int) -> List[List[int]]:
+        groups, cur, tot = [], [], 0
+        for i, b in enumerate(sizes):
+            if cur and tot + b > cap:
+                groups.append(cur)
+                cur, tot = [], 0
+            cur.append(i)
+            tot += b
+        if cur:
             groups.append(cur)
-            cur, tot = [], 0
-        cur.append(i)
-        tot += b
-    if cur:
-        groups.append(cur)
-    return groups
+        return groups
+
+    groups = fill(avail)
+    fitting = [b for b in sizes if b <= avail]
+    if len(groups) <= 1 or not fitting:
+        return groups
+    lo, hi = max(fitting), avail          # fill(hi) needs len(groups) sub-batches
+    while lo < hi:
+        mid = (lo + hi) // 2
+        if len(fill(mid)) <= len(groups):
+            hi = mid
+        else:
+            lo = mid + 1
+    return fill(hi)
 
 
 def acoustic_gradient_batched(models: Sequence[dict], residual, *, fd_order: int = 8, device=None,

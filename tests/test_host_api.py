@@ -182,3 +182,9 @@ def test_plan_sub_batches():
     assert plan_sub_batches([3, 3, 3, 3], 7) == [[0, 1], [2, 3]]
     assert plan_sub_batches([5, 9, 1], 6) == [[0], [1], [2]]
     assert plan_sub_batches([1, 1, 1], 100) == [[0, 1, 2]]
+    # as few as a greedy fill, but even: not [5 models] + [1]
+    assert plan_sub_batches([2] * 6, 10) == [[0, 1, 2], [3, 4, 5]]
+    groups = plan_sub_batches([4, 1, 3, 2, 5, 1, 2, 3], 11)
+    assert len(groups) == 2 and sorted(i for g in groups for i in g) == list(range(8))
+    assert max(sum([4, 1, 3, 2, 5, 1, 2, 3][i] for i in g) for g in groups) <= 11
+    assert [len(g) for g in plan_sub_batches([3] * 10, 20)] == [5, 5]
