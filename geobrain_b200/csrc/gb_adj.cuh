@@ -152,16 +152,12 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
                 jz[u] = ok ? load_img_raw(img_ptr, io + 2 * A.img_field_stride, img_fmt) : img_raw_zero();
             }
         }
-        if (!__syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1))) {
-            if (threadIdx.x == 0) {
-                atomicExch(A.err, -4);
-                if (k + 1 < ns) mbar_wait_bounded(&bars[b ^ 1], ((k + 1) >> 1) & 1);
-            }
-            return;
-        }
-        if (threadIdx.x == 0 && k >= 1 && k + 1 < ns)   // refill shot k-1's buffer with shot k+1
-            stage_loads<R>(mP, mVX, mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
-                           s + 1, G::P_FL, G::VX_FL);
+        // every thread waits (bounded) for this shot's stage; no CTA barrier
+        // here: the refill of shot k-1's buffer waits for the mid-shot
+        // barrier below, which every thread reaches only after finishing
+        // shot k-1.  A give-up sets the status word and the launch runs on
+        // (every thread still meets every barrier); its results are void.
+        if (!mbar_wait_bounded(&bars[b], (k >> 1) & 1)) atomicExch(A.err, -4);
         float *sP = smem + b * G::STAGE_FL;
         float *sVX = sP + G::P_FL;
         float *sVZ = sVX + G::VX_FL;
@@ -242,6 +238,11 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
             }
         }
         __syncthreads();
+        // every thread is done with shot k-1: refill its buffer with shot k+1
+        // (its generic-proxy writes were fenced at the end of shot k-1)
+        if (threadIdx.x == 0 && k >= 1 && k + 1 < ns)
+            stage_loads<R>(mP, mVX, mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
+                           s + 1, G::P_FL, G::VX_FL);
         if (A.grad_wavelet && threadIdx.x == 0) {
             // the tile that owns the source cell: mu_p / a1 there is lambda_p
             const int sz = A.src_z[s], sx = A.src_x[s];
@@ -341,6 +342,8 @@ __device__ __forceinline__ void adj_body(const CUtensorMap *mP, const CUtensorMa
                 }
             }
         }
+        // order this shot's generic-proxy shared-memory writes before the TMA
+        // that refills the buffer (after the next shot's mid-shot barrier)
         fence_proxy_async_smem();
     }
 

@@ -182,18 +182,12 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
     for (int k = 0; k < ns; ++k) {
         const int s = s0 + k;
         const int b = k & 1;
-        // every thread polls (bounded); the vote makes a give-up uniform, and
-        // also tells that every thread is done with shot k-1's buffer
-        if (!__syncthreads_and(mbar_wait_bounded(&bars[b], (k >> 1) & 1))) {
-            if (threadIdx.x == 0) {
-                atomicExch(A.err, -4);
-                if (k + 1 < ns) mbar_wait_bounded(&bars[b ^ 1], ((k + 1) >> 1) & 1);
-            }
-            return;
-        }
-        if (threadIdx.x == 0 && k >= 1 && k + 1 < ns)   // refill shot k-1's buffer with shot k+1
-            stage_loads<R>(mP, mVX, mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
-                           s + 1, G::P_FL, G::VX_FL);
+        // every thread waits (bounded) for this shot's stage; no CTA barrier
+        // here: the refill of shot k-1's buffer waits for the mid-shot
+        // barrier below, which every thread reaches only after finishing
+        // shot k-1.  A give-up sets the status word and the launch runs on
+        // (every thread still meets every barrier); its results are void.
+        if (!mbar_wait_bounded(&bars[b], (k >> 1) & 1)) atomicExch(A.err, -4);
         float *sP = smem + b * G::STAGE_FL;
         float *sVX = sP + G::P_FL;
         float *sVZ = sVX + G::VX_FL;
@@ -290,6 +284,11 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
             }
         }
         __syncthreads();
+        // every thread is done with shot k-1: refill its buffer with shot k+1
+        // (its generic-proxy writes were fenced at the end of shot k-1)
+        if (threadIdx.x == 0 && k >= 1 && k + 1 < ns)
+            stage_loads<R>(mP, mVX, mVZ, smem + (b ^ 1) * G::STAGE_FL, &bars[b ^ 1], G::STAGE_BYTES, x0, z0,
+                           s + 1, G::P_FL, G::VX_FL);
 
         if (FS && !fast) {
             // p[fs-1] = -p[fs+1] inside the rectangle
@@ -421,7 +420,8 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
             }
         }
         // order this iteration's generic-proxy shared-memory writes before the
-        // TMA that refills the buffer (issued after the next iteration's vote)
+        // TMA that refills the buffer (issued after the next iteration's
+        // mid-shot barrier)
         fence_proxy_async_smem();
     }
 
