@@ -277,6 +277,7 @@ def oracle_check_fwi(torch, wave, w, dev, imaging_dtype, shots=(5, 26), nt=150):
     the first 150 steps, 8th order, imaging fields cached in the benchmark's
     format (all 150 steps fit) and fp32 checkpoints, as timed.  The adjoint
     source is a seeded random residual (loss = sum(res * p))."""
+    nt = min(nt, w.nt)             # a shortened run (--nt) checks its own steps
     from oracle import oracle as orc
     kw, damp = _one_shot_kwargs(torch, wave, w, dev, list(shots), nt)
     res = np.random.default_rng(11).standard_normal((len(shots), nt, w.rcv_x.size)).astype(np.float32)
