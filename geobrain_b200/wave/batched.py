@@ -268,6 +268,10 @@ def _group_plan_array(plans):
     return (ctypes.c_void_p * len(plans))(*[p.h.value for p in plans])
 
 
+def _align256(n: int) -> int:
+    return (n + 255) // 256 * 256
+
+
 def full_cache_bytes(plan, with_rho: bool, imaging_dtype: str) -> int:
     """Device bytes one model of a fused batched gradient holds at its peak:
     the imaging fields of every step, the forward and gradient workspaces
@@ -359,11 +363,13 @@ def acoustic_gradient_batched(models: Sequence[dict], residual, *, fd_order: int
     losses = torch.zeros(n, dtype=torch.float32, device=device)
     grads_vp, grads_rho = [None] * n, [None] * n
     L = _bind()
-    for group in plan_sub_batches(sizes, max(avail, 0)):
+    groups = plan_sub_batches(sizes, max(avail, 0))
+
+    def store_layout(group):
+        """Per model of a sub-batch: (checkpoint_every, cached steps,
+        checkpoint offset and bytes, imaging offset and bytes) in the pool,
+        and the sub-batch's total."""
         plans = [prep.plans[i] for i in group]
-        arr = _group_plan_array(plans)
-        sub = _Sub(prep, group, arr)
-        stores, keep = [], []
         if len(group) == 1 and sizes[group[0]] > avail:
             # one model larger than the memory: cache what fits, checkpoint the rest
             p = plans[0]
@@ -372,17 +378,30 @@ def acoustic_gradient_batched(models: Sequence[dict], residual, *, fd_order: int
                                                 memory_budget)
         else:
             K, cached = max(p.geo.nt for p in plans), None
+        items, off = [], 0
         for p in plans:
             c = p.geo.nt if cached is None else cached
-            k = min(K, p.geo.nt)
-            n_ck = -(-(p.geo.nt - c) // k)
-            ck = torch.empty(max(n_ck * p.checkpoint_bytes(p.geo.nt, snapshot_dtype), 256), dtype=torch.uint8,
-                             device=device)
-            img = torch.empty(max(p.imaging_bytes(c, with_rho, imaging_dtype), 256), dtype=torch.uint8,
-                              device=device)
-            stores.append(engine.make_store(ck if n_ck > 0 else None, K, snapshot_dtype, img if c > 0 else None,
-                                            c, with_rho, imaging_dtype))
-            keep.append((ck, img))
+            n_ck = -(-(p.geo.nt - c) // min(K, p.geo.nt))
+            ckb = n_ck * p.checkpoint_bytes(p.geo.nt, snapshot_dtype) if n_ck > 0 else 0
+            imb = p.imaging_bytes(c, with_rho, imaging_dtype) if c > 0 else 0
+            items.append((K, c, off, ckb, off + _align256(ckb), imb))
+            off += _align256(ckb) + _align256(imb)
+        return items, off
+
+    # every sub-batch's stores come out of one pool, sized for the largest:
+    # allocated once, so the caching allocator is not asked for (and does not
+    # fragment on) a new set of blocks per sub-batch of other model sizes
+    layouts = [store_layout(g) for g in groups]
+    pool = torch.empty(max(max(t for _, t in layouts), 256), dtype=torch.uint8, device=device)
+    for group, (items, _) in zip(groups, layouts):
+        plans = [prep.plans[i] for i in group]
+        arr = _group_plan_array(plans)
+        sub = _Sub(prep, group, arr)
+        stores = []
+        for K, c, ck_off, ckb, im_off, imb in items:
+            ck = pool[ck_off:ck_off + ckb] if ckb else None
+            img = pool[im_off:im_off + imb] if imb else None
+            stores.append(engine.make_store(ck, K, snapshot_dtype, img, c, with_rho, imaging_dtype))
         outs = _forward(sub, [vps[i] for i in group], [rhos[i] for i in group], False, stores)
         res_list = []
         for j, i in enumerate(group):
@@ -413,7 +432,7 @@ def acoustic_gradient_batched(models: Sequence[dict], residual, *, fd_order: int
         with torch.cuda.device(device):
             rc = L.gb_batch_backward(arr, len(group), ios, bws.data_ptr(), bws.numel(), engine.stream_handle(device))
         _lib.check(rc)
-        del keep, wkeep, res_list, bws
+        del wkeep, res_list, bws
     if with_rho:
         return losses, grads_vp, grads_rho
     return losses, grads_vp
