@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--resident", choices=["auto", "on", "off", "global", "cluster"], default="auto",
                     help="--slice: resident forward (plain forward only) and its exchange")
     ap.add_argument("--resident-rows", type=int, default=0, help="--slice: resident tile rows (0 = automatic)")
+    ap.add_argument("--fused3", action="store_true", help="--slice --model 3d: the fused 3-D step kernel")
     return ap.parse_args()
 
 
@@ -126,6 +127,9 @@ def run_slice(args):
 
 
 def _slice_3d(torch, wave, args, dev, nz=200, ny=200, nx=200, shots=4, nabc=20):
+    if args.fused3:
+        from geobrain_b200 import _lib
+        _lib.load().gb3_set_fused_step(1)
     rng = np.random.default_rng(0)
     nt = args.nt
     vp = torch.tensor((2000 + 1000 * rng.random((nz, ny, nx))).astype(np.float32), device=dev)

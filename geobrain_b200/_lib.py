@@ -74,6 +74,7 @@ SIGNATURES = {
     "gb3_forward": (ctypes.c_int, [ctypes.POINTER(Desc3)] + [_P] * 6 + [_P] * 4 + [_P] * 8 + [_P, _I32] +
                     [_P, _I32] + [_P, _SZ, _P]),
     "gb3_imaging_bytes": (_SZ, [ctypes.POINTER(Desc3), _I32]),
+    "gb3_set_fused_step": (ctypes.c_int, [_I32]),
     "gb3_checkpoint_bytes": (_SZ, [ctypes.POINTER(Desc3), _I32]),
     "gb3_backward_workspace_bytes": (_SZ, [ctypes.POINTER(Desc3), _I32, _I32]),
     "gb3_backward": (ctypes.c_int, [ctypes.POINTER(Desc3)] + [_P] * 6 + [_P] * 4 + [_P] * 4 + [_P, _I32] +

@@ -64,6 +64,12 @@ int get_encoder(PFN_cuTensorMapEncodeTiled_v12000 *out)
     return GB_OK;
 }
 
+}  // namespace
+
+int gb::host::tensor_map_encoder(PFN_cuTensorMapEncodeTiled_v12000 *out) { return get_encoder(out); }
+
+namespace {
+
 // 3-D map over a field buffer laid out [n_planes][Nz][pitch] fp32, valid
 // extent Nx columns (columns >= Nx and rows outside [0, Nz) read as zero).
 int make_map(CUtensorMap *map, const float *base, int Nx, int Nz, int pitch, int n_planes, int box_x,

@@ -4,6 +4,7 @@
 #include "gb_host.h"
 
 #include "gb_3d.cuh"
+#include "gb_3d_fused.cuh"
 
 #include <algorithm>
 #include <string>
@@ -14,12 +15,160 @@ using gb::host::align256;
 using gb::host::aligned_ws;
 using gb::host::fail;
 
+namespace {
+
+// 1: one step3_fused_kernel launch per step (per 8 shots with energy maps),
+// state ping-ponging between two buffers; 0 (default): p3_kernel + v3_kernel
+// in place, the faster of the two as measured (93 against 25
+// Gcell-updates/s on 200^3 + 20 PML with 4 shots).
+int g_step3_fused = 0;
+
+constexpr int kF3Rows = 8;   // tile rows (y) of the fused step
+using F3G = F3Geo<kF3Rows>;
+using F3Fn = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const Fused3Args);
+
+F3Fn f3_kernel(bool energy, int img)
+{
+    static const F3Fn table[2][3] = {
+        {step3_fused_kernel<kF3Rows, false, 0>, step3_fused_kernel<kF3Rows, false, 1>,
+         step3_fused_kernel<kF3Rows, false, 2>},
+        {step3_fused_kernel<kF3Rows, true, 0>, step3_fused_kernel<kF3Rows, true, 1>,
+         step3_fused_kernel<kF3Rows, true, 2>}};
+    return table[energy ? 1 : 0][img];
+}
+
+// 4-D map over n_fields volumes [n_fields][Nz][Ny][pitch] fp32; boxes of 128
+// columns x box_rows rows of one plane; everything outside reads as zero.
+int make_map4(CUtensorMap *map, const float *base, const Geo3 &g, int n_fields, int box_rows)
+{
+    PFN_cuTensorMapEncodeTiled_v12000 enc;
+    if (int rc = gb::host::tensor_map_encoder(&enc)) return rc;
+    if (reinterpret_cast<uintptr_t>(base) & 15) return fail(GB_E_ARG, "3-D volume not 16-byte aligned");
+    cuuint64_t dims[4] = {(cuuint64_t)g.pitch, (cuuint64_t)g.Ny, (cuuint64_t)g.Nz, (cuuint64_t)n_fields};
+    cuuint64_t strides[3] = {(cuuint64_t)g.pitch * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.vol * 4};
+    cuuint32_t box[4] = {(cuuint32_t)F3G::ROW, (cuuint32_t)box_rows, 1, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(GB_E_CUDA, "cuTensorMapEncodeTiled (4-D) failed (" + std::to_string((int)r) + ")");
+    return GB_OK;
+}
+
+// The fused step's launch state: maps of both state buffers and of the
+// coefficients, the tiling, and which buffer holds the current state.
+struct Fused3 {
+    CUtensorMap mS[2], mY[2], mC;
+    float *buf[2];
+    int cur;
+    int tiles_x, tiles_y, chunk, n_chunks;
+};
+
+// Number of z-chunks: the launch's CTAs fill whole waves of the resident
+// slots, discounted by the 3 extra pressure planes each chunk recomputes.
+int f3_chunks(const Geo3 &g, int tiles, int ns, int slots)
+{
+    int best = 1;
+    double best_eff = 0.0;
+    for (int c = 1; c <= 32; ++c) {
+        const int chunk = (g.Nz + c - 1) / c;
+        if (chunk < 4 && c > 1) break;
+        const int n = (g.Nz + chunk - 1) / chunk;
+        const long long work = (long long)n * tiles * ns;
+        const long long waves = (work + slots - 1) / slots;
+        const double eff = (double)work / ((double)waves * slots) * chunk / (chunk + 3.0);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = n;
+        }
+    }
+    return best;
+}
+
+int fused3_setup(const Geo3 &g, float *buf0, float *buf1, const float *coef, bool energy, Fused3 *F)
+{
+    F->buf[0] = buf0;
+    F->buf[1] = buf1;
+    F->cur = 0;
+    for (int k = 0; k < 2; ++k) {
+        if (int rc = make_map4(&F->mS[k], F->buf[k], g, 4 * g.n_shots, F3G::PR)) return rc;
+        if (int rc = make_map4(&F->mY[k], F->buf[k], g, 4 * g.n_shots, F3G::YR)) return rc;
+    }
+    if (int rc = make_map4(&F->mC, coef, g, 6, F3G::PR)) return rc;
+    for (int e = 0; e < 2; ++e)
+        for (int i = 0; i < 3; ++i)
+            GB_CUDA(cudaFuncSetAttribute((const void *)f3_kernel(e != 0, i), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)F3G::SMEM));
+    int dev = 0, sms = 0, per_sm = 0;
+    GB_CUDA(cudaGetDevice(&dev));
+    GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)f3_kernel(energy, 0), F3G::NT,
+                                                          F3G::SMEM));
+    if (per_sm < 1) return fail(GB_E_UNSUPPORTED, "the fused 3-D step does not fit on this device");
+    F->tiles_x = (g.Nx + TX - 1) / TX;
+    F->tiles_y = (g.Ny + kF3Rows - 1) / kF3Rows;
+    const int ns = energy ? std::min(g.n_shots, kF3MaxCluster) : g.n_shots;
+    F->n_chunks = f3_chunks(g, F->tiles_x * F->tiles_y, ns, per_sm * sms);
+    F->chunk = (g.Nz + F->n_chunks - 1) / F->n_chunks;
+    F->n_chunks = (g.Nz + F->chunk - 1) / F->chunk;
+    return GB_OK;
+}
+
+// One time step of every shot from F->buf[cur] into the other buffer; with
+// energy maps the shots go in clusters of at most 8 (one launch each).
+int fused3_step(const Geo3 &g, Fused3 &F, Fused3Args &A, int it, cudaStream_t st)
+{
+    const bool energy = A.energy[0] != nullptr;
+    const int img = A.img_j ? 2 : A.img_i ? 1 : 0;
+    A.g = g;
+    A.it = it;
+    A.tiles_x = F.tiles_x;
+    A.tiles_y = F.tiles_y;
+    A.chunk = F.chunk;
+    A.in = F.buf[F.cur];
+    A.out = F.buf[F.cur ^ 1];
+    const int group = energy ? kF3MaxCluster : g.n_shots;
+    for (int s0 = 0; s0 < g.n_shots; s0 += group) {
+        A.shot0 = s0;
+        A.ns = std::min(group, g.n_shots - s0);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(F.n_chunks * F.tiles_y * F.tiles_x * A.ns));
+        cfg.blockDim = dim3(F3G::NT);
+        cfg.dynamicSmemBytes = F3G::SMEM;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        if (energy) {
+            attr[0].id = cudaLaunchAttributeClusterDimension;
+            attr[0].val.clusterDim.x = (unsigned)A.ns;
+            attr[0].val.clusterDim.y = 1;
+            attr[0].val.clusterDim.z = 1;
+            cfg.attrs = attr;
+            cfg.numAttrs = 1;
+        }
+        void *args[] = {(void *)&F.mS[F.cur], (void *)&F.mY[F.cur], (void *)&F.mC, (void *)&A};
+        GB_CUDA(cudaLaunchKernelExC(&cfg, (const void *)f3_kernel(energy, img), args));
+    }
+    F.cur ^= 1;
+    return GB_OK;
+}
+
+}  // namespace
+
 extern "C" {
+
+int gb3_set_fused_step(int32_t on)
+{
+    const int prev = g_step3_fused;
+    g_step3_fused = on != 0;
+    return prev;
+}
 
 namespace {
 
+// The device status word (gb_workspace_status) sits at offset 0 of both
+// layouts; state2 is the second state buffer of the fused step.
 struct Layout3 {
-    size_t state, coef, src, rcv, total;
+    size_t err, state, state2, coef, src, rcv, total;
 };
 
 bool geo3_of(const gb3_model_desc *d, Geo3 *g)
@@ -41,7 +190,9 @@ Layout3 layout3(const Geo3 &g)
 {
     Layout3 L{};
     size_t o = 0;
+    L.err = o; o = align256(o + 4);
     L.state = o; o = align256(o + (size_t)g.n_shots * 4 * g.vol * 4);
+    L.state2 = o; o = align256(o + (g_step3_fused ? (size_t)g.n_shots * 4 * g.vol * 4 : 0));
     L.coef = o; o = align256(o + 6 * (size_t)g.vol * 4);
     L.src = o; o = align256(o + 3 * (size_t)g.n_shots * 4);
     L.rcv = o; o = align256(o + 3 * (size_t)std::max(g.n_rcv, 1) * 4);
@@ -132,10 +283,15 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
         return fail(GB_E_WORKSPACE, "workspace too small");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     float *state = reinterpret_cast<float *>(ws + L.state);
+    float *state2 = reinterpret_cast<float *>(ws + L.state2);
     float *coef = reinterpret_cast<float *>(ws + L.coef);
     int *d_src = reinterpret_cast<int *>(ws + L.src), *d_rcv = reinterpret_cast<int *>(ws + L.rcv);
+    int *d_err = reinterpret_cast<int *>(ws + L.err);
+    const bool fused = L.state2 != L.coef;
     if (int rc = stage_positions3(g, src_x, src_y, src_z, rcv_x, rcv_y, rcv_z, d_src, d_rcv, st)) return rc;
+    GB_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
     GB_CUDA(cudaMemsetAsync(state, 0, (size_t)g.n_shots * 4 * g.vol * 4, st));
+    if (fused) GB_CUDA(cudaMemsetAsync(state2, 0, (size_t)g.n_shots * 4 * g.vol * 4, st));
     GB_CUDA(cudaMemsetAsync(coef, 0, 6 * (size_t)g.vol * 4, st));
     float *eout[4] = {energy_p, energy_vx, energy_vy, energy_vz};
     const bool want_energy = energy_p && energy_vx && energy_vy && energy_vz;
@@ -159,18 +315,35 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
     const bool want_tr = g.n_rcv > 0 && (trace_p || trace_vx || trace_vy || trace_vz);
     const size_t state_bytes = (size_t)g.n_shots * 4 * g.vol * 4;
     const size_t field = (size_t)g.n_shots * g.vol, blk = (imaging_rho ? 4 : 1) * field;
+    Fused3 FU{};
+    Fused3Args FA{};
+    if (fused) {
+        if (int rc = fused3_setup(g, state, state2, coef, want_energy, &FU)) return rc;
+        FA.free_surface = fs;
+        FA.a2 = A.a2; FA.k2 = A.k2; FA.k3 = A.k3; FA.k4 = A.k4;
+        FA.src = d_src;
+        FA.wavelet = wavelet;
+        for (int f = 0; f < 4; ++f) FA.energy[f] = A.energy[f];
+        FA.err = d_err;
+    }
     for (int it = 0; it < g.nt; ++it) {
         if (imaging) {   // this step's imaging fields, for a gradient without recompute
-            A.img_i = imaging + (size_t)it * blk;
-            A.img_j = imaging_rho ? A.img_i + field : nullptr;
+            A.img_i = FA.img_i = imaging + (size_t)it * blk;
+            A.img_j = FA.img_j = imaging_rho ? A.img_i + field : nullptr;
         }
+        const float *cur = fused ? FU.buf[FU.cur] : state;
         if (checkpoints && it % checkpoint_every == 0)   // the state before step it
             GB_CUDA(cudaMemcpyAsync(reinterpret_cast<char *>(checkpoints) + (size_t)(it / checkpoint_every) * state_bytes,
-                                    state, state_bytes, cudaMemcpyDeviceToDevice, st));
-        if (int rc = step3(g, A, it, fs, st)) return rc;
+                                    cur, state_bytes, cudaMemcpyDeviceToDevice, st));
+        if (fused) {
+            if (int rc = fused3_step(g, FU, FA, it, st)) return rc;
+        } else if (int rc = step3(g, A, it, fs, st)) {
+            return rc;
+        }
         if (want_tr)
-            rec3_kernel<<<(g.n_shots * g.n_rcv + 255) / 256, 256, 0, st>>>(g, state, d_rcv, trace_p, trace_vx,
-                                                                          trace_vy, trace_vz, it, nullptr);
+            rec3_kernel<<<(g.n_shots * g.n_rcv + 255) / 256, 256, 0, st>>>(g, fused ? FU.buf[FU.cur] : state, d_rcv,
+                                                                          trace_p, trace_vx, trace_vy, trace_vz, it,
+                                                                          nullptr);
         GB_CUDA(cudaGetLastError());
     }
     return GB_OK;
@@ -179,7 +352,7 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
 namespace {
 
 struct Layout3B {
-    size_t state, coef, src, rcv, lam_a, lam_b, img_i, img_j, g1, c1, g2, c2, total;
+    size_t err, state, state2, coef, src, rcv, lam_a, lam_b, img_i, img_j, g1, c1, g2, c2, total;
 };
 
 Layout3B layout3b(const Geo3 &g, int K, bool rho)
@@ -187,7 +360,9 @@ Layout3B layout3b(const Geo3 &g, int K, bool rho)
     Layout3B L{};
     size_t o = 0;
     const size_t st = (size_t)g.n_shots * 4 * g.vol * 4, f = (size_t)g.n_shots * g.vol * 4;
+    L.err = o; o = align256(o + 4);
     L.state = o; o = align256(o + st);
+    L.state2 = o; o = align256(o + (g_step3_fused && K > 0 ? st : 0));
     L.coef = o; o = align256(o + 6 * (size_t)g.vol * 4);
     L.src = o; o = align256(o + 3 * (size_t)g.n_shots * 4);
     L.rcv = o; o = align256(o + 3 * (size_t)std::max(g.n_rcv, 1) * 4);
@@ -244,6 +419,9 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
         return fail(GB_E_WORKSPACE, "workspace too small");
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     float *state = reinterpret_cast<float *>(ws + L.state);
+    float *state2 = reinterpret_cast<float *>(ws + L.state2);
+    const bool fused = L.state2 != L.coef;
+    int *d_err = reinterpret_cast<int *>(ws + L.err);
     float *coef = reinterpret_cast<float *>(ws + L.coef);
     int *d_src = reinterpret_cast<int *>(ws + L.src), *d_rcv = reinterpret_cast<int *>(ws + L.rcv);
     float *lam_a = reinterpret_cast<float *>(ws + L.lam_a), *lam_b = reinterpret_cast<float *>(ws + L.lam_b);
@@ -253,6 +431,9 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
     float *C2 = with_rho ? reinterpret_cast<float *>(ws + L.c2) : nullptr;
     if (int rc = stage_positions3(g, src_x, src_y, src_z, rcv_x, rcv_y, rcv_z, d_src, d_rcv, st)) return rc;
     const size_t state_bytes = (size_t)g.n_shots * 4 * g.vol * 4, field = (size_t)g.n_shots * g.vol;
+    GB_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
+    // columns [Nx, pitch) of both state buffers stay zero: a checkpoint brings them in as zeros
+    if (fused) GB_CUDA(cudaMemsetAsync(state2, 0, state_bytes, st));
     GB_CUDA(cudaMemsetAsync(coef, 0, 6 * (size_t)g.vol * 4, st));
     GB_CUDA(cudaMemsetAsync(lam_a, 0, state_bytes, st));
     GB_CUDA(cudaMemsetAsync(lam_b, 0, state_bytes, st));
@@ -278,6 +459,16 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
     A.a1 = F.a1; A.k1 = F.k1; A.a2 = F.a2; A.k2 = F.k2; A.k3 = F.k3; A.k4 = F.k4;
     A.G1 = G1; A.C1 = C1; A.G2 = G2; A.C2 = C2;
     const bool fs = desc->free_surface != 0;
+    Fused3 FU{};
+    Fused3Args FA{};
+    if (fused) {
+        if (int rc = fused3_setup(g, state, state2, coef, false, &FU)) return rc;
+        FA.free_surface = fs;
+        FA.a2 = F.a2; FA.k2 = F.k2; FA.k3 = F.k3; FA.k4 = F.k4;
+        FA.src = d_src;
+        FA.wavelet = wavelet;
+        FA.err = d_err;
+    }
     const dim3 block(32, 4), grid((g.Nx + 127) / 128, (g.Ny + 3) / 4, g.Nz);
     const size_t blk = (imaging_rho ? 4 : 1) * field;      // one step of the caller's imaging buffer
     const int n_seg = imaging ? 1 : (g.nt + K - 1) / K;
@@ -287,10 +478,15 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
             // recompute the segment from its checkpoint, keeping the imaging fields
             GB_CUDA(cudaMemcpyAsync(state, reinterpret_cast<const char *>(checkpoints) + (size_t)seg * state_bytes,
                                     state_bytes, cudaMemcpyDeviceToDevice, st));
+            FU.cur = 0;   // FU.buf[0] is `state`
             for (int it = t0; it < t1; ++it) {
-                F.img_i = img_i + (size_t)(it - t0) * field;
-                F.img_j = with_rho ? img_j + (size_t)(it - t0) * 3 * field : nullptr;
-                if (int rc = step3(g, F, it, fs, st)) return rc;
+                F.img_i = FA.img_i = img_i + (size_t)(it - t0) * field;
+                F.img_j = FA.img_j = with_rho ? img_j + (size_t)(it - t0) * 3 * field : nullptr;
+                if (fused) {
+                    if (int rc = fused3_step(g, FU, FA, it, st)) return rc;
+                } else if (int rc = step3(g, F, it, fs, st)) {
+                    return rc;
+                }
             }
         }
         // adjoint steps, last to first

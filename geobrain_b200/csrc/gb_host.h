@@ -5,6 +5,7 @@
 #include "../../include/geobrain_b200.h"
 
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cstddef>
 #include <cstdint>
@@ -17,6 +18,9 @@ namespace host {
 int fail(int code, const std::string &msg);
 // Clears this thread's last error (every C ABI entry point starts with it).
 void clear_error();
+// cuTensorMapEncodeTiled, looked up once through the runtime's driver entry
+// point (GB_E_CUDA if the driver has none).
+int tensor_map_encoder(PFN_cuTensorMapEncodeTiled_v12000 *out);
 
 inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 inline char *aligned_ws(void *workspace)

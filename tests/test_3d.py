@@ -237,3 +237,103 @@ def test_cuda_3d_wavelet_gradient_matches_oracle(cuda_device, imaging_cache):
                              with_wavelet=True)
     assert orc.rel_l2(w.grad.cpu().numpy(), rw) < 1e-4, orc.rel_l2(w.grad.cpu().numpy(), rw)
     assert orc.rel_l2(vp.grad.cpu().numpy(), rvp) < 1e-4
+
+
+def _fused_vs_split_case(shots, free_surface, nz=23, ny=19, nx=121, nabc=7, nt=40, seed=11):
+    rng = np.random.default_rng(seed)
+    vp = (2000 + 800 * rng.random((nz, ny, nx))).astype(np.float32)
+    rho = (1900 + 300 * rng.random((nz, ny, nx))).astype(np.float32)
+    from geobrain_b200.wave import bc_pml_3d, RickerWavelet
+    # the full padded damping (the 3-D entry point takes it whether or not the top is a free surface)
+    damp = bc_pml_3d(nx, ny, nz, 10.0, 10.0, 10.0, nabc, float(vp.max()), free_surface=False).astype(np.float32)
+    w, _ = RickerWavelet()(f0=20.0, dt=1e-3)
+    w = np.pad(w.numpy(), (0, nt))[:nt].astype(np.float32)
+    # sources: a grid corner, the last column of an x tile (padded 119), the padded border, then random
+    sx = np.concatenate([[-nabc, 119 - nabc, nx + nabc - 1], rng.integers(0, nx, shots)])[:shots]
+    sy = np.concatenate([[-nabc, 5, ny + nabc - 1], rng.integers(0, ny, shots)])[:shots]
+    sz = np.concatenate([[-nabc, 0, nz + nabc - 1], rng.integers(0, nz, shots)])[:shots]
+    return dict(nz=nz, ny=ny, nx=nx, nabc=nabc, nt=nt, dx=10.0, dt=1e-3, free_surface=free_surface, vp=vp,
+                rho=rho, damp=damp, src_x=sx, src_y=sy, src_z=sz, src_v=np.tile(w, (shots, 1)),
+                rcv_x=np.arange(0, nx, 3), rcv_y=np.full(len(range(0, nx, 3)), ny // 2),
+                rcv_z=np.full(len(range(0, nx, 3)), 3))   # below the free surface, where p is not 0
+
+
+def _with_step_kernel(fused, fn):
+    from geobrain_b200 import _lib
+    L = _lib.load()
+    prev = L.gb3_set_fused_step(int(fused))
+    try:
+        return fn()
+    finally:
+        L.gb3_set_fused_step(prev)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shots", [3, 10])
+@pytest.mark.parametrize("free_surface", [False, True])
+def test_cuda_3d_fused_step_equals_split_kernels(cuda_device, shots, free_surface):
+    """The fused step (one z-marching launch per step, csrc/gb_3d_fused.cuh)
+    against the split pressure / velocity kernels on a grid of 2 x 5 tiles
+    with ragged edges and sources on tile and grid borders: traces and both
+    gradients (recompute from checkpoints, and the imaging cache with the
+    density) bit-identical.  Energies: identical up to 8 shots (one cluster
+    adds its shots in order, as the split kernels' shot loop); above 8 the
+    clusters add to the maps one after another, within 1e-6."""
+    from geobrain_b200.wave import acoustic_forward_kernel_3d
+    c = _fused_vs_split_case(shots, free_surface)
+
+    def run():
+        out = run3(c, cuda_device)
+        grads = []
+        for segments, cache in ((3, 0), (1, "auto")):
+            vp = torch.tensor(c["vp"], device=cuda_device, requires_grad=True)
+            rho = torch.tensor(c["rho"], device=cuda_device, requires_grad=True)
+            o = acoustic_forward_kernel_3d(
+                nx=c["nx"], ny=c["ny"], nz=c["nz"], dx=c["dx"], dy=c["dx"], dz=c["dx"], nt=c["nt"], dt=c["dt"],
+                nabc=c["nabc"], free_surface=c["free_surface"], src_x=c["src_x"], src_y=c["src_y"],
+                src_z=c["src_z"], src_n=shots, src_v=torch.as_tensor(c["src_v"], device=cuda_device),
+                rcv_x=c["rcv_x"], rcv_y=c["rcv_y"], rcv_z=c["rcv_z"], rcv_n=len(c["rcv_x"]),
+                damp=torch.as_tensor(c["damp"], device=cuda_device), vp=vp, rho=rho,
+                checkpoint_segments=segments, device=cuda_device, imaging_cache=cache)
+            (0.5 * (o["p"] ** 2).sum() + o["vx"].sum() - o["vy"].sum() + o["vz"].sum()).backward()
+            grads.append((vp.grad.cpu().numpy(), rho.grad.cpu().numpy()))
+        return out, grads
+
+    split, g_split = _with_step_kernel(False, run)
+    fused, g_fused = _with_step_kernel(True, run)
+    for k in ("p", "vx", "vy", "vz"):
+        np.testing.assert_array_equal(fused[k], split[k], err_msg=k)
+    for k in KEYS[4:]:
+        if shots <= 8:
+            np.testing.assert_array_equal(fused[k], split[k], err_msg=k)
+        else:
+            assert orc.rel_l2(fused[k], split[k]) < 1e-6, k
+    assert np.abs(fused["p"]).max() > 0
+    for (gv_s, gr_s), (gv_f, gr_f) in zip(g_split, g_fused):
+        np.testing.assert_array_equal(gv_f, gv_s)
+        np.testing.assert_array_equal(gr_f, gr_s)
+
+
+@pytest.mark.gpu
+def test_cuda_3d_fused_step_at_the_benchmark_size(cuda_device):
+    """The 200^3 + 20-cell PML model with 4 shots (the 3-D rate workload),
+    20 steps: traces and energies of the fused step equal the split kernels'
+    bit for bit."""
+    rng = np.random.default_rng(0)
+    nz = ny = nx = 200
+    nabc, nt, shots = 20, 20, 4
+    from geobrain_b200.wave import bc_pml_3d, RickerWavelet
+    vp = (2000 + 1000 * rng.random((nz, ny, nx))).astype(np.float32)
+    w, _ = RickerWavelet()(f0=15.0, dt=1e-3)
+    w = np.pad(w.numpy(), (0, nt))[:nt].astype(np.float32)
+    c = dict(nz=nz, ny=ny, nx=nx, nabc=nabc, nt=nt, dx=10.0, dt=1e-3, free_surface=False, vp=vp,
+             rho=np.full((nz, ny, nx), 2000.0, np.float32),
+             damp=bc_pml_3d(nx, ny, nz, 10.0, 10.0, 10.0, nabc, 3000.0, free_surface=False).astype(np.float32),
+             src_x=np.linspace(10, nx - 10, shots).astype(np.int64), src_y=np.full(shots, ny // 2),
+             src_z=np.ones(shots, np.int64), src_v=np.tile(w, (shots, 1)), rcv_x=np.arange(0, nx, 2),
+             rcv_y=np.full(nx // 2, ny // 2), rcv_z=np.ones(nx // 2, np.int64))
+    split = _with_step_kernel(False, lambda: run3(c, cuda_device))
+    fused = _with_step_kernel(True, lambda: run3(c, cuda_device))
+    for k in KEYS:
+        np.testing.assert_array_equal(fused[k], split[k], err_msg=k)
+    assert np.abs(fused["p"]).max() > 0
