@@ -62,7 +62,8 @@ def parse():
     ap.add_argument("--resident", choices=["auto", "on", "off", "global", "cluster"], default="auto",
                     help="--slice: resident forward (plain forward only) and its exchange")
     ap.add_argument("--resident-rows", type=int, default=0, help="--slice: resident tile rows (0 = automatic)")
-    ap.add_argument("--fused3", action="store_true", help="--slice --model 3d: the fused 3-D step kernel")
+    ap.add_argument("--fused3", type=int, default=0, choices=[0, 1, 2],
+                    help="--slice --model 3d: the fused 3-D step kernel with 8- (1) or 16-row (2) tiles")
     return ap.parse_args()
 
 
@@ -129,7 +130,7 @@ def run_slice(args):
 def _slice_3d(torch, wave, args, dev, nz=200, ny=200, nx=200, shots=4, nabc=20):
     if args.fused3:
         from geobrain_b200 import _lib
-        _lib.load().gb3_set_fused_step(1)
+        _lib.load().gb3_set_fused_step(args.fused3)
     rng = np.random.default_rng(0)
     nt = args.nt
     vp = torch.tensor((2000 + 1000 * rng.random((nz, ny, nx))).astype(np.float32), device=dev)

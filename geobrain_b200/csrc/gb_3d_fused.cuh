@@ -46,6 +46,9 @@ struct F3Geo {
     static constexpr int PR = TY + 3;      // p rows: y0-1 .. y0+TY+1
     static constexpr int YR = TY + 6;      // vy rows: y0-3 .. y0+TY+2
     static constexpr int NT = PR * 32;     // one warp per p row
+    // registers per thread: 8-row tiles run 2 CTAs (22 warps) per SM, at most
+    // 6 warps per SM sub-partition of 16K registers; 16-row tiles 1 CTA of 19
+    static constexpr int MAXREG = TY <= 8 ? 80 : 96;
     static constexpr int ROW = 128;        // floats per staged row
     static constexpr int S_P = 0;
     static constexpr int S_VX = PR * ROW;
@@ -90,7 +93,14 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
         : "memory");
 }
 
+// Cluster barrier halves.  The warps that wrote squares arrive with release
+// semantics (their shared-memory writes must reach the other CTAs); the
+// others arrive relaxed, so they do not wait for their global stores.
 __device__ __forceinline__ void f3_cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void f3_cluster_arrive_relaxed()
+{
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+}
 __device__ __forceinline__ void f3_cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ float4 f3_ld_cluster4(const float *local, int rank)
@@ -112,15 +122,16 @@ __device__ __forceinline__ float4 sq4(const float4 &v)
 
 // Adds plane zr's squares over the cluster's CTAs, in shot order, into the
 // energy maps: CTA `rank` of the cluster takes every ns-th (field, tile row,
-// lane) item.  No barrier inside: the caller brackets it.
+// lane) item, spread over the 96 threads of its three halo warps (hid).  No
+// barrier inside: the caller brackets it.
 template <int TY>
 __device__ __forceinline__ void f3_energy_reduce(const Fused3Args &A, const float *ebuf, int rank, int zr, int y0,
-                                                 int x0)
+                                                 int x0, int hid)
 {
     using G = F3Geo<TY>;
     const Geo3 &g = A.g;
     if (zr < g.pml || zr >= g.pml + g.nz) return;
-    for (int it = rank + A.ns * (int)threadIdx.x; it < G::E_ITEMS; it += A.ns * G::NT) {
+    for (int it = rank + A.ns * hid; it < G::E_ITEMS; it += A.ns * 96) {
         const int f = it / (TY * 30), rest = it - f * (TY * 30);
         const int row = rest / 30, lane = 1 + rest % 30;
         const int y = y0 + row;
@@ -147,7 +158,7 @@ __device__ __forceinline__ void f3_energy_reduce(const Fused3Args &A, const floa
 // (z-chunk, tile row, tile column, shot), shot fastest; with ENERGY the
 // launch's ns shots of a tile form one cluster.
 template <int TY, bool ENERGY, int IMG>
-__global__ void __launch_bounds__(F3Geo<TY>::NT, 2)
+__global__ void __maxnreg__(F3Geo<TY>::MAXREG)
 step3_fused_kernel(const __grid_constant__ CUtensorMap mS,   // `in`: [4S][Nz][Ny][pitch], box 128 x PR
                    const __grid_constant__ CUtensorMap mY,   // `in`, box 128 x YR
                    const __grid_constant__ CUtensorMap mC,   // coefficients [6][Nz][Ny][pitch], box 128 x PR
@@ -176,6 +187,7 @@ step3_fused_kernel(const __grid_constant__ CUtensorMap mS,   // `in`: [4S][Nz][N
     const int y = y0 - 1 + pr;
     const int gx0 = x0 - 4 + 4 * lane;
     const bool vwarp = pr >= 1 && pr <= TY;
+    const int hid = (pr == 0 ? 0 : pr - TY) * 32 + lane;   // halo warps 0, TY+1, TY+2: 0 .. 95
     const bool own = vwarp && lane >= 1 && lane <= 30 && y < g.Ny && gx0 < g.Nx;
     const bool cell_ok = y >= 0 && y < g.Ny && gx0 >= 0 && gx0 < g.pitch;
     const long long rowo = (long long)y * g.pitch + gx0;   // dereferenced for in-grid cells only
@@ -216,12 +228,24 @@ step3_fused_kernel(const __grid_constant__ CUtensorMap mS,   // `in`: [4S][Nz][N
     const int sz = A.src[s], sy = A.src[g.n_shots + s], sx = A.src[2 * g.n_shots + s];
     const bool src_here = sy == y && sx >= gx0 && sx < gx0 + 4;
     const float amp = __fmul_rn(g.dt, A.wavelet[(long long)s * g.nt + A.it]);
-    if (ENERGY) f3_cluster_arrive();
+    if (ENERGY) f3_cluster_arrive_relaxed();
 
     bool live = true;   // false once a stage wait gave up (the results are then void)
     for (int j = 0; j < n_it; ++j) {
         const int zp = zs - 1 + j, zv = zp - 2;
         const int k = j & 1;
+        // the velocity phase's global loads of plane zv, issued before the
+        // stage wait and the pressure phase that hide their latency
+        float4 vx = zero4(), vy = zero4(), a2 = zero4(), k2 = zero4(), k3 = zero4(), k4 = zero4();
+        if (own && j >= 3) {
+            const long long o = (long long)zv * g.plane + rowo;
+            vx = ldg4(inS + g.vol + o);
+            vy = ldg4(inS + 2 * g.vol + o);
+            a2 = ldg4(A.a2 + o);
+            k2 = ldg4(A.k2 + o);
+            k3 = ldg4(A.k3 + o);
+            k4 = ldg4(A.k4 + o);
+        }
         if (live && !mbar_wait_bounded(&bars[k], (j >> 1) & 1)) {
             live = false;
             atomicExch(A.err, -4);
@@ -273,81 +297,66 @@ step3_fused_kernel(const __grid_constant__ CUtensorMap mS,   // `in`: [4S][Nz][N
         // every thread is done with stage k: refill it with plane zp + 2
         if (threadIdx.x == 0 && j + 2 < n_it) issue(zp + 2, k);
 
-        // ---- energy of the previous velocity plane -------------------------
-        if (ENERGY && j >= 4) {
-            f3_cluster_wait();
-            f3_energy_reduce<TY>(A, ebuf, rank, zv - 1, y0, x0);
-            f3_cluster_arrive();
+        // ---- energy of the previous velocity plane, by the halo warps -------
+        if (ENERGY && j >= 3) {
+            f3_cluster_wait();                 // the squares of plane zv-1 are in every CTA
+            if (!vwarp && j >= 4) f3_energy_reduce<TY>(A, ebuf, rank, zv - 1, y0, x0, hid);
+            f3_cluster_arrive_relaxed();       // ... and read (the sums use every value read)
         }
 
         // ---- velocities of plane zv = zp - 2 on the tile --------------------
         if (j >= 3) {
-            float4 pc = zero4(), vx = zero4(), vy = zero4(), vz = vzq[0];
+            float4 pc = zero4(), vz = vzq[0];
+            const long long o = (long long)zv * g.plane + rowo;
             if (vwarp) {
                 const float *rz = ring + (zv & 3) * PRF;
                 pc = lds4(rz + so);
                 const float pl = __shfl_up_sync(FULL, pc.w, 1);
                 const float pr1 = __shfl_down_sync(FULL, pc.x, 1), pr2 = __shfl_down_sync(FULL, pc.y, 1);
-                if (own) {
-                    const long long o = (long long)zv * g.plane + rowo;
-                    vx = ldg4(inS + g.vol + o);
-                    vy = ldg4(inS + 2 * g.vol + o);
-                    const bool zin = zv >= g.fs && zv < g.Nz - 1;
-                    const bool vx_row = zin && y >= 1 && y < g.Ny - 1;
-                    const bool vy_row = zin && y >= 1 && y < g.Ny - 2;
-                    const bool vz_row = zv >= g.fs && zv < g.Nz - 2 && y >= 1 && y < g.Ny - 1;
-                    if (vx_row || vy_row || vz_row) {
-                        const float4 a2 = ldg4(A.a2 + o), k2 = ldg4(A.k2 + o), k3 = ldg4(A.k3 + o),
-                                     k4 = ldg4(A.k4 + o);
-                        if (vx_row) {
-                            const float ps[7] = {pl, pc.x, pc.y, pc.z, pc.w, pr1, pr2};   // ps[q + 1] = p[x + q]
+                const bool zin = zv >= g.fs && zv < g.Nz - 1;
+                const bool vx_row = own && zin && y >= 1 && y < g.Ny - 1;
+                const bool vy_row = own && zin && y >= 1 && y < g.Ny - 2;
+                const bool vz_row = own && zv >= g.fs && zv < g.Nz - 2 && y >= 1 && y < g.Ny - 1;
+                if (vx_row) {
+                    const float ps[7] = {pl, pc.x, pc.y, pc.z, pc.w, pr1, pr2};   // ps[q + 1] = p[x + q]
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                const int x = gx0 + q;
-                                if (x < 1 || x >= g.Nx - 2) continue;
-                                const float dp = d4(ps[q + 2], ps[q + 1], ps[q + 3], ps[q]);
-                                at(vx, q) = __fsub_rn(__fmul_rn(__fsub_rn(1.f, at(k2, q)), at(vx, q)),
-                                                      __fmul_rn(at(a2, q), dp));
-                                if (IMG == 2) A.img_j[(long long)s * g.vol + o + q] = dp;
-                            }
-                        }
-                        if (vy_row) {
-                            const float4 ym1 = lds4(rz + so - G::ROW), yp1 = lds4(rz + so + G::ROW),
-                                         yp2 = lds4(rz + so + 2 * G::ROW);
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                const int x = gx0 + q;
-                                if (x < 1 || x >= g.Nx - 1) continue;
-                                const float dp = d4(at(yp1, q), at(pc, q), at(yp2, q), at(ym1, q));
-                                at(vy, q) = __fsub_rn(__fmul_rn(__fsub_rn(1.f, at(k3, q)), at(vy, q)),
-                                                      __fmul_rn(at(a2, q), dp));
-                                if (IMG == 2) A.img_j[((long long)g.n_shots + s) * g.vol + o + q] = dp;
-                            }
-                        }
-                        if (vz_row) {
-                            const float4 zm1 = lds4(ring + ((zv - 1) & 3) * PRF + so),
-                                         zp1 = lds4(ring + ((zv + 1) & 3) * PRF + so),
-                                         zp2 = lds4(ring + ((zv + 2) & 3) * PRF + so);
-#pragma unroll
-                            for (int q = 0; q < 4; ++q) {
-                                const int x = gx0 + q;
-                                if (x < 1 || x >= g.Nx - 1) continue;
-                                const float dp = d4(at(zp1, q), at(pc, q), at(zp2, q), at(zm1, q));
-                                at(vz, q) = __fsub_rn(__fmul_rn(__fsub_rn(1.f, at(k4, q)), at(vz, q)),
-                                                      __fmul_rn(at(a2, q), dp));
-                                if (IMG == 2) A.img_j[(2LL * g.n_shots + s) * g.vol + o + q] = dp;
-                            }
-                        }
+                    for (int q = 0; q < 4; ++q) {
+                        const int x = gx0 + q;
+                        if (x < 1 || x >= g.Nx - 2) continue;
+                        const float dp = d4(ps[q + 2], ps[q + 1], ps[q + 3], ps[q]);
+                        at(vx, q) = __fsub_rn(__fmul_rn(__fsub_rn(1.f, at(k2, q)), at(vx, q)), __fmul_rn(at(a2, q), dp));
+                        if (IMG == 2) A.img_j[(long long)s * g.vol + o + q] = dp;
                     }
-                    stg4(outS + o, pc);
-                    stg4(outS + g.vol + o, vx);
-                    stg4(outS + 2 * g.vol + o, vy);
-                    // vz[fs-1] = vz[fs]: the CTA of plane fs writes the mirror plane
-                    if (!(fs_on && zv == g.fs - 1)) stg4(outS + 3 * g.vol + o, vz);
-                    if (fs_on && zv == g.fs) stg4(outS + 3 * g.vol + (long long)(g.fs - 1) * g.plane + rowo, vz);
+                }
+                if (vy_row) {
+                    const float4 ym1 = lds4(rz + so - G::ROW), yp1 = lds4(rz + so + G::ROW),
+                                 yp2 = lds4(rz + so + 2 * G::ROW);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int x = gx0 + q;
+                        if (x < 1 || x >= g.Nx - 1) continue;
+                        const float dp = d4(at(yp1, q), at(pc, q), at(yp2, q), at(ym1, q));
+                        at(vy, q) = __fsub_rn(__fmul_rn(__fsub_rn(1.f, at(k3, q)), at(vy, q)), __fmul_rn(at(a2, q), dp));
+                        if (IMG == 2) A.img_j[((long long)g.n_shots + s) * g.vol + o + q] = dp;
+                    }
+                }
+                if (vz_row) {
+                    const float4 zm1 = lds4(ring + ((zv - 1) & 3) * PRF + so),
+                                 zp1 = lds4(ring + ((zv + 1) & 3) * PRF + so),
+                                 zp2 = lds4(ring + ((zv + 2) & 3) * PRF + so);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int x = gx0 + q;
+                        if (x < 1 || x >= g.Nx - 1) continue;
+                        const float dp = d4(at(zp1, q), at(pc, q), at(zp2, q), at(zm1, q));
+                        at(vz, q) = __fsub_rn(__fmul_rn(__fsub_rn(1.f, at(k4, q)), at(vz, q)), __fmul_rn(at(a2, q), dp));
+                        if (IMG == 2) A.img_j[(2LL * g.n_shots + s) * g.vol + o + q] = dp;
+                    }
                 }
             }
             if (ENERGY) {
+                // hand the squares to the cluster before this plane's global
+                // stores, so the release below waits for none of them
                 f3_cluster_wait();   // every CTA of the cluster is done reading the previous squares
                 if (vwarp) {
                     float *e = ebuf + ((pr - 1) * 32 + lane) * 4;
@@ -355,15 +364,25 @@ step3_fused_kernel(const __grid_constant__ CUtensorMap mS,   // `in`: [4S][Nz][N
                     sts4(e + TY * 32 * 4, sq4(vx));
                     sts4(e + 2 * TY * 32 * 4, sq4(vy));
                     sts4(e + 3 * TY * 32 * 4, sq4(vz));
+                    f3_cluster_arrive();
+                } else {
+                    f3_cluster_arrive_relaxed();
                 }
-                f3_cluster_arrive();
+            }
+            if (own) {
+                stg4(outS + o, pc);
+                stg4(outS + g.vol + o, vx);
+                stg4(outS + 2 * g.vol + o, vy);
+                // vz[fs-1] = vz[fs]: the CTA of plane fs writes the mirror plane
+                if (!(fs_on && zv == g.fs - 1)) stg4(outS + 3 * g.vol + o, vz);
+                if (fs_on && zv == g.fs) stg4(outS + 3 * g.vol + (long long)(g.fs - 1) * g.plane + rowo, vz);
             }
         }
     }
     if (ENERGY) {
         f3_cluster_wait();
-        f3_energy_reduce<TY>(A, ebuf, rank, ze - 1, y0, x0);
-        f3_cluster_arrive();
+        if (!vwarp) f3_energy_reduce<TY>(A, ebuf, rank, ze - 1, y0, x0, hid);
+        f3_cluster_arrive_relaxed();
         f3_cluster_wait();   // no CTA leaves while another reads its squares
     }
 }

@@ -17,24 +17,36 @@ using gb::host::fail;
 
 namespace {
 
-// 1: one step3_fused_kernel launch per step (per 8 shots with energy maps),
-// state ping-ponging between two buffers; 0 (default): p3_kernel + v3_kernel
-// in place, the faster of the two as measured (93 against 25
-// Gcell-updates/s on 200^3 + 20 PML with 4 shots).
+// 1 / 2: one step3_fused_kernel launch per step (per 8 shots with energy
+// maps) with tiles of 8 / 16 rows, the state ping-ponging between two
+// buffers; 0 (default): p3_kernel + v3_kernel in place, the faster as
+// measured.
 int g_step3_fused = 0;
 
-constexpr int kF3Rows = 8;   // tile rows (y) of the fused step
-using F3G = F3Geo<kF3Rows>;
 using F3Fn = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const Fused3Args);
 
-F3Fn f3_kernel(bool energy, int img)
+// What the host needs of one tile height of the fused step.
+struct F3Shape {
+    int rows, pr, yr, threads;
+    size_t smem;
+    F3Fn fn[2][3];   // [energy][imaging fields]
+};
+
+template <int TY>
+F3Shape f3_shape()
 {
-    static const F3Fn table[2][3] = {
-        {step3_fused_kernel<kF3Rows, false, 0>, step3_fused_kernel<kF3Rows, false, 1>,
-         step3_fused_kernel<kF3Rows, false, 2>},
-        {step3_fused_kernel<kF3Rows, true, 0>, step3_fused_kernel<kF3Rows, true, 1>,
-         step3_fused_kernel<kF3Rows, true, 2>}};
-    return table[energy ? 1 : 0][img];
+    using G = F3Geo<TY>;
+    return F3Shape{TY, G::PR, G::YR, G::NT, G::SMEM,
+                   {{step3_fused_kernel<TY, false, 0>, step3_fused_kernel<TY, false, 1>,
+                     step3_fused_kernel<TY, false, 2>},
+                    {step3_fused_kernel<TY, true, 0>, step3_fused_kernel<TY, true, 1>,
+                     step3_fused_kernel<TY, true, 2>}}};
+}
+
+const F3Shape &f3_shape_of(int mode)
+{
+    static const F3Shape s8 = f3_shape<8>(), s16 = f3_shape<16>();
+    return mode == 2 ? s16 : s8;
 }
 
 // 4-D map over n_fields volumes [n_fields][Nz][Ny][pitch] fp32; boxes of 128
@@ -46,7 +58,7 @@ int make_map4(CUtensorMap *map, const float *base, const Geo3 &g, int n_fields, 
     if (reinterpret_cast<uintptr_t>(base) & 15) return fail(GB_E_ARG, "3-D volume not 16-byte aligned");
     cuuint64_t dims[4] = {(cuuint64_t)g.pitch, (cuuint64_t)g.Ny, (cuuint64_t)g.Nz, (cuuint64_t)n_fields};
     cuuint64_t strides[3] = {(cuuint64_t)g.pitch * 4, (cuuint64_t)g.plane * 4, (cuuint64_t)g.vol * 4};
-    cuuint32_t box[4] = {(cuuint32_t)F3G::ROW, (cuuint32_t)box_rows, 1, 1};
+    cuuint32_t box[4] = {128, (cuuint32_t)box_rows, 1, 1};
     cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float *>(base), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -62,6 +74,7 @@ struct Fused3 {
     float *buf[2];
     int cur;
     int tiles_x, tiles_y, chunk, n_chunks;
+    const F3Shape *shape;
 };
 
 // Number of z-chunks: the launch's CTAs fill whole waves of the resident
@@ -87,26 +100,28 @@ int f3_chunks(const Geo3 &g, int tiles, int ns, int slots)
 
 int fused3_setup(const Geo3 &g, float *buf0, float *buf1, const float *coef, bool energy, Fused3 *F)
 {
+    const F3Shape &sh = f3_shape_of(g_step3_fused);
+    F->shape = &sh;
     F->buf[0] = buf0;
     F->buf[1] = buf1;
     F->cur = 0;
     for (int k = 0; k < 2; ++k) {
-        if (int rc = make_map4(&F->mS[k], F->buf[k], g, 4 * g.n_shots, F3G::PR)) return rc;
-        if (int rc = make_map4(&F->mY[k], F->buf[k], g, 4 * g.n_shots, F3G::YR)) return rc;
+        if (int rc = make_map4(&F->mS[k], F->buf[k], g, 4 * g.n_shots, sh.pr)) return rc;
+        if (int rc = make_map4(&F->mY[k], F->buf[k], g, 4 * g.n_shots, sh.yr)) return rc;
     }
-    if (int rc = make_map4(&F->mC, coef, g, 6, F3G::PR)) return rc;
+    if (int rc = make_map4(&F->mC, coef, g, 6, sh.pr)) return rc;
     for (int e = 0; e < 2; ++e)
         for (int i = 0; i < 3; ++i)
-            GB_CUDA(cudaFuncSetAttribute((const void *)f3_kernel(e != 0, i), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)F3G::SMEM));
+            GB_CUDA(cudaFuncSetAttribute((const void *)sh.fn[e][i], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sh.smem));
     int dev = 0, sms = 0, per_sm = 0;
     GB_CUDA(cudaGetDevice(&dev));
     GB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)f3_kernel(energy, 0), F3G::NT,
-                                                          F3G::SMEM));
+    GB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)sh.fn[energy ? 1 : 0][0], sh.threads,
+                                                          sh.smem));
     if (per_sm < 1) return fail(GB_E_UNSUPPORTED, "the fused 3-D step does not fit on this device");
     F->tiles_x = (g.Nx + TX - 1) / TX;
-    F->tiles_y = (g.Ny + kF3Rows - 1) / kF3Rows;
+    F->tiles_y = (g.Ny + sh.rows - 1) / sh.rows;
     const int ns = energy ? std::min(g.n_shots, kF3MaxCluster) : g.n_shots;
     F->n_chunks = f3_chunks(g, F->tiles_x * F->tiles_y, ns, per_sm * sms);
     F->chunk = (g.Nz + F->n_chunks - 1) / F->n_chunks;
@@ -133,8 +148,8 @@ int fused3_step(const Geo3 &g, Fused3 &F, Fused3Args &A, int it, cudaStream_t st
         A.ns = std::min(group, g.n_shots - s0);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)(F.n_chunks * F.tiles_y * F.tiles_x * A.ns));
-        cfg.blockDim = dim3(F3G::NT);
-        cfg.dynamicSmemBytes = F3G::SMEM;
+        cfg.blockDim = dim3(F.shape->threads);
+        cfg.dynamicSmemBytes = F.shape->smem;
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         if (energy) {
@@ -146,7 +161,7 @@ int fused3_step(const Geo3 &g, Fused3 &F, Fused3Args &A, int it, cudaStream_t st
             cfg.numAttrs = 1;
         }
         void *args[] = {(void *)&F.mS[F.cur], (void *)&F.mY[F.cur], (void *)&F.mC, (void *)&A};
-        GB_CUDA(cudaLaunchKernelExC(&cfg, (const void *)f3_kernel(energy, img), args));
+        GB_CUDA(cudaLaunchKernelExC(&cfg, (const void *)F.shape->fn[energy ? 1 : 0][img], args));
     }
     F.cur ^= 1;
     return GB_OK;
@@ -159,7 +174,7 @@ extern "C" {
 int gb3_set_fused_step(int32_t on)
 {
     const int prev = g_step3_fused;
-    g_step3_fused = on != 0;
+    g_step3_fused = (on == 1 || on == 2) ? on : 0;
     return prev;
 }
 

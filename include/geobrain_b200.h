@@ -432,9 +432,10 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
                  void *workspace, size_t workspace_bytes, void *stream);
 
 /* Selects the 3-D step kernels, process-wide (default 0):
- *   1  one fused launch per time step (per 8 shots when energy maps are
- *      asked for): pressure, source, mirrors and velocities of a z-chunk,
- *      TMA-staged, the state alternating between two workspace buffers;
+ *   1, 2  one fused launch per time step (per 8 shots when energy maps
+ *      are asked for): pressure, source, mirrors and velocities of a
+ *      z-chunk, TMA-staged, in tiles of 8 (1) or 16 (2) rows, the state
+ *      alternating between two workspace buffers;
  *   0  the split pressure and velocity kernels, one state updated in place
  *      (the faster: 93 against 25 Gcell-updates/s measured on a 200^3 model
  *      with a 20-cell PML and 4 shots).

@@ -258,10 +258,10 @@ def _fused_vs_split_case(shots, free_surface, nz=23, ny=19, nx=121, nabc=7, nt=4
                 rcv_z=np.full(len(range(0, nx, 3)), 3))   # below the free surface, where p is not 0
 
 
-def _with_step_kernel(fused, fn):
+def _with_step_kernel(mode, fn):
     from geobrain_b200 import _lib
     L = _lib.load()
-    prev = L.gb3_set_fused_step(int(fused))
+    prev = L.gb3_set_fused_step(int(mode))
     try:
         return fn()
     finally:
@@ -269,11 +269,13 @@ def _with_step_kernel(fused, fn):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("mode", [1, 2])
 @pytest.mark.parametrize("shots", [3, 10])
 @pytest.mark.parametrize("free_surface", [False, True])
-def test_cuda_3d_fused_step_equals_split_kernels(cuda_device, shots, free_surface):
-    """The fused step (one z-marching launch per step, csrc/gb_3d_fused.cuh)
-    against the split pressure / velocity kernels on a grid of 2 x 5 tiles
+def test_cuda_3d_fused_step_equals_split_kernels(cuda_device, mode, shots, free_surface):
+    """The fused step (one z-marching launch per step, csrc/gb_3d_fused.cuh;
+    mode 1: 8-row tiles, mode 2: 16-row tiles) against the split pressure /
+    velocity kernels on a grid of 2 x 5 (2 x 3) tiles
     with ragged edges and sources on tile and grid borders: traces and both
     gradients (recompute from checkpoints, and the imaging cache with the
     density) bit-identical.  Energies: identical up to 8 shots (one cluster
@@ -299,8 +301,8 @@ def test_cuda_3d_fused_step_equals_split_kernels(cuda_device, shots, free_surfac
             grads.append((vp.grad.cpu().numpy(), rho.grad.cpu().numpy()))
         return out, grads
 
-    split, g_split = _with_step_kernel(False, run)
-    fused, g_fused = _with_step_kernel(True, run)
+    split, g_split = _with_step_kernel(0, run)
+    fused, g_fused = _with_step_kernel(mode, run)
     for k in ("p", "vx", "vy", "vz"):
         np.testing.assert_array_equal(fused[k], split[k], err_msg=k)
     for k in KEYS[4:]:
@@ -315,7 +317,8 @@ def test_cuda_3d_fused_step_equals_split_kernels(cuda_device, shots, free_surfac
 
 
 @pytest.mark.gpu
-def test_cuda_3d_fused_step_at_the_benchmark_size(cuda_device):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_cuda_3d_fused_step_at_the_benchmark_size(cuda_device, mode):
     """The 200^3 + 20-cell PML model with 4 shots (the 3-D rate workload),
     20 steps: traces and energies of the fused step equal the split kernels'
     bit for bit."""
@@ -332,8 +335,8 @@ def test_cuda_3d_fused_step_at_the_benchmark_size(cuda_device):
              src_x=np.linspace(10, nx - 10, shots).astype(np.int64), src_y=np.full(shots, ny // 2),
              src_z=np.ones(shots, np.int64), src_v=np.tile(w, (shots, 1)), rcv_x=np.arange(0, nx, 2),
              rcv_y=np.full(nx // 2, ny // 2), rcv_z=np.ones(nx // 2, np.int64))
-    split = _with_step_kernel(False, lambda: run3(c, cuda_device))
-    fused = _with_step_kernel(True, lambda: run3(c, cuda_device))
+    split = _with_step_kernel(0, lambda: run3(c, cuda_device))
+    fused = _with_step_kernel(mode, lambda: run3(c, cuda_device))
     for k in KEYS:
         np.testing.assert_array_equal(fused[k], split[k], err_msg=k)
     assert np.abs(fused["p"]).max() > 0

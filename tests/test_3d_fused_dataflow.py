@@ -308,6 +308,11 @@ def test_fused_dataflow_equals_split_step(nz, ny, nx, pml, S, free_surface, chun
     run_case(nz, ny, nx, pml, S, free_surface, chunk)
 
 
+@pytest.mark.parametrize("free_surface", [False, True])
+def test_fused_dataflow_with_16_row_tiles(free_surface):
+    run_case(12, 25, 14, 3, 2, free_surface, 5, TY=16)
+
+
 def test_chunk_choice_fills_waves():
     """f3_chunks (gb_capi3d.cu) restated: the chosen chunk count for the
     200^3 + 20 PML, 4-shot workload (60 tiles of 8 x 120) on 148 SMs x 2."""
