@@ -41,6 +41,7 @@ struct AdjArgs {
     int img_fmt;                             // storage format of the imaging fields (kImg*)
     float *G1, *C1, *G2, *C2;                // [n_groups][plane] sums and compensations
     int grp0, grp_count;             // shot groups this launch covers
+    const int *tile_order;           // the tiles in dispatch order (blockIdx / grp_count), or null: in index order
     int *err;
     // dL/dwavelet [S][nt] (or null): dt * lambda_p at the source cell after
     // stage A, i.e. the adjoint of p just after the source was added
@@ -380,7 +381,8 @@ adj_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ 
                 const __grid_constant__ CUtensorMap mA2, const AdjArgs A)
 {
     const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
-    const int tile = (int)(blockIdx.x / A.grp_count);
+    const int rank = (int)(blockIdx.x / A.grp_count);
+    const int tile = A.tile_order ? A.tile_order[rank] : rank;
     adj_body<R, TZ, FS, RHO, IMGF>(&mP, &mVX, &mVZ, &mA1, &mA2, A, group, tile);
 }
 

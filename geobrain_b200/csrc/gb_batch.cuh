@@ -78,8 +78,9 @@ fwd_batch_kernel(const int4 *__restrict__ items, const BatchModel *__restrict__ 
     }
     __syncthreads();
     const BatchMaps &mp = maps[item.x];
-    fwd_body<R, TZ, FS, ENERGY, IMG>(&mp.fld[par][0], &mp.fld[par][1], &mp.fld[par][2], &mp.a1, &mp.a2, A, item.z,
-                                     item.y);
+    const int s0 = item.z * A.g.shots_per_cta;
+    fwd_body<R, TZ, FS, ENERGY, IMG>(&mp.fld[par][0], &mp.fld[par][1], &mp.fld[par][2], &mp.a1, &mp.a2, A, item.y, s0,
+                                     min(A.g.n_shots - s0, A.g.shots_per_cta));
 }
 
 // IMGF: the imaging format every model of the batch stores (kImg*), or -1

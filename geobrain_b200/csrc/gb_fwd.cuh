@@ -61,6 +61,9 @@ struct FwdArgs {
     long long img_step;
     int img_t0;
     int grp0, grp_count;             // shot groups this launch covers
+    // the launch's work list: CTA b does shots [y, y + z) of tile x of
+    // items[b]; null: CTA b does group grp0 + b % grp_count of tile b / grp_count
+    const int4 *items;
     int *err;
     // CPML option (null otherwise): profiles [bz, az (integer rows), bz, az
     // (half rows)][Nz] then [bx, ax (integer cols), bx, ax (half cols)][pitch],
@@ -108,13 +111,13 @@ __device__ __forceinline__ bool tile_is_interior(const StepGeom &g, int z0, int 
 
 // IMG: 0 no imaging fields; 1 store I = -div(v^n) on the p mask (velocity
 // gradient); 2 also store Jx = dx(p), Jz = dz(p) on the vx / vz masks (density).
-// The body of one CTA: tile `tile`, shot group `group` of the model A
-// describes; the maps are the TMA descriptors of the input state and of the
-// a1 / a2 planes.
+// The body of one CTA: shots [s0, s0 + ns) (ns <= kMaxShotsPerCta) of tile
+// `tile` of the model A describes; the maps are the TMA descriptors of the
+// input state and of the a1 / a2 planes.
 template <int R, int TZ, bool FS, bool ENERGY, int IMG>
 __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMap *mVX, const CUtensorMap *mVZ,
                                          const CUtensorMap *mA1, const CUtensorMap *mA2,
-                                         const FwdArgs &__restrict__ A, const int group, const int tile)
+                                         const FwdArgs &__restrict__ A, const int tile, const int s0, const int ns)
 {
     using G = Geo<R, TZ>;
     using SM = StepSmem<R, TZ>;
@@ -127,8 +130,6 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
 
     const int z0 = (tile / g.tiles_x) * TZ;
     const int x0 = (tile % g.tiles_x) * TX;
-    const int s0 = group * g.shots_per_cta;
-    const int ns = min(g.n_shots - s0, g.shots_per_cta);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     if (threadIdx.x == 0) {
@@ -442,16 +443,26 @@ __device__ __forceinline__ void fwd_body(const CUtensorMap *mP, const CUtensorMa
 
 // Single-model launch: blockIdx covers shot groups [grp0, grp0 + grp_count)
 // of every tile (one launch for all groups, or one per group when the groups
-// run on their own streams).
+// run on their own streams), in the order of the work list when there is one.
 template <int R, int TZ, bool FS, bool ENERGY, int IMG>
 __global__ void __launch_bounds__(NTHR, TZ <= 16 ? 2 : 1)
 fwd_step_kernel(const __grid_constant__ CUtensorMap mP, const __grid_constant__ CUtensorMap mVX,
                 const __grid_constant__ CUtensorMap mVZ, const __grid_constant__ CUtensorMap mA1,
                 const __grid_constant__ CUtensorMap mA2, const FwdArgs A)
 {
-    const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
-    const int tile = (int)(blockIdx.x / A.grp_count);
-    fwd_body<R, TZ, FS, ENERGY, IMG>(&mP, &mVX, &mVZ, &mA1, &mA2, A, group, tile);
+    int tile, s0, ns;
+    if (A.items) {
+        const int4 w = A.items[blockIdx.x];
+        tile = w.x;
+        s0 = w.y;
+        ns = w.z;
+    } else {
+        const int group = A.grp0 + (int)(blockIdx.x % A.grp_count);
+        tile = (int)(blockIdx.x / A.grp_count);
+        s0 = group * A.g.shots_per_cta;
+        ns = min(A.g.n_shots - s0, A.g.shots_per_cta);
+    }
+    fwd_body<R, TZ, FS, ENERGY, IMG>(&mP, &mVX, &mVZ, &mA1, &mA2, A, tile, s0, ns);
 }
 
 template <int R, int TZ>

@@ -144,6 +144,12 @@ class Plan:
         _lib.check(self._lib.gb_plan_set_group_streams(self.h, int(enable)))
         self.group_streams = bool(enable)
 
+    def set_schedule(self, mode: int) -> None:
+        """Order of the tile kernels' CTAs (gb_plan_set_schedule): 0 =
+        blockIdx order (default), 1 = the slow-path tiles first and the
+        forward's last items split in two.  Results are the same either way."""
+        _lib.check(self._lib.gb_plan_set_schedule(self.h, int(mode)))
+
     def set_graph_steps(self, steps: int) -> None:
         """Plain forward as replays of a CUDA graph of `steps` steps (0 = off)."""
         _lib.check(self._lib.gb_plan_set_graph_steps(self.h, int(steps)))

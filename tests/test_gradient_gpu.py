@@ -88,6 +88,29 @@ def test_group_streams_do_not_change_results(cuda_device):
     assert a[2] == b[2]
 
 
+@pytest.mark.parametrize("imaging_cache", [0, "auto"])
+def test_cta_schedule_does_not_change_gradient(cuda_device, imaging_cache):
+    """The guided CTA order against blockIdx order: the gradients and the
+    loss bit for bit (each (group, cell) gradient sum keeps one owner and
+    its time order)."""
+    from geobrain_b200.wave import engine
+    c = load_case("small_fs")
+    geo = engine.Geometry(c["nz"], c["nx"], c["nabc"], c["nt"], c["dt"], c["dx"], 2, True)
+    plan = engine.get_plan(geo, c["src_x"], c["src_z"], c["rcv_x"], c["rcv_z"])
+    plan.set_tiling(16, 1)                 # three groups of one shot
+    try:
+        plan.set_schedule(0)
+        a = cuda_grad(c, cuda_device, imaging_cache=imaging_cache, checkpoint_every=50)
+        plan.set_schedule(1)
+        b = cuda_grad(c, cuda_device, imaging_cache=imaging_cache, checkpoint_every=50)
+    finally:
+        plan.set_schedule(0)
+        plan.set_tiling(16, 0)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    assert a[2] == b[2]
+
+
 @pytest.mark.parametrize("fmt,every,tol", [("fp24", 10, GTOL), ("fp24", 20, GTOL), ("fp16", 20, 1e-3),
                                            ("bf16", 20, 1e-2)])
 def test_short_checkpoints_within_budget(cuda_device, fmt, every, tol):
