@@ -7,6 +7,7 @@
 #include "gb_3d_fused.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -20,8 +21,8 @@ namespace {
 // 1 / 2: one step3_fused_kernel launch per step (per 8 shots with energy
 // maps) with tiles of 8 / 16 rows, the state ping-ponging between two
 // buffers; 0 (default): p3_kernel + v3_kernel in place, the faster as
-// measured.
-int g_step3_fused = 0;
+// measured.  Each call reads it once: its layout and its kernels agree.
+std::atomic<int> g_step3_fused{0};
 
 using F3Fn = void (*)(const CUtensorMap, const CUtensorMap, const CUtensorMap, const Fused3Args);
 
@@ -98,9 +99,9 @@ int f3_chunks(const Geo3 &g, int tiles, int ns, int slots)
     return best;
 }
 
-int fused3_setup(const Geo3 &g, float *buf0, float *buf1, const float *coef, bool energy, Fused3 *F)
+int fused3_setup(const Geo3 &g, float *buf0, float *buf1, const float *coef, bool energy, int mode, Fused3 *F)
 {
-    const F3Shape &sh = f3_shape_of(g_step3_fused);
+    const F3Shape &sh = f3_shape_of(mode);
     F->shape = &sh;
     F->buf[0] = buf0;
     F->buf[1] = buf1;
@@ -173,9 +174,7 @@ extern "C" {
 
 int gb3_set_fused_step(int32_t on)
 {
-    const int prev = g_step3_fused;
-    g_step3_fused = (on == 1 || on == 2) ? on : 0;
-    return prev;
+    return g_step3_fused.exchange((on == 1 || on == 2) ? on : 0);
 }
 
 namespace {
@@ -201,13 +200,14 @@ bool geo3_of(const gb3_model_desc *d, Geo3 *g)
     return true;
 }
 
-Layout3 layout3(const Geo3 &g)
+// mode: the step kernels (gb3_set_fused_step) the layout is for
+Layout3 layout3(const Geo3 &g, int mode)
 {
     Layout3 L{};
     size_t o = 0;
     L.err = o; o = align256(o + 4);
     L.state = o; o = align256(o + (size_t)g.n_shots * 4 * g.vol * 4);
-    L.state2 = o; o = align256(o + (g_step3_fused ? (size_t)g.n_shots * 4 * g.vol * 4 : 0));
+    L.state2 = o; o = align256(o + (mode ? (size_t)g.n_shots * 4 * g.vol * 4 : 0));
     L.coef = o; o = align256(o + 6 * (size_t)g.vol * 4);
     L.src = o; o = align256(o + 3 * (size_t)g.n_shots * 4);
     L.rcv = o; o = align256(o + 3 * (size_t)std::max(g.n_rcv, 1) * 4);
@@ -221,7 +221,7 @@ size_t gb3_workspace_bytes(const gb3_model_desc *desc)
 {
     Geo3 g;
     if (!geo3_of(desc, &g)) return 0;
-    return layout3(g).total + 256;
+    return layout3(g, g_step3_fused.load()).total + 256;
 }
 
 size_t gb3_checkpoint_bytes(const gb3_model_desc *desc, int32_t checkpoint_every)
@@ -292,7 +292,8 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
     if (!vp || !rho || !damp || !wavelet) return fail(GB_E_ARG, "null argument");
     if (!(desc->dt > 0.f) || !(desc->dz > 0.f)) return fail(GB_E_ARG, "dt and dz must be positive");
     if (g.Nz > 65535) return fail(GB_E_ARG, "at most 65535 padded z planes");
-    const Layout3 L = layout3(g);
+    const int mode = g_step3_fused.load();
+    const Layout3 L = layout3(g, mode);
     char *ws = aligned_ws(workspace);
     if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
         return fail(GB_E_WORKSPACE, "workspace too small");
@@ -333,7 +334,7 @@ int gb3_forward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t 
     Fused3 FU{};
     Fused3Args FA{};
     if (fused) {
-        if (int rc = fused3_setup(g, state, state2, coef, want_energy, &FU)) return rc;
+        if (int rc = fused3_setup(g, state, state2, coef, want_energy, mode, &FU)) return rc;
         FA.free_surface = fs;
         FA.a2 = A.a2; FA.k2 = A.k2; FA.k3 = A.k3; FA.k4 = A.k4;
         FA.src = d_src;
@@ -370,14 +371,14 @@ struct Layout3B {
     size_t err, state, state2, coef, src, rcv, lam_a, lam_b, img_i, img_j, g1, c1, g2, c2, total;
 };
 
-Layout3B layout3b(const Geo3 &g, int K, bool rho)
+Layout3B layout3b(const Geo3 &g, int K, bool rho, int mode)
 {
     Layout3B L{};
     size_t o = 0;
     const size_t st = (size_t)g.n_shots * 4 * g.vol * 4, f = (size_t)g.n_shots * g.vol * 4;
     L.err = o; o = align256(o + 4);
     L.state = o; o = align256(o + st);
-    L.state2 = o; o = align256(o + (g_step3_fused && K > 0 ? st : 0));
+    L.state2 = o; o = align256(o + (mode && K > 0 ? st : 0));
     L.coef = o; o = align256(o + 6 * (size_t)g.vol * 4);
     L.src = o; o = align256(o + 3 * (size_t)g.n_shots * 4);
     L.rcv = o; o = align256(o + 3 * (size_t)std::max(g.n_rcv, 1) * 4);
@@ -406,7 +407,7 @@ size_t gb3_backward_workspace_bytes(const gb3_model_desc *desc, int32_t checkpoi
 {
     Geo3 g;
     if (!geo3_of(desc, &g) || checkpoint_every < 0) return 0;
-    return layout3b(g, std::min<int>(checkpoint_every, g.nt), with_rho != 0).total + 256;
+    return layout3b(g, std::min<int>(checkpoint_every, g.nt), with_rho != 0, g_step3_fused.load()).total + 256;
 }
 
 int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t *src_y, const int64_t *src_z,
@@ -428,7 +429,8 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
         return fail(GB_E_ARG, "the density gradient needs imaging fields kept with imaging_rho");
     // with every step's imaging fields there is no recompute and no segment buffer
     const int K = imaging ? 0 : std::min<int>(checkpoint_every, g.nt);
-    const Layout3B L = layout3b(g, K, with_rho);
+    const int mode = g_step3_fused.load();
+    const Layout3B L = layout3b(g, K, with_rho, mode);
     char *ws = aligned_ws(workspace);
     if (!workspace || workspace_bytes < L.total + (size_t)(ws - reinterpret_cast<char *>(workspace)))
         return fail(GB_E_WORKSPACE, "workspace too small");
@@ -477,7 +479,7 @@ int gb3_backward(const gb3_model_desc *desc, const int64_t *src_x, const int64_t
     Fused3 FU{};
     Fused3Args FA{};
     if (fused) {
-        if (int rc = fused3_setup(g, state, state2, coef, false, &FU)) return rc;
+        if (int rc = fused3_setup(g, state, state2, coef, false, mode, &FU)) return rc;
         FA.free_surface = fs;
         FA.a2 = F.a2; FA.k2 = F.k2; FA.k3 = F.k3; FA.k4 = F.k4;
         FA.src = d_src;
