@@ -66,6 +66,8 @@ SIGNATURES = {
     "gb_plan_set_group_streams": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_plan_set_graph_steps": (ctypes.c_int, [_P, ctypes.c_int]),
     "gb_plan_set_schedule": (ctypes.c_int, [_P, ctypes.c_int]),
+    "gb_plan_schedule_items": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _P, ctypes.c_int,
+                                              ctypes.POINTER(ctypes.c_int)]),
     "gb_plan_set_resident": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
     "gb_plan_launch_calls": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_longlong)]),
     "gb_plan_get_resident": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),

@@ -1398,6 +1398,25 @@ int gb_plan_set_schedule(gb_plan *p, int mode)
     return GB_OK;
 }
 
+int gb_plan_schedule_items(gb_plan *p, int slots, int config, int32_t *items, int cap, int *n_items)
+{
+    if (!p || !n_items) return fail(GB_E_ARG, "null argument");
+    if (slots < 1 || config < 0 || config > p->n_groups || cap < 0) return fail(GB_E_ARG, "invalid slots or configuration");
+    build_schedule(p, slots);
+    const int n = p->sched_cnt[config];
+    *n_items = n;
+    if (items) {
+        if (cap < n) return fail(GB_E_ARG, "item buffer too small");
+        const int4 *src = p->sched_items.data() + p->sched_off[config];
+        for (int i = 0; i < n; ++i) {
+            items[3 * i] = src[i].x;
+            items[3 * i + 1] = src[i].y;
+            items[3 * i + 2] = src[i].z;
+        }
+    }
+    return GB_OK;
+}
+
 int gb_plan_set_graph_steps(gb_plan *p, int steps)
 {
     if (!p) return fail(GB_E_ARG, "null plan");

@@ -129,6 +129,13 @@ int gb_plan_set_graph_steps(gb_plan *plan, int steps);
  * are the same either way; energy sums are atomic in both. */
 int gb_plan_set_schedule(gb_plan *plan, int mode);
 
+/* The forward work list that schedule mode 1 builds for `slots` resident
+ * CTAs (no device call).  config g < n_groups: the launch of shot group g
+ * alone (group streams); config n_groups: one launch of every group.
+ * Writes *n_items, and, when items is not NULL (cap >= *n_items), the items
+ * as (tile, first shot, shots) triples. */
+int gb_plan_schedule_items(gb_plan *plan, int slots, int config, int32_t *items, int cap, int *n_items);
+
 /* Autotuner.  Times `steps` plain forward steps of this plan (no traces, no
  * energy) for each launch configuration:
  *   - tile rows 16 / 32;
